@@ -1,0 +1,230 @@
+"""Small seeded scenarios that pin the solver path, shared by every runner.
+
+Each case is a plain dict of numpy inputs plus a stepping recipe. The same case is
+run (a) through the reference's own kernel source by ``make_golden.py`` to make the
+committed fixtures, (b) through the CPU oracle by ``tests/test_oracle_golden.py``,
+and (c) through the CUDA path by the GPU parity tests. Sizes are small on purpose:
+the reference run goes through a per-thread Python interpreter.
+
+Every optional physics branch of the reference step is reached by at least one
+case: the donor limiter, closed/open/fixed_stage edges, compensated and plain
+uniform rain, compensated and plain rain fields, infiltration, inflow point sources
+(compensated), bedload accumulation with Exner activations and bounds, wet/dry
+fronts, dry cells and one-row domains.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+
+EDGES = ("north", "south", "east", "west")
+
+
+def _bc(**kw):
+    return {e: kw.get(e, "closed") for e in EDGES}
+
+
+def _bumps(ny, nx, dx, rng, n_bumps, amp, sigma):
+    yy, xx = np.mgrid[0:ny, 0:nx].astype(np.float64)
+    z = np.zeros((ny, nx))
+    for _ in range(n_bumps):
+        a = rng.uniform(*amp)
+        s = rng.uniform(*sigma)
+        cy, cx = rng.uniform(0, ny), rng.uniform(0, nx)
+        z += a * np.exp(-(((yy - cy) ** 2 + (xx - cx) ** 2) * dx * dx) / (2 * s * s))
+    return z
+
+
+def case_li_closed_random():
+    rng = np.random.default_rng(0)
+    bed = rng.uniform(0.0, 5.0, size=(6, 7)).astype(np.float32)
+    depth = rng.uniform(0.5, 3.0, size=(6, 7)).astype(np.float32)
+    return dict(scheme="local_inertial", bed=bed, dx=5.0, depth=depth, manning=0.03,
+                steps=10, alpha=0.5, dt_max=5.0)  # fmt: skip
+
+
+def case_li_steep_sheet():
+    ny = nx = 12
+    yy = np.arange(ny)[:, None] * np.ones((1, nx))
+    bed = (yy * 5.0).astype(np.float32)
+    return dict(scheme="local_inertial", bed=bed, dx=10.0, depth=0.005, manning=0.03,
+                steps=25, alpha=0.7, dt_max=5.0)  # fmt: skip
+
+
+def case_li_rain_open_infil():
+    rng = np.random.default_rng(1)
+    ny, nx, dx = 10, 12, 10.0
+    xx = np.broadcast_to(np.arange(nx), (ny, nx))
+    bed = (1e-2 * (nx - 1 - xx) * dx + _bumps(ny, nx, dx, rng, 4, (0.1, 0.6), (10, 30))).astype(np.float32)
+    infil = rng.uniform(0.0, 20.0, size=(ny, nx)) / 1000.0 / 3600.0
+    return dict(scheme="local_inertial", bed=bed, dx=dx, depth=0.05, manning=0.03,
+                boundaries=_bc(east="open", south="open"), infil=infil.astype(np.float32),
+                compensated=True, rain=50.0 / 1000.0 / 3600.0, steps=20, alpha=0.7, dt_max=5.0)  # fmt: skip
+
+
+def case_li_rain_field_plain():
+    rng = np.random.default_rng(2)
+    ny, nx, dx = 9, 8, 10.0
+    bed = rng.uniform(0.0, 0.3, size=(ny, nx)).astype(np.float32)
+    rain = ((np.arange(ny * nx).reshape(ny, nx) + 1.0) * 2.0 / 1000.0 / 3600.0).astype(np.float32)
+    manning = rng.uniform(0.02, 0.06, size=(ny, nx)).astype(np.float32)
+    return dict(scheme="local_inertial", bed=bed, dx=dx, depth=0.1, manning=manning, rain_field=rain,
+                rain_scale=1.0, boundaries=_bc(west="open"), steps=15, alpha=0.7, dt_max=5.0)  # fmt: skip
+
+
+def case_li_rain_field_comp():
+    rng = np.random.default_rng(3)
+    ny, nx, dx = 8, 9, 20.0
+    bed = rng.uniform(0.0, 0.5, size=(ny, nx)).astype(np.float32)
+    rain = rng.uniform(1e-6, 2e-5, size=(ny, nx)).astype(np.float32)
+    return dict(scheme="local_inertial", bed=bed, dx=dx, depth=0.2, manning=0.035, rain_field=rain,
+                compensated=True, rain_scale=1.0, boundaries=_bc(north="open", west="open"),
+                steps=12, alpha=0.7, dt_max=10.0)  # fmt: skip
+
+
+def case_li_inflow():
+    ny = nx = 10
+    bed = np.zeros((ny, nx), np.float32)
+    inflows = [((3, 3), [(0.0, 0.0), (30.0, 4.0), (90.0, 0.0)]), ((6, 7), [(0.0, 1.5), (200.0, 1.5)])]
+    return dict(scheme="local_inertial", bed=bed, dx=10.0, depth=0.05, manning=0.03, inflows=inflows,
+                steps=20, alpha=0.5, dt_max=5.0)  # fmt: skip
+
+
+def case_li_sediment():
+    ny, nx, dx = 8, 14, 5.0
+    xx = np.broadcast_to(np.arange(nx), (ny, nx)).astype(np.float64)
+    yy = np.arange(ny)[:, None] * np.ones((1, nx))
+    bed = (0.01 * (nx - 1 - xx) * dx + 0.05 * np.cos(yy * 0.7) + 0.03 * np.sin(xx * 1.3)).astype(np.float32)
+    qx0 = np.zeros((ny, nx + 1), np.float32)
+    qx0[:, 1:nx] = 0.8
+    d50 = np.full((ny, nx), 0.002, np.float32)
+    d50[2:4, 5:9] = 0.004
+    lo = np.full((ny, nx), -np.inf, np.float32)
+    hi = np.full((ny, nx), np.inf, np.float32)
+    lo[:, 3:6] = -0.002  # an alluvium floor
+    lo[4, 10] = hi[4, 10] = 0.0  # a frozen structure cell
+    return dict(scheme="local_inertial", bed=bed, dx=dx, depth=0.5, manning=0.03, qx0=qx0,
+                boundaries=_bc(east="open"), sediment=dict(d50=d50, porosity=0.4, every=10, dz_lo=lo, dz_hi=hi),
+                steps=25, alpha=0.7, dt_max=2.0)  # fmt: skip
+
+
+def case_li_dambreak_row():
+    nx, dx = 40, 0.5
+    x = (np.arange(nx) + 0.5 - nx / 2.0) * dx
+    depth = np.where(x < 0.0, 1.0, 0.3).astype(np.float32).reshape(1, nx)
+    return dict(scheme="local_inertial", bed=np.zeros((1, nx), np.float32), dx=dx, depth=depth,
+                manning=0.01, steps=15, alpha=0.7, dt_max=8.0)  # fmt: skip
+
+
+def _hllc_bumpy(ny, nx, dx):
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    return (0.5 * np.sin(xx * 0.2) + 0.002 * xx * dx + 0.3 * np.cos(yy * 0.3)).astype(np.float32)
+
+
+def case_hllc_bumpy_moving():
+    ny, nx, dx = 10, 12, 10.0
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    depth = (0.5 + 0.3 * np.sin(xx * 0.5 + yy * 0.3)).astype(np.float32)
+    return dict(scheme="hllc_fv", bed=_hllc_bumpy(ny, nx, dx), dx=dx, depth=depth, manning=0.03,
+                rain=1e-5, steps=12, alpha=0.45, dt_max=5.0)  # fmt: skip
+
+
+def case_hllc_open_comp_infil():
+    rng = np.random.default_rng(4)
+    ny, nx, dx = 10, 11, 10.0
+    bed = rng.uniform(0.0, 0.4, size=(ny, nx)).astype(np.float32)
+    depth = rng.uniform(0.2, 0.8, size=(ny, nx)).astype(np.float32)
+    hu0 = rng.uniform(-0.3, 0.3, size=(ny, nx)).astype(np.float32)
+    hv0 = rng.uniform(-0.3, 0.3, size=(ny, nx)).astype(np.float32)
+    infil = rng.uniform(0.0, 3e-5, size=(ny, nx)).astype(np.float32)
+    return dict(scheme="hllc_fv", bed=bed, dx=dx, depth=depth, manning=0.035, hu0=hu0, hv0=hv0,
+                boundaries=_bc(west="open", north="open"), infil=infil, compensated=True,
+                rain=20.0 / 1000.0 / 3600.0, steps=10, alpha=0.45, dt_max=5.0)  # fmt: skip
+
+
+def case_hllc_stage():
+    ny, nx, dx = 8, 10, 10.0
+    xx = np.broadcast_to(np.arange(nx), (ny, nx))
+    bed = (0.01 * xx * dx * 0.1).astype(np.float32)
+    return dict(scheme="hllc_fv", bed=bed, dx=dx, depth=0.5, manning=0.03,
+                boundaries=_bc(east="fixed_stage", west="open"),
+                stage_curves={"east": [(0.0, 0.6), (20.0, 0.9), (60.0, 0.9)]},
+                steps=10, alpha=0.45, dt_max=5.0)  # fmt: skip
+
+
+def case_hllc_shoreline():
+    ny = nx = 14
+    dx = 5.0
+    yy, xx = np.mgrid[0:ny, 0:nx].astype(float)
+    z = 0.05 * ((xx - 6.5) ** 2 + (yy - 6.5) ** 2)
+    z += 2.6 * np.exp(-(((xx - 4) ** 2 + (yy - 7) ** 2) / 4.0))
+    z += 3.2 * np.exp(-(((xx - 9) ** 2 + (yy - 5) ** 2) / 5.0))
+    z = z.astype(np.float32)
+    h0 = np.maximum(3.0 - z, 0.0).astype(np.float32)
+    return dict(scheme="hllc_fv", bed=z, dx=dx, depth=h0, manning=0.03, steps=10, alpha=0.45, dt_max=5.0)
+
+
+def case_hllc_rain_field_plain():
+    rng = np.random.default_rng(5)
+    ny, nx, dx = 8, 8, 10.0
+    bed = rng.uniform(0.0, 0.2, size=(ny, nx)).astype(np.float32)
+    rain = rng.uniform(0.0, 3e-5, size=(ny, nx)).astype(np.float32)
+    infil = rng.uniform(0.0, 1e-5, size=(ny, nx)).astype(np.float32)
+    return dict(scheme="hllc_fv", bed=bed, dx=dx, depth=0.3, manning=0.03, rain_field=rain, rain_scale=1.0,
+                infil=infil, boundaries=_bc(south="open"), steps=8, alpha=0.45, dt_max=5.0)  # fmt: skip
+
+
+def case_hllc_dambreak_row():
+    nx, dx = 40, 0.5
+    x = (np.arange(nx) + 0.5 - nx / 2.0) * dx
+    depth = np.where(x < 0.0, 1.0, 0.3).astype(np.float32).reshape(1, nx)
+    return dict(scheme="hllc_fv", bed=np.zeros((1, nx), np.float32), dx=dx, depth=depth, manning=0.01,
+                steps=15, alpha=0.45, dt_max=8.0)  # fmt: skip
+
+
+def case_hllc_dry_front_row():
+    nx, dx = 30, 0.5
+    x = (np.arange(nx) + 0.5 - nx / 2.0) * dx
+    depth = np.where(x < 0.0, 1.0, 0.0).astype(np.float32).reshape(1, nx)
+    return dict(scheme="hllc_fv", bed=np.zeros((1, nx), np.float32), dx=dx, depth=depth, manning=0.0,
+                boundaries=_bc(east="open", west="open"), steps=15, alpha=0.45, dt_max=6.0)  # fmt: skip
+
+
+CASES = {
+    name[len("case_"):]: fn
+    for name, fn in sorted(globals().items())
+    if name.startswith("case_") and callable(fn)
+}
+
+
+def run_case(case: dict, api) -> dict:
+    """Step ``case`` through ``api`` and return the recorded outputs.
+
+    ``api`` adapts one implementation (reference, oracle or CUDA) to a fixed set of
+    calls: ``make_state(case)``, ``compute_dt(st, alpha, dt_max)``,
+    ``step(st, dt, rain, rain_scale, t)``, ``injector(case, st)`` returning an object
+    with ``apply(st, t, dt)``, ``morphology(case, st)`` returning an object with
+    ``advance(t, elapsed)``, and ``outputs(st, case)`` returning a dict of arrays.
+    """
+    st = api.make_state(case)
+    inj = api.injector(case, st) if case.get("inflows") else None
+    morph = api.morphology(case, st) if case.get("sediment") else None
+    every = case["sediment"]["every"] if morph else 0
+    t = 0.0
+    dts, vols = [], []
+    last_act = 0.0
+    for k in range(case["steps"]):
+        dt = api.compute_dt(st, case["alpha"], case["dt_max"])
+        dts.append(dt)
+        if inj is not None:
+            vols.append(inj.apply(st, t, dt))
+        api.step(st, dt, case.get("rain", 0.0), case.get("rain_scale", 1.0), t)
+        t += dt
+        if morph is not None and (k + 1) % every == 0:
+            morph.advance(t, t - last_act)
+            last_act = t
+    out = api.outputs(st, case)
+    out["dts"] = np.asarray(dts, np.float64)
+    if inj is not None:
+        out["inflow_volumes"] = np.asarray(vols, np.float64)
+    return out
