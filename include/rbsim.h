@@ -1,0 +1,165 @@
+/*
+ * rbsim.h -- C ABI of librbsim.so, the B200 solver hot path of river-basin-sim.
+ *
+ * The reference path is Python driving NVIDIA Warp kernels behind a scheme module
+ * with two calls (solver/core/schemes.py:1-26, :41-52):
+ *     compute_dt(state, alpha, dt_max) -> float
+ *     step(state, dt, rain, rain_scale, t)      (LI adds limit=True)
+ * plus the point-source injector (solver/processes/inflow.py:167), the Exner
+ * activation (solver/processes/morphology.py:223) and the float64 mass ledger
+ * (solver/core/massbalance.py:66). This header is what a ctypes binding of that
+ * seam calls. Conventions:
+ *   - Every buffer is caller-owned device memory (raw pointers; nothing here
+ *     frees or allocates device memory). Library scratch lives in a caller-
+ *     allocated workspace sized by rb_*_workspace_bytes and zeroed once by
+ *     rb_workspace_init.
+ *   - Layout: row-major float32, cells (ny, nx), x-faces (ny, nx+1),
+ *     y-faces (ny+1, nx) (solver/core/grid.py:9-31). qx > 0 flows +x, qy > 0 flows
+ *     +y (increasing row index).
+ *   - Fields that neighbouring cells read (h, qx, qy; h, hu, hv) are double
+ *     buffered: a step reads buffer [cur] and writes buffer [cur ^ 1]. The caller
+ *     flips `cur` after a successful step.
+ *   - `stream` is a cudaStream_t (NULL = legacy default stream). Calls are
+ *     asynchronous unless documented as synchronising; calls on one workspace
+ *     must not overlap.
+ *   - Return value: RB_OK (0) or a negative RB_ERR_*; rb_last_error() gives the
+ *     message of the calling thread's last failure.
+ */
+#ifndef RBSIM_H
+#define RBSIM_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RB_OK 0
+#define RB_ERR_ARG (-1)      /* bad shape, size or pointer (the reference raises ValueError) */
+#define RB_ERR_CUDA (-2)     /* a CUDA runtime call failed */
+#define RB_ERR_DEVICE (-3)   /* a kernel raised a device error bit (see RB_DEVERR_*) */
+#define RB_ERR_TIMEOUT (-4)  /* a bounded device wait expired */
+#define RB_ERR_STEP (-5)     /* non-positive or non-finite timestep (scheduler.py:221-227) */
+
+/* Device error bits, OR-ed into the workspace error word. */
+#define RB_DEVERR_NONFINITE 1u /* a step produced a NaN/inf depth */
+#define RB_DEVERR_CLOCK 2u     /* the device clock produced a non-positive timestep */
+#define RB_DEVERR_STEPS 4u     /* the device clock hit its step budget before its target */
+
+/* Edge order of every per-edge array: north, south, east, west (state.py:35). */
+enum { RB_EDGE_NORTH = 0, RB_EDGE_SOUTH = 1, RB_EDGE_EAST = 2, RB_EDGE_WEST = 3 };
+/* Edge kinds (state.py:84-96). */
+enum { RB_BC_CLOSED = 0, RB_BC_OPEN = 1, RB_BC_STAGE = 2 };
+
+/* Local-inertial state: the arrays of solver/core/state.py:38-96 that the step
+ * touches. Optional physics is armed by a non-NULL pointer, as the reference arms
+ * it by presence (state.py:98-171, sediment.py:658). */
+typedef struct rb_li_fields {
+  int32_t ny, nx;
+  double dx;                 /* Grid.dx (grid.py:52-63) */
+  float *h[2];               /* depth (ny, nx), double buffered */
+  float *qx[2];              /* x-face discharge (ny, nx+1), double buffered */
+  float *qy[2];              /* y-face discharge (ny+1, nx), double buffered */
+  const float *z;            /* bed (ny, nx) */
+  const float *n;            /* Manning roughness (ny, nx) */
+  float *h_comp;             /* Kahan residue of areal sources (sources.py), or NULL */
+  const float *rain_field;   /* rain rate field m/s (state.py:106), or NULL */
+  const float *infil;        /* infiltration rate m/s (state.py:98), or NULL */
+  int32_t bc[4];             /* RB_BC_* per edge; LI honours closed and open */
+  /* Morphology (sediment.py:549-571); d50 == NULL leaves the bed static. */
+  const float *d50;
+  float *qs_int_x, *qs_comp_x; /* (ny, nx+1) transport integral + Kahan residue */
+  float *qs_int_y, *qs_comp_y; /* (ny+1, nx) */
+} rb_li_fields;
+
+/* HLLC state (state.py:52-57, hllc.py:96-152). */
+typedef struct rb_hllc_fields {
+  int32_t ny, nx;
+  double dx;
+  float *h[2], *hu[2], *hv[2]; /* (ny, nx), double buffered */
+  const float *z, *n;
+  float *h_comp;
+  const float *rain_field;
+  const float *infil;
+  int32_t bc[4];               /* closed = reflective wall, open = transmissive + banked,
+                                  fixed_stage = prescribed-surface ghost + banked */
+} rb_hllc_fields;
+
+/* Per-step forcing, as the reference passes it to step(): dt and rain in float64
+ * host precision (each kernel rounds them exactly where the reference does). */
+typedef struct rb_step_args {
+  double dt;          /* seconds */
+  double rain;        /* uniform rain rate, m/s (scalar path) */
+  double rain_scale;  /* temporal multiplier of the rain field */
+  int32_t limit;      /* LI donor limiter (local_inertial.py:551); ignored by HLLC */
+  int32_t reserved;
+  double stage[4];    /* HLLC fixed_stage surface per edge at t + dt/2 (hllc.py:1308-1312) */
+} rb_step_args;
+
+/* --- workspace ----------------------------------------------------------- */
+/* Bytes of library scratch a domain of this size needs (reduction slots, the
+ * error word, per-tile float64 ledger partials, HLLC stage-1 state). */
+size_t rb_li_workspace_bytes(int32_t ny, int32_t nx);
+size_t rb_hllc_workspace_bytes(int32_t ny, int32_t nx);
+/* Zero a workspace (ledger partials, error word). Asynchronous on `stream`. */
+int rb_workspace_init(void *ws, size_t bytes, void *stream);
+
+/* --- local-inertial scheme (solver/core/local_inertial.py) ------------------ */
+/* One step: replaces step() (local_inertial.py:547-727): eta, both face updates
+ * with semi-implicit Manning, closed edges, donor limiter, bedload integral,
+ * continuity, compensated or plain rain, infiltration and open-edge sinks, fused
+ * in one launch. Infiltration and open-edge losses are banked into the
+ * workspace ledger (replacing the per-cell float64 loss_cum). */
+int rb_li_step(const rb_li_fields *f, int32_t cur, const rb_step_args *a, void *ws, void *stream);
+/* Replaces compute_dt() (local_inertial.py:515-544). Synchronising: reduces
+ * max(h) of buffer [cur] on the device and returns dt in *dt_out (host). */
+int rb_li_compute_dt(const rb_li_fields *f, int32_t cur, double alpha, double dt_max, void *ws, void *stream,
+                     double *dt_out);
+
+/* --- HLLC scheme (solver/core/hllc.py) ---------------------------------- */
+/* One SSP-RK2 step: replaces step() (hllc.py:1272-1373) in two launches (one
+ * per Heun stage). Open and fixed_stage boundary flux and infiltration are
+ * banked into the workspace ledger (replacing loss_cum). */
+int rb_hllc_step(const rb_hllc_fields *f, int32_t cur, const rb_step_args *a, void *ws, void *stream);
+/* One Heun stage of rb_hllc_step (stage 1: U^n -> U1 in the workspace; stage 2:
+ * (U^n, U1) -> U^{n+1} with friction and sources). rb_hllc_step == stage 1 then
+ * stage 2; split so a caller can time or interleave the two launches. */
+int rb_hllc_stage(const rb_hllc_fields *f, int32_t cur, const rb_step_args *a, void *ws, void *stream,
+                  int32_t stage);
+/* Replaces compute_dt() (hllc.py:972-990). Synchronising. */
+int rb_hllc_compute_dt(const rb_hllc_fields *f, int32_t cur, double alpha, double dt_max, void *ws, void *stream,
+                       double *dt_out);
+
+/* --- sources, morphology, ledger ---------------------------------------- */
+/* Point sources: replaces the _inject_point_sources[_c] launch of
+ * InflowInjector.apply (inflow.py:74-113, :183-199). comp == NULL adds plainly. */
+int rb_inject_points(float *h, int32_t ny, int32_t nx, int32_t nsrc, const int32_t *rows, const int32_t *cols,
+                     const float *add_depth, float *comp, void *stream);
+/* Exner activation: replaces exner_update + rebuild_bed (sediment.py:383-441) as
+ * launched by MorphologyProcess.advance (morphology.py:261-270); then zeroes the
+ * transport integrals and keeps their Kahan residue (sediment.py:513-524). */
+int rb_exner_apply(int32_t ny, int32_t nx, double dx, float *qs_int_x, float *qs_int_y, const float *dz_lo,
+                   const float *dz_hi, float inv_one_minus_p, double *dz_cum, double *dz_unapplied, const float *z0,
+                   float *z, void *stream);
+/* Ledger outflow: the float64 sum of everything banked into the workspace
+ * ledger since rb_workspace_init, in metres of depth summed over cells (the
+ * reference's loss_cum.sum(), massbalance.py:173-177). Synchronising. */
+int rb_ledger_loss(void *ws, int32_t ny, int32_t nx, void *stream, double *out);
+/* Deterministic float64 sum of a float32 field (the stored-volume term,
+ * massbalance.py:292-295), fixed reduction order. Synchronising. */
+int rb_sum_f64(const float *x, int64_t n, void *ws, size_t ws_bytes, void *stream, double *out);
+/* Read and clear the workspace device error word. Synchronising. */
+int rb_read_device_error(void *ws, void *stream, uint32_t *err_out);
+
+/* --- diagnostics ------------------------------------------------------------ */
+/* Message of this thread's last failed call (empty if none). Returns its length. */
+int rb_last_error(char *buf, size_t n);
+/* Library version and the SM architecture it was built for (e.g. 100). */
+int rb_version(int32_t *major, int32_t *minor, int32_t *sm_arch);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RBSIM_H */

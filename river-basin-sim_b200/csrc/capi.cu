@@ -1,0 +1,346 @@
+// capi.cu -- the extern "C" entry points of librbsim.so (declared in include/rbsim.h).
+//
+// Host-side float64 arithmetic here mirrors the reference's Python exactly where
+// the reference computes in float64 (compute_dt, the open-edge drain factor, the
+// Heun banking weight), and every float32 kernel argument is rounded from the
+// float64 value exactly as Warp rounds a Python float at launch.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+
+#include "rb_common.cuh"
+#include "rb_kernels.h"
+
+namespace {
+
+thread_local char g_err[512] = {0};
+
+int fail(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_err, sizeof g_err, fmt, ap);
+  va_end(ap);
+  return code;
+}
+
+int cuda_fail(cudaError_t e, const char* where) {
+  return fail(RB_ERR_CUDA, "%s: %s (%s)", where, cudaGetErrorString(e), cudaGetErrorName(e));
+}
+
+#define RB_CUDA(call, where)                      \
+  do {                                            \
+    cudaError_t e_ = (call);                      \
+    if (e_ != cudaSuccess) return cuda_fail(e_, where); \
+  } while (0)
+
+inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+int check_grid(int ny, int nx, double dx, const char* who) {
+  if (ny < 1 || nx < 1) return fail(RB_ERR_ARG, "%s: grid %d x %d must be at least 1 x 1", who, ny, nx);
+  if ((long long)ny * (long long)(nx + 1) > (1LL << 40)) return fail(RB_ERR_ARG, "%s: grid too large", who);
+  if (!(dx > 0.0) || !std::isfinite(dx)) return fail(RB_ERR_ARG, "%s: dx must be a positive finite number", who);
+  return RB_OK;
+}
+
+int check_bc(const int32_t* bc, bool allow_stage, const char* who) {
+  for (int e = 0; e < 4; e++) {
+    if (bc[e] < RB_BC_CLOSED || bc[e] > RB_BC_STAGE || (!allow_stage && bc[e] == RB_BC_STAGE))
+      return fail(RB_ERR_ARG, "%s: edge %d has unsupported boundary kind %d", who, e, bc[e]);
+  }
+  return RB_OK;
+}
+
+int check_dt(double dt, const char* who) {
+  if (!(dt > 0.0) || !std::isfinite(dt)) return fail(RB_ERR_STEP, "%s: non-positive timestep %.17g", who, dt);
+  return RB_OK;
+}
+
+rb::WsHeader* header(void* ws) { return static_cast<rb::WsHeader*>(ws); }
+
+bool any_bc(const int32_t* bc, int kind) {
+  return bc[0] == kind || bc[1] == kind || bc[2] == kind || bc[3] == kind;
+}
+
+}  // namespace
+
+namespace rb {
+
+size_t ws_ledger_bytes(int ny, int nx) {
+  const int t = li_tiles(ny, nx) > hllc_tiles(ny, nx) ? li_tiles(ny, nx) : hllc_tiles(ny, nx);
+  return align256((size_t)t * 2 * sizeof(double));
+}
+size_t ws_li_bytes(int ny, int nx) { return WS_LEDGER + ws_ledger_bytes(ny, nx); }
+size_t ws_hllc_u1_offset(int ny, int nx) { return WS_LEDGER + ws_ledger_bytes(ny, nx); }
+size_t ws_hllc_bytes(int ny, int nx) {
+  return ws_hllc_u1_offset(ny, nx) + 3 * align256((size_t)ny * nx * sizeof(float));
+}
+
+}  // namespace rb
+
+extern "C" {
+
+int rb_last_error(char* buf, size_t n) {
+  const int len = (int)strlen(g_err);
+  if (buf != nullptr && n > 0) {
+    strncpy(buf, g_err, n - 1);
+    buf[n - 1] = '\0';
+  }
+  return len;
+}
+
+int rb_version(int32_t* major, int32_t* minor, int32_t* sm_arch) {
+  if (major) *major = 0;
+  if (minor) *minor = 1;
+  if (sm_arch) *sm_arch = 100;
+  return RB_OK;
+}
+
+size_t rb_li_workspace_bytes(int32_t ny, int32_t nx) {
+  if (ny < 1 || nx < 1) return 0;
+  return rb::ws_li_bytes(ny, nx);
+}
+
+size_t rb_hllc_workspace_bytes(int32_t ny, int32_t nx) {
+  if (ny < 1 || nx < 1) return 0;
+  return rb::ws_hllc_bytes(ny, nx);
+}
+
+int rb_workspace_init(void* ws, size_t bytes, void* stream) {
+  if (ws == nullptr || bytes < rb::WS_LEDGER) return fail(RB_ERR_ARG, "rb_workspace_init: workspace too small");
+  RB_CUDA(cudaMemsetAsync(ws, 0, bytes, (cudaStream_t)stream), "rb_workspace_init");
+  return RB_OK;
+}
+
+int rb_li_step(const rb_li_fields* f, int32_t cur, const rb_step_args* a, void* ws, void* stream) {
+  if (f == nullptr || a == nullptr || ws == nullptr) return fail(RB_ERR_ARG, "rb_li_step: null argument");
+  int rc = check_grid(f->ny, f->nx, f->dx, "rb_li_step");
+  if (rc) return rc;
+  if ((rc = check_bc(f->bc, false, "rb_li_step"))) return rc;
+  if ((rc = check_dt(a->dt, "rb_li_step"))) return rc;
+  if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_li_step: cur must be 0 or 1");
+  const int nxt = cur ^ 1;
+  if (!f->h[0] || !f->h[1] || !f->qx[0] || !f->qx[1] || !f->qy[0] || !f->qy[1] || !f->z || !f->n)
+    return fail(RB_ERR_ARG, "rb_li_step: missing state buffer");
+  if (f->d50 && (!f->qs_int_x || !f->qs_comp_x || !f->qs_int_y || !f->qs_comp_y))
+    return fail(RB_ERR_ARG, "rb_li_step: d50 given without the transport accumulators");
+  const bool banks = f->infil != nullptr || any_bc(f->bc, RB_BC_OPEN);
+
+  rb::LiParams p{};
+  p.ny = f->ny;
+  p.nx = f->nx;
+  p.dx32 = (float)f->dx;
+  p.dt32 = (float)a->dt;
+  const bool comp = f->h_comp != nullptr;
+  p.rain_cont = comp ? 0.0f : (float)a->rain;  // local_inertial.py:697
+  p.rain32 = (float)a->rain;
+  p.scale32 = (float)a->rain_scale;
+  p.dxdt = (float)(a->dt / f->dx);  // boundaries.py:329
+  p.limit = a->limit ? 1 : 0;
+  for (int e = 0; e < 4; e++) p.bc[e] = f->bc[e];
+  p.h = f->h[cur];
+  p.qx = f->qx[cur];
+  p.qy = f->qy[cur];
+  p.z = f->z;
+  p.n = f->n;
+  p.h_out = f->h[nxt];
+  p.qx_out = f->qx[nxt];
+  p.qy_out = f->qy[nxt];
+  p.h_comp = f->h_comp;
+  p.rain_field = f->rain_field;
+  p.infil = f->infil;
+  p.d50 = f->d50;
+  p.qs_int_x = f->qs_int_x;
+  p.qs_comp_x = f->qs_comp_x;
+  p.qs_int_y = f->qs_int_y;
+  p.qs_comp_y = f->qs_comp_y;
+  p.ledger = banks ? (double*)((char*)ws + rb::WS_LEDGER) : nullptr;
+  p.hmax_key = nullptr;
+  p.err = &header(ws)->err;
+  RB_CUDA(rb::li_step_launch(p, (cudaStream_t)stream), "rb_li_step launch");
+  return RB_OK;
+}
+
+int rb_li_compute_dt(const rb_li_fields* f, int32_t cur, double alpha, double dt_max, void* ws, void* stream,
+                     double* dt_out) {
+  if (f == nullptr || ws == nullptr || dt_out == nullptr) return fail(RB_ERR_ARG, "rb_li_compute_dt: null argument");
+  int rc = check_grid(f->ny, f->nx, f->dx, "rb_li_compute_dt");
+  if (rc) return rc;
+  if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_li_compute_dt: cur must be 0 or 1");
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned int* key = &header(ws)->red_key;
+  RB_CUDA(rb::reduce_max_h(f->h[cur], (size_t)f->ny * f->nx, key, s), "rb_li_compute_dt reduce");
+  unsigned int host_key = 0;
+  RB_CUDA(cudaMemcpyAsync(&host_key, key, sizeof host_key, cudaMemcpyDeviceToHost, s), "rb_li_compute_dt copy");
+  RB_CUDA(cudaStreamSynchronize(s), "rb_li_compute_dt sync");
+  float hmax32;
+  memcpy(&hmax32, &host_key, sizeof hmax32);
+  // local_inertial.py:540-544, in host float64 as the reference computes it.
+  const double h_max = (double)hmax32;
+  if (h_max <= 1.0e-3) {
+    *dt_out = dt_max;
+    return RB_OK;
+  }
+  const double dt = alpha * f->dx / std::sqrt(9.81 * h_max);
+  *dt_out = dt < dt_max ? dt : dt_max;
+  return RB_OK;
+}
+
+static int hllc_stage_impl(const rb_hllc_fields* f, int32_t cur, const rb_step_args* a, void* ws, void* stream,
+                           int stage_mask) {
+  if (f == nullptr || a == nullptr || ws == nullptr) return fail(RB_ERR_ARG, "rb_hllc_step: null argument");
+  int rc = check_grid(f->ny, f->nx, f->dx, "rb_hllc_step");
+  if (rc) return rc;
+  if ((rc = check_bc(f->bc, true, "rb_hllc_step"))) return rc;
+  if ((rc = check_dt(a->dt, "rb_hllc_step"))) return rc;
+  if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_hllc_step: cur must be 0 or 1");
+  const int nxt = cur ^ 1;
+  if (!f->h[0] || !f->h[1] || !f->hu[0] || !f->hu[1] || !f->hv[0] || !f->hv[1] || !f->z || !f->n)
+    return fail(RB_ERR_ARG, "rb_hllc_step: missing state buffer");
+  const bool banks = f->infil != nullptr || any_bc(f->bc, RB_BC_OPEN) || any_bc(f->bc, RB_BC_STAGE);
+  const size_t cells = (size_t)f->ny * f->nx;
+  char* u1 = (char*)ws + rb::ws_hllc_u1_offset(f->ny, f->nx);
+  const size_t plane = align256(cells * sizeof(float));
+
+  rb::HllcParams p{};
+  p.ny = f->ny;
+  p.nx = f->nx;
+  p.dx32 = (float)f->dx;
+  p.dt32 = (float)a->dt;
+  p.z = f->z;
+  p.n = f->n;
+  p.h1 = (float*)u1;
+  p.hu1 = (float*)(u1 + plane);
+  p.hv1 = (float*)(u1 + 2 * plane);
+  p.h_comp = f->h_comp;
+  p.rain_field = f->rain_field;
+  p.infil = f->infil;
+  p.rain32 = (float)a->rain;
+  p.scale32 = (float)a->rain_scale;
+  const bool comp = f->h_comp != nullptr;
+  p.rain_mode = (comp && f->rain_field == nullptr) ? 1 : (a->rain != 0.0 ? 2 : 0);  // hllc.py:1350-1356
+  for (int e = 0; e < 4; e++) {
+    p.bc[e] = f->bc[e];
+    p.stage[e] = (float)a->stage[e];
+  }
+  p.wt = 0.5 * a->dt / f->dx;  // hllc.py:1320
+  p.ledger = banks ? (double*)((char*)ws + rb::WS_LEDGER) : nullptr;
+  p.err = &header(ws)->err;
+  p.smax_key = nullptr;
+  cudaStream_t s = (cudaStream_t)stream;
+  if (stage_mask & 1) {  // stage 1: U^n -> U1
+    p.h_s = f->h[cur];
+    p.hu_s = f->hu[cur];
+    p.hv_s = f->hv[cur];
+    RB_CUDA(rb::hllc_stage_launch(p, 1, s), "rb_hllc_step stage 1");
+  }
+  if (stage_mask & 2) {  // stage 2: (U^n, U1) -> U^{n+1}
+    p.h_s = p.h1;
+    p.hu_s = p.hu1;
+    p.hv_s = p.hv1;
+    p.h_n = f->h[cur];
+    p.hu_n = f->hu[cur];
+    p.hv_n = f->hv[cur];
+    p.h_out = f->h[nxt];
+    p.hu_out = f->hu[nxt];
+    p.hv_out = f->hv[nxt];
+    RB_CUDA(rb::hllc_stage_launch(p, 2, s), "rb_hllc_step stage 2");
+  }
+  return RB_OK;
+}
+
+int rb_hllc_step(const rb_hllc_fields* f, int32_t cur, const rb_step_args* a, void* ws, void* stream) {
+  return hllc_stage_impl(f, cur, a, ws, stream, 3);
+}
+
+int rb_hllc_stage(const rb_hllc_fields* f, int32_t cur, const rb_step_args* a, void* ws, void* stream,
+                  int32_t stage) {
+  if (stage != 1 && stage != 2) return fail(RB_ERR_ARG, "rb_hllc_stage: stage must be 1 or 2");
+  return hllc_stage_impl(f, cur, a, ws, stream, stage);
+}
+
+int rb_hllc_compute_dt(const rb_hllc_fields* f, int32_t cur, double alpha, double dt_max, void* ws, void* stream,
+                       double* dt_out) {
+  if (f == nullptr || ws == nullptr || dt_out == nullptr) return fail(RB_ERR_ARG, "rb_hllc_compute_dt: null argument");
+  int rc = check_grid(f->ny, f->nx, f->dx, "rb_hllc_compute_dt");
+  if (rc) return rc;
+  if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_hllc_compute_dt: cur must be 0 or 1");
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned int* key = &header(ws)->red_key;
+  RB_CUDA(rb::reduce_wavespeed(f->h[cur], f->hu[cur], f->hv[cur], (size_t)f->ny * f->nx, key, s),
+          "rb_hllc_compute_dt reduce");
+  unsigned int host_key = 0;
+  RB_CUDA(cudaMemcpyAsync(&host_key, key, sizeof host_key, cudaMemcpyDeviceToHost, s), "rb_hllc_compute_dt copy");
+  RB_CUDA(cudaStreamSynchronize(s), "rb_hllc_compute_dt sync");
+  float smax32;
+  memcpy(&smax32, &host_key, sizeof smax32);
+  const double smax = (double)smax32;  // hllc.py:987-990
+  if (smax <= 0.0) {
+    *dt_out = dt_max;
+    return RB_OK;
+  }
+  const double dt = alpha * f->dx / smax;
+  *dt_out = dt < dt_max ? dt : dt_max;
+  return RB_OK;
+}
+
+int rb_inject_points(float* h, int32_t ny, int32_t nx, int32_t nsrc, const int32_t* rows, const int32_t* cols,
+                     const float* add_depth, float* comp, void* stream) {
+  if (ny < 1 || nx < 1 || nsrc < 0) return fail(RB_ERR_ARG, "rb_inject_points: bad sizes");
+  if (nsrc == 0) return RB_OK;
+  if (!h || !rows || !cols || !add_depth) return fail(RB_ERR_ARG, "rb_inject_points: null argument");
+  RB_CUDA(rb::inject_points(h, nx, nsrc, rows, cols, add_depth, comp, (cudaStream_t)stream), "rb_inject_points");
+  return RB_OK;
+}
+
+int rb_exner_apply(int32_t ny, int32_t nx, double dx, float* qs_int_x, float* qs_int_y, const float* dz_lo,
+                   const float* dz_hi, float inv_one_minus_p, double* dz_cum, double* dz_unapplied, const float* z0,
+                   float* z, void* stream) {
+  int rc = check_grid(ny, nx, dx, "rb_exner_apply");
+  if (rc) return rc;
+  if (!qs_int_x || !qs_int_y || !dz_lo || !dz_hi || !dz_cum || !dz_unapplied || !z0 || !z)
+    return fail(RB_ERR_ARG, "rb_exner_apply: null argument");
+  RB_CUDA(rb::exner_apply(ny, nx, (float)dx, inv_one_minus_p, qs_int_x, qs_int_y, dz_lo, dz_hi, dz_cum,
+                          dz_unapplied, z0, z, (cudaStream_t)stream),
+          "rb_exner_apply");
+  return RB_OK;
+}
+
+int rb_ledger_loss(void* ws, int32_t ny, int32_t nx, void* stream, double* out) {
+  if (ws == nullptr || out == nullptr) return fail(RB_ERR_ARG, "rb_ledger_loss: null argument");
+  if (ny < 1 || nx < 1) return fail(RB_ERR_ARG, "rb_ledger_loss: bad grid %d x %d", ny, nx);
+  cudaStream_t s = (cudaStream_t)stream;
+  const size_t nslots = rb::ws_ledger_bytes(ny, nx) / (2 * sizeof(double));
+  const double* ledger = (const double*)((char*)ws + rb::WS_LEDGER);
+  double* partials = (double*)((char*)ws + rb::WS_PARTIALS);
+  double* res = &header(ws)->sum;
+  RB_CUDA(rb::sum_ledger(ledger, nslots, partials, res, s), "rb_ledger_loss");
+  RB_CUDA(cudaMemcpyAsync(out, res, sizeof(double), cudaMemcpyDeviceToHost, s), "rb_ledger_loss copy");
+  RB_CUDA(cudaStreamSynchronize(s), "rb_ledger_loss sync");
+  return RB_OK;
+}
+
+int rb_sum_f64(const float* x, int64_t n, void* ws, size_t ws_bytes, void* stream, double* out) {
+  if (x == nullptr || ws == nullptr || out == nullptr || n < 0 || ws_bytes < rb::WS_LEDGER)
+    return fail(RB_ERR_ARG, "rb_sum_f64: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  double* partials = (double*)((char*)ws + rb::WS_PARTIALS);
+  double* res = &header(ws)->sum;
+  RB_CUDA(rb::sum_f64(x, (size_t)n, partials, res, s), "rb_sum_f64");
+  RB_CUDA(cudaMemcpyAsync(out, res, sizeof(double), cudaMemcpyDeviceToHost, s), "rb_sum_f64 copy");
+  RB_CUDA(cudaStreamSynchronize(s), "rb_sum_f64 sync");
+  return RB_OK;
+}
+
+int rb_read_device_error(void* ws, void* stream, uint32_t* err_out) {
+  if (ws == nullptr || err_out == nullptr) return fail(RB_ERR_ARG, "rb_read_device_error: null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned int host = 0;
+  RB_CUDA(cudaMemcpyAsync(&host, &header(ws)->err, sizeof host, cudaMemcpyDeviceToHost, s), "rb_read_device_error");
+  RB_CUDA(cudaMemsetAsync(&header(ws)->err, 0, sizeof(unsigned int), s), "rb_read_device_error clear");
+  RB_CUDA(cudaStreamSynchronize(s), "rb_read_device_error sync");
+  *err_out = host;
+  return RB_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,434 @@
+// hllc_step.cu -- the well-balanced HLLC finite-volume step (SSP-RK2, Heun).
+//
+// Each Heun stage is one launch; the reference launches ~11 kernels per stage
+// (solver/core/hllc.py:1152-1269 _eval_L) plus the RK, friction and source
+// kernels (:1272-1373):
+//   _primitives (:262) -> _flux_x/_flux_y (:285/:357, _hllc :191, MUSCL-minmod :158,
+//   _dryfactor :174, Audusse hydrostatic reconstruction) -> _apply_boundaries
+//   (:993; walls :442-521, fixed_stage ghosts :537-628) -> _mass_beta (:700) ->
+//   _limit_fx/_limit_fy (:739/:758) -> _bank_* (:638-677) -> _accumulate (:776) ->
+//   _rk_stage1 (:850)                      [stage 1]
+//   _rk_stage2 (:881) -> _friction (:912) -> rain / rain field / infiltration
+//   (:1350-1373) -> _reduce_wavespeed (:948) for the next dt   [stage 2]
+//
+// Tiling. A CTA owns a TX x TY tile of cells. The limited mass flux of a tile face
+// needs the beta of both neighbouring cells, and a beta needs the four faces of
+// its cell, each of which reads a 4-cell MUSCL stencil: a halo of 3 cells of
+// (h, u, v, z) is staged in shared memory with edge-clamped indices (exactly the
+// reference's _cget transmissive ghosts). Mass fluxes are computed for the tile's
+// faces plus a 1-cell ring (for beta), the momentum components only for the tile's
+// own faces. Stage 1 writes U1 = (h1, hu1, hv1) to workspace buffers; stage 2
+// reads U1 with the halo and U^n on the tile and writes U^{n+1} to the other
+// buffer of the caller's double-buffered (h, hu, hv).
+#include <cfloat>
+
+#include "rb_common.cuh"
+#include "rb_kernels.h"
+
+namespace rb {
+
+// hllc.py:158-165 _minmod
+__device__ __forceinline__ float minmod(float a, float b) {
+  if (a * b <= 0.0f) return 0.0f;
+  if (fabsf(a) < fabsf(b)) return a;
+  return b;
+}
+
+// hllc.py:174-188 _dryfactor
+__device__ __forceinline__ float dryfactor(float h0, float hm, float hp) {
+  return (h0 <= kHDry || hm <= kHDry || hp <= kHDry) ? 0.0f : 1.0f;
+}
+
+// hllc.py:191-256 _hllc: (mass, normal momentum, transverse momentum) flux.
+__device__ __forceinline__ void hllc_flux(float hl, float ul, float vtl, float hr, float ur, float vtr, float& f0,
+                                          float& f1, float& f2) {
+  const float g = kG;
+  const float cl = sqrtf(g * rmax(hl, 0.0f));
+  const float cr = sqrtf(g * rmax(hr, 0.0f));
+  const bool dry_l = hl <= kHDry, dry_r = hr <= kHDry;
+  if (dry_l && dry_r) {
+    f0 = 0.0f;
+    f1 = 0.0f;
+    f2 = 0.0f;
+    return;
+  }
+  float sl, sr;
+  if (dry_l) {
+    sl = ur - 2.0f * cr;
+    sr = ur + cr;
+  } else if (dry_r) {
+    sl = ul - cl;
+    sr = ul + 2.0f * cl;
+  } else {
+    const float hs = 0.5f * (cl + cr) + 0.25f * (ul - ur);
+    const float h_star = rmax(hs * hs / g, 0.0f);
+    const float c_star = sqrtf(g * h_star);
+    const float u_star = 0.5f * (ul + ur) + cl - cr;
+    sl = rmin(ul - cl, u_star - c_star);
+    sr = rmax(ur + cr, u_star + c_star);
+  }
+  const float fh_l = hl * ul;
+  const float fmn_l = hl * ul * ul + 0.5f * g * hl * hl;
+  const float fh_r = hr * ur;
+  const float fmn_r = hr * ur * ur + 0.5f * g * hr * hr;
+  float fh, fmn;
+  if (sl >= 0.0f) {
+    fh = fh_l;
+    fmn = fmn_l;
+  } else if (sr <= 0.0f) {
+    fh = fh_r;
+    fmn = fmn_r;
+  } else {
+    const float inv = 1.0f / (sr - sl);
+    fh = (sr * fh_l - sl * fh_r + sl * sr * (hr - hl)) * inv;
+    fmn = (sr * fmn_l - sl * fmn_r + sl * sr * (hr * ur - hl * ul)) * inv;
+  }
+  const float den_s = hr * (ur - sr) - hl * (ul - sl);
+  float s_star = 0.5f * (ul + ur);
+  if (fabsf(den_s) > 1.0e-12f) s_star = (sl * hr * (ur - sr) - sr * hl * (ul - sl)) / den_s;
+  const float vt = s_star >= 0.0f ? vtl : vtr;
+  f0 = fh;
+  f1 = fmn;
+  f2 = fh * vt;
+}
+
+// One face of the MUSCL + Audusse reconstruction (hllc.py:306-354 / :378-424):
+// four cells along the normal (m2, m1 | p0, p1), the face between m1 and p0.
+struct Cell {
+  float h, un, ut, z;  // depth, normal velocity, transverse velocity, bed
+};
+
+__device__ __forceinline__ void muscl_face(const Cell& c0, const Cell& c1, const Cell& c2, const Cell& c3, float& fh,
+                                           float& fmn_l, float& fmn_r, float& fmt) {
+  const float g = kG;
+  const float e0 = c0.h + c0.z, e1 = c1.h + c1.z, e2 = c2.h + c2.z, e3 = c3.h + c3.z;
+  const float wl = dryfactor(c1.h, c0.h, c2.h);
+  const float wr = dryfactor(c2.h, c1.h, c3.h);
+  const float eta_l = e1 + 0.5f * wl * minmod(e1 - e0, e2 - e1);
+  const float eta_r = e2 - 0.5f * wr * minmod(e2 - e1, e3 - e2);
+  const float zf_l = c1.z + 0.5f * wl * minmod(c1.z - c0.z, c2.z - c1.z);
+  const float zf_r = c2.z - 0.5f * wr * minmod(c2.z - c1.z, c3.z - c2.z);
+  const float un_l = c1.un + 0.5f * wl * minmod(c1.un - c0.un, c2.un - c1.un);
+  const float un_r = c2.un - 0.5f * wr * minmod(c2.un - c1.un, c3.un - c2.un);
+  const float ut_l = c1.ut + 0.5f * wl * minmod(c1.ut - c0.ut, c2.ut - c1.ut);
+  const float ut_r = c2.ut - 0.5f * wr * minmod(c2.ut - c1.ut, c3.ut - c2.ut);
+  const float h_l = rmax(eta_l - zf_l, 0.0f);
+  const float h_r = rmax(eta_r - zf_r, 0.0f);
+  const float z_star = rmax(zf_l, zf_r);
+  const float hl_star = rmax(eta_l - z_star, 0.0f);
+  const float hr_star = rmax(eta_r - z_star, 0.0f);
+  float f0, f1, f2;
+  hllc_flux(hl_star, un_l, ut_l, hr_star, un_r, ut_r, f0, f1, f2);
+  fh = f0;
+  fmn_l = f1 + 0.5f * g * (h_l * h_l - hl_star * hl_star);
+  fmn_r = f1 + 0.5f * g * (h_r * h_r - hr_star * hr_star);
+  fmt = f2;
+}
+
+template <int TX, int TY, int NT, int STAGE>
+__global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
+  constexpr int H = 3;                      // halo
+  constexpr int RW = TX + 2 * H, RH = TY + 2 * H;
+  constexpr int XW = TX + 3, XH = TY + 2;   // x-face mass flux: cols x0-1..x0+TX+1, rows y0-1..y0+TY
+  constexpr int YW = TX + 2, YH = TY + 3;   // y-face mass flux: cols x0-1..x0+TX,   rows y0-1..y0+TY+1
+  constexpr int BW = TX + 2, BH = TY + 2;   // beta on the tile + ring
+  __shared__ float s_h[RH][RW], s_u[RH][RW], s_v[RH][RW], s_z[RH][RW];
+  __shared__ float s_fxh[XH][XW], s_fyh[YH][YW];
+  __shared__ float s_fxl[TY][TX + 1], s_fxr[TY][TX + 1], s_fxt[TY][TX + 1];  // tile x-faces
+  __shared__ float s_fyl[TY + 1][TX], s_fyr[TY + 1][TX], s_fyt[TY + 1][TX];  // tile y-faces
+  __shared__ float s_beta[BH][BW];
+  __shared__ double s_red[NT / 32];
+  __shared__ float s_redf[NT / 32];
+
+  const int ny = p.ny, nx = p.nx;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const float dt = p.dt32, dx = p.dx32;
+
+  // 1. stage the clamped halo and the primitives (hllc.py:262-282).
+  for (int k = threadIdx.x; k < RH * RW; k += NT) {
+    const int r = k / RW, c = k - r * RW;
+    const int gi = min(max(y0 - H + r, 0), ny - 1), gj = min(max(x0 - H + c, 0), nx - 1);
+    const size_t id = (size_t)gi * nx + gj;
+    const float hh = p.h_s[id];
+    float u = 0.0f, v = 0.0f;
+    if (hh > kHDry) {
+      u = p.hu_s[id] / hh;
+      v = p.hv_s[id] / hh;
+    }
+    s_h[r][c] = hh;
+    s_u[r][c] = u;
+    s_v[r][c] = v;
+    s_z[r][c] = p.z[id];
+  }
+  __syncthreads();
+
+  // 2. x-face fluxes (hllc.py:285-354), boundary corrections (:993-1109).
+  for (int k = threadIdx.x; k < XH * XW; k += NT) {
+    const int a = k / XW, b = k - a * XW;
+    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+    if (gi < 0 || gi >= ny || gj < 0 || gj > nx) continue;
+    const int r = a + 2;  // cell row; stencil columns c = b .. b+3 (cells gj-2 .. gj+1)
+    float fh, fl, fr, ft;
+    const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
+    if (kind == RB_BC_OPEN) {
+      const Cell c0{s_h[r][b], s_u[r][b], s_v[r][b], s_z[r][b]};
+      const Cell c1{s_h[r][b + 1], s_u[r][b + 1], s_v[r][b + 1], s_z[r][b + 1]};
+      const Cell c2{s_h[r][b + 2], s_u[r][b + 2], s_v[r][b + 2], s_z[r][b + 2]};
+      const Cell c3{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
+      muscl_face(c0, c1, c2, c3, fh, fl, fr, ft);
+    } else {
+      // The edge cell is column 0 (west) or nx-1 (east): region column b+2 or b+1.
+      const int ce = gj == 0 ? b + 2 : b + 1;
+      const float h0 = s_h[r][ce], u0 = s_u[r][ce], v0 = s_v[r][ce];
+      fl = 0.0f;
+      fr = 0.0f;
+      float f1;
+      if (kind == RB_BC_CLOSED) {  // reflective wall, hllc.py:442-481
+        if (gj == 0)
+          hllc_flux(h0, -u0, v0, h0, u0, v0, fh, f1, ft);
+        else
+          hllc_flux(h0, u0, v0, h0, -u0, v0, fh, f1, ft);
+      } else {  // prescribed surface, hllc.py:537-581
+        const float stage = gj == 0 ? p.stage[RB_EDGE_WEST] : p.stage[RB_EDGE_EAST];
+        const float h_g = rmax(stage - s_z[r][ce], 0.0f);
+        if (gj == 0)
+          hllc_flux(h_g, u0, v0, h0, u0, v0, fh, f1, ft);
+        else
+          hllc_flux(h0, u0, v0, h_g, u0, v0, fh, f1, ft);
+      }
+      if (gj == 0)
+        fr = f1;  // only the inward slot is read (hllc.py:439-440)
+      else
+        fl = f1;
+    }
+    s_fxh[a][b] = fh;
+    if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
+      s_fxl[a - 1][b - 1] = fl;
+      s_fxr[a - 1][b - 1] = fr;
+      s_fxt[a - 1][b - 1] = ft;
+    }
+  }
+  // y-face fluxes (hllc.py:357-424): normal velocity v, transverse u.
+  for (int k = threadIdx.x; k < YH * YW; k += NT) {
+    const int a = k / YW, b = k - a * YW;
+    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+    if (gj < 0 || gj >= nx || gi < 0 || gi > ny) continue;
+    const int c = b + 2;  // cell column; stencil rows r = a .. a+3 (cells gi-2 .. gi+1)
+    float fh, fl, fr, ft;
+    const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
+    if (kind == RB_BC_OPEN) {
+      const Cell c0{s_h[a][c], s_v[a][c], s_u[a][c], s_z[a][c]};
+      const Cell c1{s_h[a + 1][c], s_v[a + 1][c], s_u[a + 1][c], s_z[a + 1][c]};
+      const Cell c2{s_h[a + 2][c], s_v[a + 2][c], s_u[a + 2][c], s_z[a + 2][c]};
+      const Cell c3{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
+      muscl_face(c0, c1, c2, c3, fh, fl, fr, ft);
+    } else {
+      const int re = gi == 0 ? a + 2 : a + 1;
+      const float h0 = s_h[re][c], u0 = s_u[re][c], v0 = s_v[re][c];
+      fl = 0.0f;
+      fr = 0.0f;
+      float f1;
+      if (kind == RB_BC_CLOSED) {  // hllc.py:483-521
+        if (gi == 0)
+          hllc_flux(h0, -v0, u0, h0, v0, u0, fh, f1, ft);
+        else
+          hllc_flux(h0, v0, u0, h0, -v0, u0, fh, f1, ft);
+      } else {  // hllc.py:584-628
+        const float stage = gi == 0 ? p.stage[RB_EDGE_NORTH] : p.stage[RB_EDGE_SOUTH];
+        const float h_g = rmax(stage - s_z[re][c], 0.0f);
+        if (gi == 0)
+          hllc_flux(h_g, v0, u0, h0, v0, u0, fh, f1, ft);
+        else
+          hllc_flux(h0, v0, u0, h_g, v0, u0, fh, f1, ft);
+      }
+      if (gi == 0)
+        fr = f1;
+      else
+        fl = f1;
+    }
+    s_fyh[a][b] = fh;
+    if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
+      s_fyl[a - 1][b - 1] = fl;
+      s_fyr[a - 1][b - 1] = fr;
+      s_fyt[a - 1][b - 1] = ft;
+    }
+  }
+  __syncthreads();
+
+  // 3. mass-only donor beta on the tile + ring (hllc.py:700-736).
+  const float dtdx = dt / dx;
+  for (int k = threadIdx.x; k < BH * BW; k += NT) {
+    const int a = k / BW, b = k - a * BW;
+    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+    float beta = 1.0f;
+    if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
+      float q_out = 0.0f;
+      const float fl = s_fxh[a][b];
+      if (fl < 0.0f) q_out = q_out - fl;
+      const float fr = s_fxh[a][b + 1];
+      if (fr > 0.0f) q_out = q_out + fr;
+      const float ft = s_fyh[a][b];
+      if (ft < 0.0f) q_out = q_out - ft;
+      const float fb = s_fyh[a + 1][b];
+      if (fb > 0.0f) q_out = q_out + fb;
+      const float out_depth = dtdx * q_out;
+      if (out_depth > 0.0f) beta = rclamp(s_h[a + 2][b + 2] / out_depth, 0.0f, 1.0f);
+    }
+    s_beta[a][b] = beta;
+  }
+  __syncthreads();
+
+  // 4. limit the tile's mass faces by their donor (hllc.py:739-773); bank the
+  //    limited boundary flux of open / fixed_stage edges (hllc.py:638-677).
+  double loss = 0.0;
+  for (int k = threadIdx.x; k < TY * (TX + 1); k += NT) {
+    const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
+    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+    if (gi >= ny || gj > nx) continue;
+    float q = s_fxh[a][b];
+    if (q > 0.0f) {
+      if (gj >= 1) q = q * s_beta[a][b - 1];
+    } else if (q < 0.0f) {
+      if (gj <= nx - 1) q = q * s_beta[a][b];
+    }
+    s_fxh[a][b] = q;
+    if (p.ledger != nullptr) {
+      if (gj == 0 && p.bc[RB_EDGE_WEST] != RB_BC_CLOSED) loss -= p.wt * (double)q;
+      if (gj == nx && (b <= TX || gj == nx) && p.bc[RB_EDGE_EAST] != RB_BC_CLOSED) loss += p.wt * (double)q;
+    }
+  }
+  for (int k = threadIdx.x; k < (TY + 1) * TX; k += NT) {
+    const int a = 1 + k / TX, b = 1 + (k - (a - 1) * TX);
+    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+    if (gj >= nx || gi > ny) continue;
+    float q = s_fyh[a][b];
+    if (q > 0.0f) {
+      if (gi >= 1) q = q * s_beta[a - 1][b];
+    } else if (q < 0.0f) {
+      if (gi <= ny - 1) q = q * s_beta[a][b];
+    }
+    s_fyh[a][b] = q;
+    if (p.ledger != nullptr) {
+      if (gi == 0 && p.bc[RB_EDGE_NORTH] != RB_BC_CLOSED) loss -= p.wt * (double)q;
+      if (gi == ny && p.bc[RB_EDGE_SOUTH] != RB_BC_CLOSED) loss += p.wt * (double)q;
+    }
+  }
+  __syncthreads();
+
+  // 5. divergence + centred bed source (hllc.py:776-847) and the Heun update.
+  const float inv_dx = 1.0f / dx;
+  const float g = kG;
+  float smax = 0.0f;
+  bool bad = false;
+  for (int k = threadIdx.x; k < TY * TX; k += NT) {
+    const int r = k / TX, c = k - r * TX;
+    const int gi = y0 + r, gj = x0 + c;
+    if (gi >= ny || gj >= nx) continue;
+    const size_t id = (size_t)gi * nx + gj;
+    const int R = r + H, Cc = c + H;  // this cell in the staged region
+    const float dh = -((s_fxh[r + 1][c + 2] - s_fxh[r + 1][c + 1]) + (s_fyh[r + 2][c + 1] - s_fyh[r + 1][c + 1])) *
+                     inv_dx;
+    const float hg = s_h[R][Cc];
+    const float wx = dryfactor(hg, s_h[R][Cc - 1], s_h[R][Cc + 1]);
+    const float wy = dryfactor(hg, s_h[R - 1][Cc], s_h[R + 1][Cc]);
+    const float zc = s_z[R][Cc];
+    const float ec = hg + zc;
+    const float sz_x = wx * minmod(zc - s_z[R][Cc - 1], s_z[R][Cc + 1] - zc);
+    const float se_x =
+        wx * minmod(ec - (s_h[R][Cc - 1] + s_z[R][Cc - 1]), (s_h[R][Cc + 1] + s_z[R][Cc + 1]) - ec);
+    const float hp_x = rmax((ec + 0.5f * se_x) - (zc + 0.5f * sz_x), 0.0f);
+    const float hm_x = rmax((ec - 0.5f * se_x) - (zc - 0.5f * sz_x), 0.0f);
+    const float src_x = -g * 0.5f * (hp_x + hm_x) * sz_x;
+    const float dhu = (-((s_fxl[r][c + 1] - s_fxr[r][c]) + (s_fyt[r + 1][c] - s_fyt[r][c])) + src_x) * inv_dx;
+    const float sz_y = wy * minmod(zc - s_z[R - 1][Cc], s_z[R + 1][Cc] - zc);
+    const float se_y =
+        wy * minmod(ec - (s_h[R - 1][Cc] + s_z[R - 1][Cc]), (s_h[R + 1][Cc] + s_z[R + 1][Cc]) - ec);
+    const float hp_y = rmax((ec + 0.5f * se_y) - (zc + 0.5f * sz_y), 0.0f);
+    const float hm_y = rmax((ec - 0.5f * se_y) - (zc - 0.5f * sz_y), 0.0f);
+    const float src_y = -g * 0.5f * (hp_y + hm_y) * sz_y;
+    const float dhv = (-((s_fyl[r + 1][c] - s_fyr[r][c]) + (s_fxt[r][c + 1] - s_fxt[r][c])) + src_y) * inv_dx;
+
+    if (STAGE == 1) {  // hllc.py:850-878
+      const float hh = rmax(hg + dt * dh, 0.0f);
+      float hu1 = 0.0f, hv1 = 0.0f;
+      if (hh > kHDry) {
+        hu1 = p.hu_s[id] + dt * dhu;
+        hv1 = p.hv_s[id] + dt * dhv;
+      }
+      p.h1[id] = hh;
+      p.hu1[id] = hu1;
+      p.hv1[id] = hv1;
+    } else {  // hllc.py:881-909, then friction :912-939, then sources :1350-1373
+      float hh = rmax(0.5f * (p.h_n[id] + hg + dt * dh), 0.0f);
+      float hu = 0.0f, hv = 0.0f;
+      if (hh > kHDry) {
+        hu = 0.5f * (p.hu_n[id] + p.hu_s[id] + dt * dhu);
+        hv = 0.5f * (p.hv_n[id] + p.hv_s[id] + dt * dhv);
+        const float mom = sqrtf(hu * hu + hv * hv);
+        const float denom = manning_denominator(mom, hh, p.n[id], g, dt);
+        hu = hu / denom;
+        hv = hv / denom;
+      }
+      if (p.rain_mode == 1) {
+        float comp = p.h_comp[id];
+        kahan_add(hh, comp, p.rain32 * dt);
+        p.h_comp[id] = comp;
+      } else if (p.rain_mode == 2) {
+        hh = hh + p.rain32 * dt;  // hllc.py:942-945
+      }
+      if (p.rain_field != nullptr) {
+        if (p.h_comp != nullptr) {
+          float comp = p.h_comp[id];
+          kahan_add(hh, comp, p.rain_field[id] * p.scale32 * dt);
+          p.h_comp[id] = comp;
+        } else {
+          hh = hh + p.rain_field[id] * p.scale32 * dt;
+        }
+      }
+      if (p.infil != nullptr) {  // local_inertial.py:170-194
+        const float avail = hh;
+        float inf = p.infil[id] * dt;
+        if (inf > avail) inf = avail;
+        if (inf < 0.0f) inf = 0.0f;
+        hh = avail - inf;
+        loss += (double)avail - (double)hh;
+      }
+      p.h_out[id] = hh;
+      p.hu_out[id] = hu;
+      p.hv_out[id] = hv;
+      // hllc.py:948-966 _reduce_wavespeed on the new state
+      const float cw = sqrtf(g * rmax(hh, 0.0f));
+      float s = cw;
+      if (hh > kHDry) s = rmax(fabsf(hu) / hh, fabsf(hv) / hh) + cw;
+      smax = s > smax ? s : smax;
+      bad |= !(fabsf(hh) <= FLT_MAX);
+    }
+  }
+
+  if (p.ledger != nullptr) {
+    const double s = block_sum<NT>(loss, s_red);
+    if (threadIdx.x == 0) ledger_add(p.ledger + 2 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x), s);
+  }
+  if (STAGE == 2) {
+    if (p.smax_key != nullptr) block_max_to<NT>(smax, p.smax_key, s_redf);
+    if (bad) flag_error(p.err, RB_DEVERR_NONFINITE);
+  }
+}
+
+template <int TX, int TY, int NT>
+static cudaError_t launch_hllc(const HllcParams& p, int stage, cudaStream_t s) {
+  const dim3 grid((p.nx + TX - 1) / TX, (p.ny + TY - 1) / TY);
+  if (stage == 1)
+    hllc_stage_kernel<TX, TY, NT, 1><<<grid, NT, 0, s>>>(p);
+  else
+    hllc_stage_kernel<TX, TY, NT, 2><<<grid, NT, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s) {
+  return launch_hllc<HLLC_TX, HLLC_TY, HLLC_NT>(p, stage, s);
+}
+
+int hllc_tiles(int ny, int nx) { return ((nx + HLLC_TX - 1) / HLLC_TX) * ((ny + HLLC_TY - 1) / HLLC_TY); }
+
+}  // namespace rb

@@ -1,0 +1,295 @@
+// li_step.cu -- the fused local-inertial step (Bates et al. 2010).
+//
+// One launch performs what the reference launches as ~12 kernels per step
+// (solver/core/local_inertial.py:547-727):
+//   compute_eta (:61) -> update_qx/update_qy (:72/:102, friction.py:18) ->
+//   apply_closed_bc (boundaries.py:237) -> compute_outflow_beta (:197) ->
+//   limit_qx/limit_qy (:242/:254) -> accumulate_qs_x/y (sediment.py:218/:247) ->
+//   update_h (:132) -> add_uniform_rain_c / add_rain_field_c (sources.py:85/:104)
+//   or apply_rain_field (:154) -> apply_infiltration (:170) ->
+//   apply_open_outflow (boundaries.py:321).
+//
+// Tiling. A CTA owns a TX x TY tile of cells. The donor limiter makes a cell's new
+// depth depend on the limited fluxes of its four faces, which depend on the beta of
+// the neighbouring cells, which depend on *their* four unlimited faces: a halo of 2
+// cells of (h, z, n) is staged in shared memory, the unlimited faces of the tile
+// and a 1-cell ring are computed there (redundantly with the neighbouring CTAs),
+// then beta on the tile plus ring, then the limited faces of the tile, then the
+// cell updates. Each output is written by exactly one CTA. Because neighbours read
+// the old h, qx, qy while this CTA writes new ones, the step reads buffer [cur]
+// and writes buffer [cur ^ 1].
+//
+// Per-cell HBM traffic (compulsory): read h, z, n, qx, qy, write h, qx, qy (32 B),
+// + h_comp read/write (8 B) when compensated rain is armed, + rain field / infil
+// reads (4 B each), + d50 and the four transport accumulators (36 B) when
+// morphology is armed. Infiltration and open-edge losses go to one float64 ledger
+// slot per tile instead of a per-cell float64 field.
+#include <cfloat>
+
+#include "rb_common.cuh"
+#include "rb_kernels.h"
+
+namespace rb {
+
+// sediment.py:161-207 kinematic_shear / shields_number / mpm_capacity / face_capacity.
+__device__ __forceinline__ float face_capacity(float q, float h, float radius, float n, float d50) {
+  if (h < kHDry || d50 <= 0.0f || q == 0.0f) return 0.0f;
+  const float tau = kG * n * n * q * q / (h * h * rb_pow13f(radius));
+  const float theta = tau / (1.65f * kG * d50);
+  float qs;
+  if (theta <= 0.047f) {
+    qs = 0.0f;
+  } else {
+    const float excess = theta - 0.047f;
+    qs = 8.0f * rb_pow15f(excess) * sqrtf(1.65f * kG * d50 * d50 * d50);
+  }
+  return q < 0.0f ? -qs : qs;
+}
+
+// boundaries.py:244-256 _drain
+__device__ __forceinline__ float drain(float h_edge, float q_out, float dxdt) {
+  float removed = dxdt * q_out;
+  if (removed > h_edge) removed = h_edge;
+  if (removed < 0.0f) removed = 0.0f;
+  return h_edge - removed;
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
+  constexpr int RW = TX + 4, RH = TY + 4;  // cells: cols x0-2 .. x0+TX+1, rows y0-2 .. y0+TY+1
+  constexpr int XW = TX + 3, XH = TY + 2;  // x-faces: cols x0-1 .. x0+TX+1, rows y0-1 .. y0+TY
+  constexpr int YW = TX + 2, YH = TY + 3;  // y-faces: cols x0-1 .. x0+TX,   rows y0-1 .. y0+TY+1
+  constexpr int BW = TX + 2, BH = TY + 2;  // beta:    cols x0-1 .. x0+TX,   rows y0-1 .. y0+TY
+  __shared__ float s_h[RH][RW], s_z[RH][RW], s_n[RH][RW], s_eta[RH][RW];
+  __shared__ float s_qx[XH][XW], s_qy[YH][YW], s_beta[BH][BW];
+  __shared__ double s_red[NT / 32];
+  __shared__ float s_redf[NT / 32];
+
+  const int ny = p.ny, nx = p.nx;
+  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const float dt = p.dt32, dx = p.dx32;
+  const float dtdx = dt / dx;
+
+  // 1. stage h, z, n (halo 2) and eta = h + z (local_inertial.py:61-69).
+  for (int k = threadIdx.x; k < RH * RW; k += NT) {
+    const int r = k / RW, c = k - r * RW;
+    const int gi = y0 - 2 + r, gj = x0 - 2 + c;
+    float h = 0.0f, z = 0.0f, n = 0.0f;
+    if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
+      const size_t id = (size_t)gi * nx + gj;
+      h = p.h[id];
+      z = p.z[id];
+      n = p.n[id];
+    }
+    s_h[r][c] = h;
+    s_z[r][c] = z;
+    s_n[r][c] = n;
+    s_eta[r][c] = h + z;
+  }
+  __syncthreads();
+
+  // 2. unlimited face updates (local_inertial.py:72-129); boundary faces stay 0,
+  //    which is the closed boundary (boundaries.py:223-241).
+  for (int k = threadIdx.x; k < XH * XW; k += NT) {
+    const int a = k / XW, b = k - a * XW;
+    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+    float q = 0.0f;
+    if (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1) {
+      const float eta_l = s_eta[a + 1][b], eta_r = s_eta[a + 1][b + 1];
+      const float h_flow = rmax(eta_l, eta_r) - rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
+      if (!(h_flow < kHDry)) {
+        const float qo = p.qx[(size_t)gi * (nx + 1) + gj];
+        const float n_face = 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]);
+        const float slope = (eta_r - eta_l) / dx;
+        const float num = qo - kG * h_flow * dt * slope;
+        const float den = manning_denominator(qo, h_flow, n_face, kG, dt);
+        q = num / den;
+      }
+    }
+    s_qx[a][b] = q;
+  }
+  for (int k = threadIdx.x; k < YH * YW; k += NT) {
+    const int a = k / YW, b = k - a * YW;
+    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+    float q = 0.0f;
+    if (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx) {
+      const float eta_t = s_eta[a][b + 1], eta_b = s_eta[a + 1][b + 1];
+      const float h_flow = rmax(eta_t, eta_b) - rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
+      if (!(h_flow < kHDry)) {
+        const float qo = p.qy[(size_t)gi * nx + gj];
+        const float n_face = 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]);
+        const float slope = (eta_b - eta_t) / dx;
+        const float num = qo - kG * h_flow * dt * slope;
+        const float den = manning_denominator(qo, h_flow, n_face, kG, dt);
+        q = num / den;
+      }
+    }
+    s_qy[a][b] = q;
+  }
+  __syncthreads();
+
+  // 3. donor-cell beta on the tile plus a 1-cell ring (local_inertial.py:197-239).
+  if (p.limit) {
+    for (int k = threadIdx.x; k < BH * BW; k += NT) {
+      const int a = k / BW, b = k - a * BW;
+      float q_out = 0.0f;
+      const float ql = s_qx[a][b];
+      if (ql < 0.0f) q_out = q_out - ql;
+      const float qr = s_qx[a][b + 1];
+      if (qr > 0.0f) q_out = q_out + qr;
+      const float qt = s_qy[a][b];
+      if (qt < 0.0f) q_out = q_out - qt;
+      const float qb = s_qy[a + 1][b];
+      if (qb > 0.0f) q_out = q_out + qb;
+      const float out_depth = dtdx * q_out;
+      s_beta[a][b] = out_depth > 0.0f ? rclamp(s_h[a + 1][b + 1] / out_depth, 0.0f, 1.0f) : 1.0f;
+    }
+    __syncthreads();
+
+    // 4. scale each interior face of the tile by its donor's beta (:242-263).
+    for (int k = threadIdx.x; k < TY * (TX + 1); k += NT) {
+      const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
+      const int gj = x0 - 1 + b;
+      if (gj >= 1 && gj <= nx - 1) {
+        const float q = s_qx[a][b];
+        if (q > 0.0f)
+          s_qx[a][b] = q * s_beta[a][b - 1];
+        else if (q < 0.0f)
+          s_qx[a][b] = q * s_beta[a][b];
+      }
+    }
+    for (int k = threadIdx.x; k < (TY + 1) * TX; k += NT) {
+      const int a = 1 + k / TX, b = 1 + (k - (a - 1) * TX);
+      const int gi = y0 - 1 + a;
+      if (gi >= 1 && gi <= ny - 1) {
+        const float q = s_qy[a][b];
+        if (q > 0.0f)
+          s_qy[a][b] = q * s_beta[a - 1][b];
+        else if (q < 0.0f)
+          s_qy[a][b] = q * s_beta[a][b];
+      }
+    }
+    __syncthreads();
+  }
+
+  // 5. write the tile's faces; integrate bedload on them (sediment.py:218-273).
+  for (int k = threadIdx.x; k < TY * (TX + 1); k += NT) {
+    const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
+    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+    if (gi >= ny || gj > nx || (b == TX + 1 && gj != nx)) continue;
+    const size_t fid = (size_t)gi * (nx + 1) + gj;
+    const float q = s_qx[a][b];
+    p.qx_out[fid] = q;
+    if (p.d50 != nullptr && gj >= 1 && gj <= nx - 1) {
+      const float eta_max = rmax(s_eta[a + 1][b], s_eta[a + 1][b + 1]);
+      const float z_bank = rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
+      const float h_face = eta_max - z_bank;
+      const size_t cl = (size_t)gi * nx + gj - 1;
+      const float qs = face_capacity(q, h_face, h_face, 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]),
+                                     0.5f * (p.d50[cl] + p.d50[cl + 1]));
+      float tot = p.qs_int_x[fid], comp = p.qs_comp_x[fid];
+      kahan_add(tot, comp, qs * dt);
+      p.qs_int_x[fid] = tot;
+      p.qs_comp_x[fid] = comp;
+    }
+  }
+  for (int k = threadIdx.x; k < (TY + 1) * TX; k += NT) {
+    const int a = 1 + k / TX, b = 1 + (k - (a - 1) * TX);
+    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+    if (gj >= nx || gi > ny || (a == TY + 1 && gi != ny)) continue;
+    const size_t fid = (size_t)gi * nx + gj;
+    const float q = s_qy[a][b];
+    p.qy_out[fid] = q;
+    if (p.d50 != nullptr && gi >= 1 && gi <= ny - 1) {
+      const float eta_max = rmax(s_eta[a][b + 1], s_eta[a + 1][b + 1]);
+      const float z_bank = rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
+      const float h_face = eta_max - z_bank;
+      const float qs = face_capacity(q, h_face, h_face, 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]),
+                                     0.5f * (p.d50[fid - nx] + p.d50[fid]));
+      float tot = p.qs_int_y[fid], comp = p.qs_comp_y[fid];
+      kahan_add(tot, comp, qs * dt);
+      p.qs_int_y[fid] = tot;
+      p.qs_comp_y[fid] = comp;
+    }
+  }
+
+  // 6. continuity, areal sources, infiltration, open-edge sinks, per tile cell.
+  const float rain_dt = p.rain_cont * dt;
+  double loss = 0.0;
+  float hmax = 0.0f;
+  bool bad = false;
+  for (int k = threadIdx.x; k < TY * TX; k += NT) {
+    const int r = k / TX, c = k - r * TX;
+    const int gi = y0 + r, gj = x0 + c;
+    if (gi >= ny || gj >= nx) continue;
+    const size_t id = (size_t)gi * nx + gj;
+    const float qxl = s_qx[r + 1][c + 1], qxr = s_qx[r + 1][c + 2];
+    const float qyt = s_qy[r + 1][c + 1], qyb = s_qy[r + 2][c + 1];
+    const float net = qxl - qxr + qyt - qyb;
+    float h = s_h[r + 2][c + 2] + dtdx * net + rain_dt;  // local_inertial.py:150-151
+    if (p.h_comp != nullptr) {
+      float comp = p.h_comp[id];
+      if (p.rain_field == nullptr)
+        kahan_add(h, comp, p.rain32 * dt);  // sources.py:85-101
+      else
+        kahan_add(h, comp, p.rain_field[id] * p.scale32 * dt);  // sources.py:104-121
+      p.h_comp[id] = comp;
+    } else if (p.rain_field != nullptr) {
+      h = h + p.rain_field[id] * p.scale32 * dt;  // local_inertial.py:154-167
+    }
+    if (p.infil != nullptr) {  // local_inertial.py:170-194
+      const float avail = h;
+      float inf = p.infil[id] * dt;
+      if (inf > avail) inf = avail;
+      if (inf < 0.0f) inf = 0.0f;
+      h = avail - inf;
+      loss += (double)avail - (double)h;
+    }
+    // boundaries.py:259-318, launched west, east, north, south.
+    if (p.bc[RB_EDGE_WEST] == RB_BC_OPEN && nx > 1 && gj == 0) {
+      const float avail = h;
+      h = drain(avail, rmax(-qxr, 0.0f), p.dxdt);
+      loss += (double)avail - (double)h;
+    }
+    if (p.bc[RB_EDGE_EAST] == RB_BC_OPEN && nx > 1 && gj == nx - 1) {
+      const float avail = h;
+      h = drain(avail, rmax(qxl, 0.0f), p.dxdt);
+      loss += (double)avail - (double)h;
+    }
+    if (p.bc[RB_EDGE_NORTH] == RB_BC_OPEN && ny > 1 && gi == 0) {
+      const float avail = h;
+      h = drain(avail, rmax(-qyb, 0.0f), p.dxdt);
+      loss += (double)avail - (double)h;
+    }
+    if (p.bc[RB_EDGE_SOUTH] == RB_BC_OPEN && ny > 1 && gi == ny - 1) {
+      const float avail = h;
+      h = drain(avail, rmax(qyt, 0.0f), p.dxdt);
+      loss += (double)avail - (double)h;
+    }
+    p.h_out[id] = h;
+    hmax = h > hmax ? h : hmax;
+    bad |= !(fabsf(h) <= FLT_MAX);
+  }
+
+  if (p.ledger != nullptr) {
+    const double s = block_sum<NT>(loss, s_red);
+    if (threadIdx.x == 0) ledger_add(p.ledger + 2 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x), s);
+  }
+  if (p.hmax_key != nullptr) block_max_to<NT>(hmax, p.hmax_key, s_redf);
+  if (bad) flag_error(p.err, RB_DEVERR_NONFINITE);
+}
+
+template <int TX, int TY, int NT>
+static cudaError_t launch_li(const LiParams& p, cudaStream_t s) {
+  const dim3 grid((p.nx + TX - 1) / TX, (p.ny + TY - 1) / TY);
+  li_step_kernel<TX, TY, NT><<<grid, NT, 0, s>>>(p);
+  return cudaGetLastError();
+}
+
+cudaError_t li_step_launch(const LiParams& p, cudaStream_t s) {
+  return launch_li<LI_TX, LI_TY, LI_NT>(p, s);
+}
+
+int li_tiles(int ny, int nx) { return ((nx + LI_TX - 1) / LI_TX) * ((ny + LI_TY - 1) / LI_TY); }
+
+}  // namespace rb

@@ -1,0 +1,99 @@
+"""The C ABI library loads without a GPU and exports every entry point of include/rbsim.h."""
+
+from __future__ import annotations
+
+import ctypes
+import os
+import re
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADERS = [os.path.join(ROOT, "include", "rbsim.h")]
+
+
+def declared_functions(path):
+    text = open(path).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(rb_[a-z0-9_]+)\s*\(", text, flags=re.M)))
+
+
+def _lib():
+    import build  # river-basin-sim_b200/build.py
+
+    build.build()
+    from rbsim import _lib
+
+    return _lib.lib()
+
+
+def test_every_declared_entry_point_is_exported():
+    L = _lib()
+    names = [n for h in HEADERS for n in declared_functions(h)]
+    assert len(names) >= 15, names
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, f"declared in include/ but not exported: {missing}"
+
+
+def test_binding_table_covers_the_header():
+    from rbsim import _lib
+
+    names = [n for h in HEADERS for n in declared_functions(h)]
+    assert sorted(_lib.SIGNATURES) == sorted(names)
+
+
+def test_struct_layouts_match_the_c_compiler(tmp_path):
+    """The ctypes mirrors have exactly the layout gcc gives the header's structs."""
+    import subprocess
+
+    from rbsim import _lib
+
+    structs = {"rb_li_fields": _lib.LiFields, "rb_hllc_fields": _lib.HllcFields, "rb_step_args": _lib.StepArgs}
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "rbsim.h"', "int main(void) {"]
+    for cname, cls in structs.items():
+        lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')
+        for fname, _ in cls._fields_:
+            lines.append(f'  printf("{cname}.{fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines.append("  return 0;\n}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True,
+                                                       check=True).stdout.splitlines())
+    for cname, cls in structs.items():
+        assert int(got[cname]) == ctypes.sizeof(cls), cname
+        for fname, _ in cls._fields_:
+            assert int(got[f"{cname}.{fname}"]) == getattr(cls, fname).offset, f"{cname}.{fname}"
+
+
+def test_host_only_calls_work_without_a_device():
+    L = _lib()
+    assert L.rb_li_workspace_bytes(2048, 2048) > 0
+    assert L.rb_hllc_workspace_bytes(2048, 2048) > 3 * 2048 * 2048 * 4
+    assert L.rb_li_workspace_bytes(0, 5) == 0
+    major, minor, arch = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+    assert L.rb_version(ctypes.byref(major), ctypes.byref(minor), ctypes.byref(arch)) == 0
+    assert arch.value == 100
+
+
+def test_argument_errors_are_reported_without_touching_the_device():
+    from rbsim import _lib
+
+    L = _lib.lib()
+    f = _lib.LiFields()
+    f.ny, f.nx, f.dx = 0, 4, 1.0
+    a = _lib.StepArgs(1.0, 0.0, 1.0, 1, 0)
+    rc = L.rb_li_step(ctypes.byref(f), 0, ctypes.byref(a), ctypes.c_void_p(1), None)
+    assert rc == _lib.RB_ERR_ARG
+    assert "grid 0 x 4" in _lib.last_error()
+    f.ny = 4
+    a.dt = -1.0
+    f.bc[:] = [0, 0, 0, 0]
+    rc = L.rb_li_step(ctypes.byref(f), 0, ctypes.byref(a), ctypes.c_void_p(1), None)
+    assert rc == _lib.RB_ERR_STEP
+    try:
+        _lib.check(rc)
+    except RuntimeError as e:
+        assert "non-positive timestep" in str(e)
+    f.bc[:] = [2, 0, 0, 0]
+    a.dt = 1.0
+    assert L.rb_li_step(ctypes.byref(f), 0, ctypes.byref(a), ctypes.c_void_p(1), None) == _lib.RB_ERR_ARG

@@ -1,0 +1,164 @@
+"""CUDA path vs the CPU oracle: bit-for-bit on seeded inputs.
+
+The kernels and the oracle share one arithmetic contract (one IEEE rounding per
+operation in the reference's expression order, no fused multiply-add, the
+deterministic powers of include/rb_detmath.h), so with the oracle in
+``pow_mode=1`` every state field must match exactly -- depth, discharge,
+momenta, Kahan residues, transport integrals, float64 bed change -- after many
+steps. The only quantity compared with a tolerance is the float64 loss ledger,
+whose per-tile partial sums are added in a different order from the oracle's
+per-cell field (relative 1e-12).
+
+The oracle itself is pinned bit-for-bit to the reference's own kernels
+(tests/test_oracle_golden.py), and within 1e-5 relative in this power mode.
+"""
+
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+import oracle  # noqa: E402
+from cases import CASES, run_case  # noqa: E402
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _cuda():
+    if not torch.cuda.is_available():
+        pytest.fail("the gpu tests need a CUDA device")
+    from rbsim import _lib
+
+    _lib.lib()
+    oracle.set_pow_mode(1)
+    yield
+    oracle.set_pow_mode(0)
+
+
+def _oracle_outputs(case):
+    from test_oracle_golden import OracleAPI
+
+    out = run_case(case, OracleAPI())
+    if "loss_cum" in out:
+        out["loss_total"] = np.float64(out.pop("loss_cum").sum())
+    return out
+
+
+def _compare(got, want, name):
+    assert sorted(got) == sorted(want), (sorted(got), sorted(want))
+    for key in want:
+        if key == "loss_total":
+            np.testing.assert_allclose(got[key], want[key], rtol=1e-12, atol=1e-300, err_msg=f"{name}:{key}")
+        else:
+            np.testing.assert_array_equal(got[key], want[key], err_msg=f"{name}:{key}")
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_golden_cases_match_oracle_bitwise(name):
+    from gpu_api import GpuAPI
+
+    case = CASES[name]()
+    _compare(run_case(case, GpuAPI()), _oracle_outputs(case), name)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_golden_cases_track_reference_fixtures(name):
+    """The CUDA path against the reference-kernel fixtures, at the solver tolerance."""
+    from gpu_api import GpuAPI
+
+    want = dict(np.load(os.path.join(GOLDEN, f"{name}.npz")))
+    got = run_case(CASES[name](), GpuAPI())
+    for key, ref in want.items():
+        if key in ("h_comp", "qs_comp_x", "qs_comp_y"):
+            continue
+        if key == "loss_cum":
+            np.testing.assert_allclose(got["loss_total"], ref.sum(), rtol=1e-5, atol=1e-9)
+            continue
+        np.testing.assert_allclose(got[key], ref, rtol=1e-5, atol=1e-6, err_msg=f"{name}:{key}")
+
+
+def _synthetic_li(ny, nx, seed):
+    rng = np.random.default_rng(seed)
+    dx = 10.0
+    yy, xx = np.mgrid[0:ny, 0:nx].astype(np.float64)
+    z = 1e-3 * xx * dx
+    for _ in range(12):
+        a, s = rng.uniform(0.5, 5.0), rng.uniform(50.0, 300.0)
+        cy, cx = rng.uniform(0, ny), rng.uniform(0, nx)
+        z += a * np.exp(-(((yy - cy) ** 2 + (xx - cx) ** 2) * dx * dx) / (2 * s * s))
+    return dict(
+        scheme="local_inertial", bed=z.astype(np.float32), dx=dx, depth=rng.uniform(0.0, 0.3, (ny, nx)).astype(
+            np.float32), manning=0.03, compensated=True, rain=50.0 / 1000.0 / 3600.0,
+        infil=rng.uniform(0, 1e-5, (ny, nx)).astype(np.float32),
+        boundaries={"north": "open", "south": "open", "east": "open", "west": "open"},
+        steps=40, alpha=0.7, dt_max=30.0,
+    )  # fmt: skip
+
+
+def _synthetic_hllc(ny, nx, seed):
+    rng = np.random.default_rng(seed)
+    dx = 1.0
+    yy, xx = np.mgrid[0:ny, 0:nx].astype(np.float64)
+    z = np.zeros((ny, nx))
+    for _ in range(10):
+        a, s = rng.uniform(0.5, 3.5), rng.uniform(10.0, 80.0)
+        cy, cx = rng.uniform(0, ny), rng.uniform(0, nx)
+        z += a * np.exp(-(((yy - cy) ** 2 + (xx - cx) ** 2)) / (2 * s * s))
+    depth = np.where(xx < nx / 2, 10.0, 1.0) - 0.5 * z
+    return dict(scheme="hllc_fv", bed=z.astype(np.float32), dx=dx, depth=np.maximum(depth, 0).astype(np.float32),
+                manning=0.02, steps=25, alpha=0.45, dt_max=30.0)  # fmt: skip
+
+
+@pytest.mark.parametrize("shape", [(256, 256), (333, 517), (1, 700), (700, 1), (37, 3)])
+def test_li_seeded_grids_match_oracle_bitwise(shape):
+    """Ragged sizes (not multiples of the tile), one-row / one-column domains."""
+    from gpu_api import GpuAPI
+
+    case = _synthetic_li(*shape, seed=11)
+    _compare(run_case(case, GpuAPI()), _oracle_outputs(case), f"li{shape}")
+
+
+@pytest.mark.parametrize("shape", [(256, 256), (301, 419), (1, 600), (5, 2)])
+def test_hllc_seeded_grids_match_oracle_bitwise(shape):
+    from gpu_api import GpuAPI
+
+    case = _synthetic_hllc(*shape, seed=12)
+    _compare(run_case(case, GpuAPI()), _oracle_outputs(case), f"hllc{shape}")
+
+
+def test_li_config_scale_512_matches_oracle_bitwise():
+    """The 512 x 512 rain-on-grid configuration shape, 60 steps."""
+    from gpu_api import GpuAPI
+
+    case = _synthetic_li(512, 512, seed=1)
+    case["steps"] = 60
+    _compare(run_case(case, GpuAPI()), _oracle_outputs(case), "li512")
+
+
+def test_hllc_dambreak_2048_matches_oracle_bitwise():
+    """The 2048 x 2048 dam-break configuration (flat bed, h 10 | 1 m), 12 steps."""
+    from gpu_api import GpuAPI
+
+    n = 2048
+    depth = np.ones((n, n), np.float32)
+    depth[:, : n // 2] = 10.0
+    case = dict(scheme="hllc_fv", bed=np.zeros((n, n), np.float32), dx=1.0, depth=depth, manning=0.0,
+                steps=12, alpha=0.45, dt_max=30.0)  # fmt: skip
+    _compare(run_case(case, GpuAPI()), _oracle_outputs(case), "hllc2048")
+
+
+@pytest.mark.parametrize("name", ["hllc_bumpy_moving", "li_rain_open_infil", "li_sediment"])
+def test_reruns_are_bitwise_identical(name):
+    from gpu_api import GpuAPI
+
+    a = run_case(CASES[name](), GpuAPI())
+    b = run_case(CASES[name](), GpuAPI())
+    for key in a:
+        np.testing.assert_array_equal(a[key], b[key], err_msg=key)
