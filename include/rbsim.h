@@ -152,6 +152,56 @@ int rb_sum_f64(const float *x, int64_t n, void *ws, size_t ws_bytes, void *strea
 /* Read and clear the workspace device error word. Synchronising. */
 int rb_read_device_error(void *ws, void *stream, uint32_t *err_out);
 
+/* --- device-resident clock ----------------------------------------------------
+ * The run loop of solver/run.py:369-388 with the scheduler of
+ * solver/scheduler.py:171-246, moved onto the device: a one-thread plan kernel
+ * turns the max the previous step folded into the clock into compute_dt's dt,
+ * clamps it with fill_span to the next sync time, gates the rain and banks its
+ * volume, all in float64 in the reference's operation order, so K steps run
+ * without host round trips and can be captured in a CUDA graph. The clock lives
+ * in the workspace. Fixed_stage edges and point sources stay on the host loop. */
+typedef struct rb_clock_config {
+  double alpha, dt_max;      /* compute_dt arguments */
+  double t0;                 /* simulated time of the current state */
+  const double *sync;        /* device array, ascending: output times, forcing
+                                breakpoints, slow-process activations, end time
+                                (scheduler.py:136-147); must outlive the clock */
+  int32_t nsync;
+  int32_t rain_is_field;     /* 0: uniform rain_rate; 1: the state's rain field */
+  double rain_rate;          /* m/s while t < rain_until - 1e-6 (run.py:378) */
+  double rain_until;         /* rain duration, s */
+  double rain_field_sum;     /* float64 sum of the rain field, m/s (run.py:276) */
+  int32_t limit;             /* LI donor limiter */
+  int32_t reserved;
+} rb_clock_config;
+
+typedef struct rb_clock_state {
+  double t;            /* simulated time of the committed state */
+  double dt;           /* the last planned step */
+  double rain_volume;  /* areal rain banked since start, m^3 (ledger add_rain_step) */
+  int32_t cur;         /* the buffer holding the state */
+  int32_t steps;       /* steps taken since start */
+  uint32_t err;        /* RB_DEVERR_* bits raised by the clock or the steps */
+  int32_t reserved;
+} rb_clock_state;
+
+/* Arm the clock for the state in buffer [cur] (seeds compute_dt's reduction).
+ * Not capturable: copies the configuration from host memory. */
+int rb_li_clock_start(const rb_li_fields *f, int32_t cur, const rb_clock_config *cfg, void *ws, void *stream);
+int rb_hllc_clock_start(const rb_hllc_fields *f, int32_t cur, const rb_clock_config *cfg, void *ws, void *stream);
+/* Let the clock run until t_target (a sync time) or max_steps more steps. Capturable. */
+int rb_clock_set_target(void *ws, double t_target, int32_t max_steps, void *stream);
+/* One plan (commit the previous step, plan the next). Capturable. */
+int rb_clock_plan(void *ws, void *stream);
+/* One clocked launch: a no-op when the plan stopped the clock. Capturable. */
+int rb_li_step_clocked(const rb_li_fields *f, void *ws, void *stream);
+int rb_hllc_stage_clocked(const rb_hllc_fields *f, int32_t stage, void *ws, void *stream);
+/* nsteps x (plan, step). Capturable. */
+int rb_li_enqueue_steps(const rb_li_fields *f, int32_t nsteps, void *ws, void *stream);
+int rb_hllc_enqueue_steps(const rb_hllc_fields *f, int32_t nsteps, void *ws, void *stream);
+/* Commit the last planned step and read the clock. Synchronising. */
+int rb_clock_read(void *ws, void *stream, rb_clock_state *out);
+
 /* --- diagnostics ------------------------------------------------------------ */
 /* Message of this thread's last failed call (empty if none). Returns its length. */
 int rb_last_error(char *buf, size_t n);

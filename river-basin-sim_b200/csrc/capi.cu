@@ -112,6 +112,51 @@ int rb_workspace_init(void* ws, size_t bytes, void* stream) {
   return RB_OK;
 }
 
+static int li_params(const rb_li_fields* f, void* ws, rb::LiParams& p, const char* who) {
+  if (f == nullptr || ws == nullptr) return fail(RB_ERR_ARG, "%s: null argument", who);
+  int rc = check_grid(f->ny, f->nx, f->dx, who);
+  if (rc) return rc;
+  if ((rc = check_bc(f->bc, false, who))) return rc;
+  if (!f->h[0] || !f->h[1] || !f->qx[0] || !f->qx[1] || !f->qy[0] || !f->qy[1] || !f->z || !f->n)
+    return fail(RB_ERR_ARG, "%s: missing state buffer", who);
+  if (f->d50 && (!f->qs_int_x || !f->qs_comp_x || !f->qs_int_y || !f->qs_comp_y))
+    return fail(RB_ERR_ARG, "%s: d50 given without the transport accumulators", who);
+  const bool banks = f->infil != nullptr || any_bc(f->bc, RB_BC_OPEN);
+  p = rb::LiParams{};
+  p.ny = f->ny;
+  p.nx = f->nx;
+  p.dx32 = (float)f->dx;
+  for (int e = 0; e < 4; e++) p.bc[e] = f->bc[e];
+  for (int b = 0; b < 2; b++) {
+    p.hb[b] = f->h[b];
+    p.qxb[b] = f->qx[b];
+    p.qyb[b] = f->qy[b];
+  }
+  p.z = f->z;
+  p.n = f->n;
+  p.h_comp = f->h_comp;
+  p.rain_field = f->rain_field;
+  p.infil = f->infil;
+  p.d50 = f->d50;
+  p.qs_int_x = f->qs_int_x;
+  p.qs_comp_x = f->qs_comp_x;
+  p.qs_int_y = f->qs_int_y;
+  p.qs_comp_y = f->qs_comp_y;
+  p.ledger = banks ? (double*)((char*)ws + rb::WS_LEDGER) : nullptr;
+  p.err = &header(ws)->err;
+  return RB_OK;
+}
+
+int rb_li_step_clocked(const rb_li_fields* f, void* ws, void* stream) {
+  rb::LiParams p;
+  int rc = li_params(f, ws, p, "rb_li_step_clocked");
+  if (rc) return rc;
+  p.clk = &header(ws)->clock;
+  p.hmax_key = &header(ws)->clock.red_key;
+  RB_CUDA(rb::li_step_launch(p, (cudaStream_t)stream), "rb_li_step_clocked launch");
+  return RB_OK;
+}
+
 int rb_li_step(const rb_li_fields* f, int32_t cur, const rb_step_args* a, void* ws, void* stream) {
   if (f == nullptr || a == nullptr || ws == nullptr) return fail(RB_ERR_ARG, "rb_li_step: null argument");
   int rc = check_grid(f->ny, f->nx, f->dx, "rb_li_step");
@@ -119,7 +164,6 @@ int rb_li_step(const rb_li_fields* f, int32_t cur, const rb_step_args* a, void* 
   if ((rc = check_bc(f->bc, false, "rb_li_step"))) return rc;
   if ((rc = check_dt(a->dt, "rb_li_step"))) return rc;
   if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_li_step: cur must be 0 or 1");
-  const int nxt = cur ^ 1;
   if (!f->h[0] || !f->h[1] || !f->qx[0] || !f->qx[1] || !f->qy[0] || !f->qy[1] || !f->z || !f->n)
     return fail(RB_ERR_ARG, "rb_li_step: missing state buffer");
   if (f->d50 && (!f->qs_int_x || !f->qs_comp_x || !f->qs_int_y || !f->qs_comp_y))
@@ -138,14 +182,15 @@ int rb_li_step(const rb_li_fields* f, int32_t cur, const rb_step_args* a, void* 
   p.dxdt = (float)(a->dt / f->dx);  // boundaries.py:329
   p.limit = a->limit ? 1 : 0;
   for (int e = 0; e < 4; e++) p.bc[e] = f->bc[e];
-  p.h = f->h[cur];
-  p.qx = f->qx[cur];
-  p.qy = f->qy[cur];
+  for (int b = 0; b < 2; b++) {
+    p.hb[b] = f->h[b];
+    p.qxb[b] = f->qx[b];
+    p.qyb[b] = f->qy[b];
+  }
+  p.cur = cur;
   p.z = f->z;
   p.n = f->n;
-  p.h_out = f->h[nxt];
-  p.qx_out = f->qx[nxt];
-  p.qy_out = f->qy[nxt];
+  p.clk = nullptr;
   p.h_comp = f->h_comp;
   p.rain_field = f->rain_field;
   p.infil = f->infil;
@@ -186,27 +231,21 @@ int rb_li_compute_dt(const rb_li_fields* f, int32_t cur, double alpha, double dt
   return RB_OK;
 }
 
-static int hllc_stage_impl(const rb_hllc_fields* f, int32_t cur, const rb_step_args* a, void* ws, void* stream,
-                           int stage_mask) {
-  if (f == nullptr || a == nullptr || ws == nullptr) return fail(RB_ERR_ARG, "rb_hllc_step: null argument");
-  int rc = check_grid(f->ny, f->nx, f->dx, "rb_hllc_step");
+static int hllc_params(const rb_hllc_fields* f, void* ws, rb::HllcParams& p, const char* who) {
+  if (f == nullptr || ws == nullptr) return fail(RB_ERR_ARG, "%s: null argument", who);
+  int rc = check_grid(f->ny, f->nx, f->dx, who);
   if (rc) return rc;
-  if ((rc = check_bc(f->bc, true, "rb_hllc_step"))) return rc;
-  if ((rc = check_dt(a->dt, "rb_hllc_step"))) return rc;
-  if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_hllc_step: cur must be 0 or 1");
-  const int nxt = cur ^ 1;
+  if ((rc = check_bc(f->bc, true, who))) return rc;
   if (!f->h[0] || !f->h[1] || !f->hu[0] || !f->hu[1] || !f->hv[0] || !f->hv[1] || !f->z || !f->n)
-    return fail(RB_ERR_ARG, "rb_hllc_step: missing state buffer");
+    return fail(RB_ERR_ARG, "%s: missing state buffer", who);
   const bool banks = f->infil != nullptr || any_bc(f->bc, RB_BC_OPEN) || any_bc(f->bc, RB_BC_STAGE);
   const size_t cells = (size_t)f->ny * f->nx;
   char* u1 = (char*)ws + rb::ws_hllc_u1_offset(f->ny, f->nx);
   const size_t plane = align256(cells * sizeof(float));
-
-  rb::HllcParams p{};
+  p = rb::HllcParams{};
   p.ny = f->ny;
   p.nx = f->nx;
   p.dx32 = (float)f->dx;
-  p.dt32 = (float)a->dt;
   p.z = f->z;
   p.n = f->n;
   p.h1 = (float*)u1;
@@ -215,37 +254,38 @@ static int hllc_stage_impl(const rb_hllc_fields* f, int32_t cur, const rb_step_a
   p.h_comp = f->h_comp;
   p.rain_field = f->rain_field;
   p.infil = f->infil;
+  for (int e = 0; e < 4; e++) p.bc[e] = f->bc[e];
+  for (int b = 0; b < 2; b++) {
+    p.hb[b] = f->h[b];
+    p.hub[b] = f->hu[b];
+    p.hvb[b] = f->hv[b];
+  }
+  p.ledger = banks ? (double*)((char*)ws + rb::WS_LEDGER) : nullptr;
+  p.err = &header(ws)->err;
+  return RB_OK;
+}
+
+static int hllc_stage_impl(const rb_hllc_fields* f, int32_t cur, const rb_step_args* a, void* ws, void* stream,
+                           int stage_mask) {
+  if (a == nullptr) return fail(RB_ERR_ARG, "rb_hllc_step: null argument");
+  rb::HllcParams p;
+  int rc = hllc_params(f, ws, p, "rb_hllc_step");
+  if (rc) return rc;
+  if ((rc = check_dt(a->dt, "rb_hllc_step"))) return rc;
+  if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_hllc_step: cur must be 0 or 1");
+  p.cur = cur;
+  p.dt32 = (float)a->dt;
   p.rain32 = (float)a->rain;
   p.scale32 = (float)a->rain_scale;
   const bool comp = f->h_comp != nullptr;
   p.rain_mode = (comp && f->rain_field == nullptr) ? 1 : (a->rain != 0.0 ? 2 : 0);  // hllc.py:1350-1356
-  for (int e = 0; e < 4; e++) {
-    p.bc[e] = f->bc[e];
-    p.stage[e] = (float)a->stage[e];
-  }
+  for (int e = 0; e < 4; e++) p.stage[e] = (float)a->stage[e];
   p.wt = 0.5 * a->dt / f->dx;  // hllc.py:1320
-  p.ledger = banks ? (double*)((char*)ws + rb::WS_LEDGER) : nullptr;
-  p.err = &header(ws)->err;
+  p.clk = nullptr;
   p.smax_key = nullptr;
   cudaStream_t s = (cudaStream_t)stream;
-  if (stage_mask & 1) {  // stage 1: U^n -> U1
-    p.h_s = f->h[cur];
-    p.hu_s = f->hu[cur];
-    p.hv_s = f->hv[cur];
-    RB_CUDA(rb::hllc_stage_launch(p, 1, s), "rb_hllc_step stage 1");
-  }
-  if (stage_mask & 2) {  // stage 2: (U^n, U1) -> U^{n+1}
-    p.h_s = p.h1;
-    p.hu_s = p.hu1;
-    p.hv_s = p.hv1;
-    p.h_n = f->h[cur];
-    p.hu_n = f->hu[cur];
-    p.hv_n = f->hv[cur];
-    p.h_out = f->h[nxt];
-    p.hu_out = f->hu[nxt];
-    p.hv_out = f->hv[nxt];
-    RB_CUDA(rb::hllc_stage_launch(p, 2, s), "rb_hllc_step stage 2");
-  }
+  if (stage_mask & 1) RB_CUDA(rb::hllc_stage_launch(p, 1, s), "rb_hllc_step stage 1");  // U^n -> U1
+  if (stage_mask & 2) RB_CUDA(rb::hllc_stage_launch(p, 2, s), "rb_hllc_step stage 2");  // (U^n, U1) -> U^{n+1}
   return RB_OK;
 }
 
@@ -281,6 +321,141 @@ int rb_hllc_compute_dt(const rb_hllc_fields* f, int32_t cur, double alpha, doubl
   }
   const double dt = alpha * f->dx / smax;
   *dt_out = dt < dt_max ? dt : dt_max;
+  return RB_OK;
+}
+
+// --- device-resident clock ---------------------------------------------------
+static int clock_start(int scheme, int ny, int nx, double dx, int32_t cur, const rb_clock_config* cfg, void* ws,
+                       cudaStream_t s) {
+  if (cfg == nullptr) return fail(RB_ERR_ARG, "clock start: null config");
+  if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "clock start: cur must be 0 or 1");
+  if (cfg->nsync < 0 || (cfg->nsync > 0 && cfg->sync == nullptr))
+    return fail(RB_ERR_ARG, "clock start: nsync > 0 needs a device sync array");
+  if (!(cfg->alpha > 0.0) || !(cfg->dt_max > 0.0)) return fail(RB_ERR_ARG, "clock start: alpha and dt_max must be > 0");
+  rb::DevClock c{};
+  c.t = cfg->t0;
+  c.t1 = cfg->t0;
+  c.t_target = cfg->t0;
+  c.alpha = cfg->alpha;
+  c.dt_max = cfg->dt_max;
+  c.dx = dx;
+  c.rain_rate = cfg->rain_rate;
+  c.rain_until = cfg->rain_until;
+  c.rain_field_sum = cfg->rain_field_sum;
+  c.cell_area = dx * dx;
+  c.n_cells = (double)ny * (double)nx;
+  c.sync = cfg->sync;
+  c.nsync = cfg->nsync;
+  c.sync_pos = 0;
+  c.scheme = scheme;
+  c.rain_is_field = cfg->rain_is_field ? 1 : 0;
+  c.cur = cur;
+  c.limit = cfg->limit ? 1 : 0;
+  rb::DevClock* dc = &header(ws)->clock;
+  RB_CUDA(cudaMemcpyAsync(dc, &c, sizeof c, cudaMemcpyHostToDevice, s), "clock start copy");
+  RB_CUDA(cudaStreamSynchronize(s), "clock start sync");  // the source is a stack object
+  return RB_OK;
+}
+
+int rb_li_clock_start(const rb_li_fields* f, int32_t cur, const rb_clock_config* cfg, void* ws, void* stream) {
+  rb::LiParams p;
+  int rc = li_params(f, ws, p, "rb_li_clock_start");
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  if ((rc = clock_start(0, f->ny, f->nx, f->dx, cur, cfg, ws, s))) return rc;
+  RB_CUDA(rb::reduce_max_h(f->h[cur], (size_t)f->ny * f->nx, &header(ws)->clock.red_key, s), "rb_li_clock_start");
+  return RB_OK;
+}
+
+int rb_hllc_clock_start(const rb_hllc_fields* f, int32_t cur, const rb_clock_config* cfg, void* ws, void* stream) {
+  rb::HllcParams p;
+  int rc = hllc_params(f, ws, p, "rb_hllc_clock_start");
+  if (rc) return rc;
+  if (any_bc(f->bc, RB_BC_STAGE))
+    return fail(RB_ERR_ARG, "rb_hllc_clock_start: fixed_stage edges are stepped by the host loop (rb_hllc_step)");
+  cudaStream_t s = (cudaStream_t)stream;
+  if ((rc = clock_start(1, f->ny, f->nx, f->dx, cur, cfg, ws, s))) return rc;
+  RB_CUDA(rb::reduce_wavespeed(f->h[cur], f->hu[cur], f->hv[cur], (size_t)f->ny * f->nx, &header(ws)->clock.red_key,
+                               s),
+          "rb_hllc_clock_start");
+  return RB_OK;
+}
+
+int rb_clock_set_target(void* ws, double t_target, int32_t max_steps, void* stream) {
+  if (ws == nullptr || max_steps < 0) return fail(RB_ERR_ARG, "rb_clock_set_target: bad argument");
+  RB_CUDA(rb::clock_target_launch(&header(ws)->clock, t_target, max_steps, (cudaStream_t)stream), "rb_clock_set_target");
+  return RB_OK;
+}
+
+int rb_clock_plan(void* ws, void* stream) {
+  if (ws == nullptr) return fail(RB_ERR_ARG, "rb_clock_plan: null workspace");
+  RB_CUDA(rb::clock_plan_launch(&header(ws)->clock, (cudaStream_t)stream), "rb_clock_plan");
+  return RB_OK;
+}
+
+int rb_hllc_stage_clocked(const rb_hllc_fields* f, int32_t stage, void* ws, void* stream) {
+  if (stage != 1 && stage != 2) return fail(RB_ERR_ARG, "rb_hllc_stage_clocked: stage must be 1 or 2");
+  rb::HllcParams p;
+  int rc = hllc_params(f, ws, p, "rb_hllc_stage_clocked");
+  if (rc) return rc;
+  if (any_bc(f->bc, RB_BC_STAGE))
+    return fail(RB_ERR_ARG, "rb_hllc_stage_clocked: fixed_stage edges are stepped by the host loop");
+  p.clk = &header(ws)->clock;
+  p.smax_key = &header(ws)->clock.red_key;
+  RB_CUDA(rb::hllc_stage_launch(p, stage, (cudaStream_t)stream), "rb_hllc_stage_clocked");
+  return RB_OK;
+}
+
+int rb_li_enqueue_steps(const rb_li_fields* f, int32_t nsteps, void* ws, void* stream) {
+  if (nsteps < 0) return fail(RB_ERR_ARG, "rb_li_enqueue_steps: nsteps < 0");
+  rb::LiParams p;
+  int rc = li_params(f, ws, p, "rb_li_enqueue_steps");
+  if (rc) return rc;
+  p.clk = &header(ws)->clock;
+  p.hmax_key = &header(ws)->clock.red_key;
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int k = 0; k < nsteps; k++) {
+    RB_CUDA(rb::clock_plan_launch(&header(ws)->clock, s), "rb_li_enqueue_steps plan");
+    RB_CUDA(rb::li_step_launch(p, s), "rb_li_enqueue_steps step");
+  }
+  return RB_OK;
+}
+
+int rb_hllc_enqueue_steps(const rb_hllc_fields* f, int32_t nsteps, void* ws, void* stream) {
+  if (nsteps < 0) return fail(RB_ERR_ARG, "rb_hllc_enqueue_steps: nsteps < 0");
+  rb::HllcParams p;
+  int rc = hllc_params(f, ws, p, "rb_hllc_enqueue_steps");
+  if (rc) return rc;
+  if (any_bc(f->bc, RB_BC_STAGE))
+    return fail(RB_ERR_ARG, "rb_hllc_enqueue_steps: fixed_stage edges are stepped by the host loop");
+  p.clk = &header(ws)->clock;
+  p.smax_key = &header(ws)->clock.red_key;
+  cudaStream_t s = (cudaStream_t)stream;
+  for (int k = 0; k < nsteps; k++) {
+    RB_CUDA(rb::clock_plan_launch(&header(ws)->clock, s), "rb_hllc_enqueue_steps plan");
+    RB_CUDA(rb::hllc_stage_launch(p, 1, s), "rb_hllc_enqueue_steps stage 1");
+    RB_CUDA(rb::hllc_stage_launch(p, 2, s), "rb_hllc_enqueue_steps stage 2");
+  }
+  return RB_OK;
+}
+
+int rb_clock_read(void* ws, void* stream, rb_clock_state* out) {
+  if (ws == nullptr || out == nullptr) return fail(RB_ERR_ARG, "rb_clock_read: null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  rb::DevClock* dc = &header(ws)->clock;
+  RB_CUDA(rb::clock_commit_launch(dc, s), "rb_clock_read commit");
+  rb::DevClock c;
+  unsigned int err = 0;
+  RB_CUDA(cudaMemcpyAsync(&c, dc, sizeof c, cudaMemcpyDeviceToHost, s), "rb_clock_read copy");
+  RB_CUDA(cudaMemcpyAsync(&err, &header(ws)->err, sizeof err, cudaMemcpyDeviceToHost, s), "rb_clock_read err");
+  RB_CUDA(cudaStreamSynchronize(s), "rb_clock_read sync");
+  out->t = c.t;
+  out->dt = c.dt;
+  out->rain_volume = c.rain_in[0];
+  out->cur = c.cur;
+  out->steps = c.steps;
+  out->err = c.err | err;
+  out->reserved = 0;
   return RB_OK;
 }
 

@@ -142,18 +142,38 @@ __global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
 
   const int ny = p.ny, nx = p.nx;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const float dt = p.dt32, dx = p.dx32;
+  int cur = p.cur, rain_mode = p.rain_mode;
+  float dt = p.dt32, rain32 = p.rain32, scale32 = p.scale32;
+  double wt = p.wt;
+  if (p.clk != nullptr) {  // device-resident clock: this step's dt and forcing
+    const DevClock* c = p.clk;
+    if (!c->active) return;
+    cur = c->cur;
+    dt = c->dt32;
+    wt = c->wt;
+    rain32 = c->rain32;
+    scale32 = c->scale32;
+    rain_mode = (p.h_comp != nullptr && p.rain_field == nullptr) ? 1 : (rain32 != 0.0f ? 2 : 0);
+  }
+  // Stage input U_s (U^n for stage 1, U1 for stage 2) and U^n.
+  const float* __restrict__ h_s = STAGE == 1 ? p.hb[cur] : p.h1;
+  const float* __restrict__ hu_s = STAGE == 1 ? p.hub[cur] : p.hu1;
+  const float* __restrict__ hv_s = STAGE == 1 ? p.hvb[cur] : p.hv1;
+  const float* __restrict__ h_n = p.hb[cur];
+  const float* __restrict__ hu_n = p.hub[cur];
+  const float* __restrict__ hv_n = p.hvb[cur];
+  const float dx = p.dx32;
 
   // 1. stage the clamped halo and the primitives (hllc.py:262-282).
   for (int k = threadIdx.x; k < RH * RW; k += NT) {
     const int r = k / RW, c = k - r * RW;
     const int gi = min(max(y0 - H + r, 0), ny - 1), gj = min(max(x0 - H + c, 0), nx - 1);
     const size_t id = (size_t)gi * nx + gj;
-    const float hh = p.h_s[id];
+    const float hh = h_s[id];
     float u = 0.0f, v = 0.0f;
     if (hh > kHDry) {
-      u = p.hu_s[id] / hh;
-      v = p.hv_s[id] / hh;
+      u = hu_s[id] / hh;
+      v = hv_s[id] / hh;
     }
     s_h[r][c] = hh;
     s_u[r][c] = u;
@@ -293,8 +313,8 @@ __global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
     }
     s_fxh[a][b] = q;
     if (p.ledger != nullptr) {
-      if (gj == 0 && p.bc[RB_EDGE_WEST] != RB_BC_CLOSED) loss -= p.wt * (double)q;
-      if (gj == nx && (b <= TX || gj == nx) && p.bc[RB_EDGE_EAST] != RB_BC_CLOSED) loss += p.wt * (double)q;
+      if (gj == 0 && p.bc[RB_EDGE_WEST] != RB_BC_CLOSED) loss -= wt * (double)q;
+      if (gj == nx && (b <= TX || gj == nx) && p.bc[RB_EDGE_EAST] != RB_BC_CLOSED) loss += wt * (double)q;
     }
   }
   for (int k = threadIdx.x; k < (TY + 1) * TX; k += NT) {
@@ -309,8 +329,8 @@ __global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
     }
     s_fyh[a][b] = q;
     if (p.ledger != nullptr) {
-      if (gi == 0 && p.bc[RB_EDGE_NORTH] != RB_BC_CLOSED) loss -= p.wt * (double)q;
-      if (gi == ny && p.bc[RB_EDGE_SOUTH] != RB_BC_CLOSED) loss += p.wt * (double)q;
+      if (gi == 0 && p.bc[RB_EDGE_NORTH] != RB_BC_CLOSED) loss -= wt * (double)q;
+      if (gi == ny && p.bc[RB_EDGE_SOUTH] != RB_BC_CLOSED) loss += wt * (double)q;
     }
   }
   __syncthreads();
@@ -352,37 +372,37 @@ __global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
       const float hh = rmax(hg + dt * dh, 0.0f);
       float hu1 = 0.0f, hv1 = 0.0f;
       if (hh > kHDry) {
-        hu1 = p.hu_s[id] + dt * dhu;
-        hv1 = p.hv_s[id] + dt * dhv;
+        hu1 = hu_s[id] + dt * dhu;
+        hv1 = hv_s[id] + dt * dhv;
       }
       p.h1[id] = hh;
       p.hu1[id] = hu1;
       p.hv1[id] = hv1;
     } else {  // hllc.py:881-909, then friction :912-939, then sources :1350-1373
-      float hh = rmax(0.5f * (p.h_n[id] + hg + dt * dh), 0.0f);
+      float hh = rmax(0.5f * (h_n[id] + hg + dt * dh), 0.0f);
       float hu = 0.0f, hv = 0.0f;
       if (hh > kHDry) {
-        hu = 0.5f * (p.hu_n[id] + p.hu_s[id] + dt * dhu);
-        hv = 0.5f * (p.hv_n[id] + p.hv_s[id] + dt * dhv);
+        hu = 0.5f * (hu_n[id] + hu_s[id] + dt * dhu);
+        hv = 0.5f * (hv_n[id] + hv_s[id] + dt * dhv);
         const float mom = sqrtf(hu * hu + hv * hv);
         const float denom = manning_denominator(mom, hh, p.n[id], g, dt);
         hu = hu / denom;
         hv = hv / denom;
       }
-      if (p.rain_mode == 1) {
+      if (rain_mode == 1) {
         float comp = p.h_comp[id];
-        kahan_add(hh, comp, p.rain32 * dt);
+        kahan_add(hh, comp, rain32 * dt);
         p.h_comp[id] = comp;
-      } else if (p.rain_mode == 2) {
-        hh = hh + p.rain32 * dt;  // hllc.py:942-945
+      } else if (rain_mode == 2) {
+        hh = hh + rain32 * dt;  // hllc.py:942-945
       }
       if (p.rain_field != nullptr) {
         if (p.h_comp != nullptr) {
           float comp = p.h_comp[id];
-          kahan_add(hh, comp, p.rain_field[id] * p.scale32 * dt);
+          kahan_add(hh, comp, p.rain_field[id] * scale32 * dt);
           p.h_comp[id] = comp;
         } else {
-          hh = hh + p.rain_field[id] * p.scale32 * dt;
+          hh = hh + p.rain_field[id] * scale32 * dt;
         }
       }
       if (p.infil != nullptr) {  // local_inertial.py:170-194
@@ -393,9 +413,9 @@ __global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
         hh = avail - inf;
         loss += (double)avail - (double)hh;
       }
-      p.h_out[id] = hh;
-      p.hu_out[id] = hu;
-      p.hv_out[id] = hv;
+      p.hb[cur ^ 1][id] = hh;
+      p.hub[cur ^ 1][id] = hu;
+      p.hvb[cur ^ 1][id] = hv;
       // hllc.py:948-966 _reduce_wavespeed on the new state
       const float cw = sqrtf(g * rmax(hh, 0.0f));
       float s = cw;

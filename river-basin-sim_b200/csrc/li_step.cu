@@ -67,7 +67,26 @@ __global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
 
   const int ny = p.ny, nx = p.nx;
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
-  const float dt = p.dt32, dx = p.dx32;
+  int cur = p.cur, limit = p.limit;
+  float dt = p.dt32, rain_cont = p.rain_cont, rain32 = p.rain32, scale32 = p.scale32, dxdt = p.dxdt;
+  if (p.clk != nullptr) {  // device-resident clock: this step's dt and forcing
+    const DevClock* c = p.clk;
+    if (!c->active) return;
+    cur = c->cur;
+    limit = c->limit;
+    dt = c->dt32;
+    rain32 = c->rain32;
+    rain_cont = p.h_comp != nullptr ? 0.0f : rain32;
+    scale32 = c->scale32;
+    dxdt = c->dxdt32;
+  }
+  const float* __restrict__ h_in = p.hb[cur];
+  const float* __restrict__ qx_in = p.qxb[cur];
+  const float* __restrict__ qy_in = p.qyb[cur];
+  float* __restrict__ h_out = p.hb[cur ^ 1];
+  float* __restrict__ qx_out = p.qxb[cur ^ 1];
+  float* __restrict__ qy_out = p.qyb[cur ^ 1];
+  const float dx = p.dx32;
   const float dtdx = dt / dx;
 
   // 1. stage h, z, n (halo 2) and eta = h + z (local_inertial.py:61-69).
@@ -77,7 +96,7 @@ __global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
     float h = 0.0f, z = 0.0f, n = 0.0f;
     if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
       const size_t id = (size_t)gi * nx + gj;
-      h = p.h[id];
+      h = h_in[id];
       z = p.z[id];
       n = p.n[id];
     }
@@ -98,7 +117,7 @@ __global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
       const float eta_l = s_eta[a + 1][b], eta_r = s_eta[a + 1][b + 1];
       const float h_flow = rmax(eta_l, eta_r) - rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
       if (!(h_flow < kHDry)) {
-        const float qo = p.qx[(size_t)gi * (nx + 1) + gj];
+        const float qo = qx_in[(size_t)gi * (nx + 1) + gj];
         const float n_face = 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]);
         const float slope = (eta_r - eta_l) / dx;
         const float num = qo - kG * h_flow * dt * slope;
@@ -116,7 +135,7 @@ __global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
       const float eta_t = s_eta[a][b + 1], eta_b = s_eta[a + 1][b + 1];
       const float h_flow = rmax(eta_t, eta_b) - rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
       if (!(h_flow < kHDry)) {
-        const float qo = p.qy[(size_t)gi * nx + gj];
+        const float qo = qy_in[(size_t)gi * nx + gj];
         const float n_face = 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]);
         const float slope = (eta_b - eta_t) / dx;
         const float num = qo - kG * h_flow * dt * slope;
@@ -129,7 +148,7 @@ __global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
   __syncthreads();
 
   // 3. donor-cell beta on the tile plus a 1-cell ring (local_inertial.py:197-239).
-  if (p.limit) {
+  if (limit) {
     for (int k = threadIdx.x; k < BH * BW; k += NT) {
       const int a = k / BW, b = k - a * BW;
       float q_out = 0.0f;
@@ -179,7 +198,7 @@ __global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
     if (gi >= ny || gj > nx || (b == TX + 1 && gj != nx)) continue;
     const size_t fid = (size_t)gi * (nx + 1) + gj;
     const float q = s_qx[a][b];
-    p.qx_out[fid] = q;
+    qx_out[fid] = q;
     if (p.d50 != nullptr && gj >= 1 && gj <= nx - 1) {
       const float eta_max = rmax(s_eta[a + 1][b], s_eta[a + 1][b + 1]);
       const float z_bank = rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
@@ -199,7 +218,7 @@ __global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
     if (gj >= nx || gi > ny || (a == TY + 1 && gi != ny)) continue;
     const size_t fid = (size_t)gi * nx + gj;
     const float q = s_qy[a][b];
-    p.qy_out[fid] = q;
+    qy_out[fid] = q;
     if (p.d50 != nullptr && gi >= 1 && gi <= ny - 1) {
       const float eta_max = rmax(s_eta[a][b + 1], s_eta[a + 1][b + 1]);
       const float z_bank = rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
@@ -214,7 +233,7 @@ __global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
   }
 
   // 6. continuity, areal sources, infiltration, open-edge sinks, per tile cell.
-  const float rain_dt = p.rain_cont * dt;
+  const float rain_dt = rain_cont * dt;
   double loss = 0.0;
   float hmax = 0.0f;
   bool bad = false;
@@ -230,12 +249,12 @@ __global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
     if (p.h_comp != nullptr) {
       float comp = p.h_comp[id];
       if (p.rain_field == nullptr)
-        kahan_add(h, comp, p.rain32 * dt);  // sources.py:85-101
+        kahan_add(h, comp, rain32 * dt);  // sources.py:85-101
       else
-        kahan_add(h, comp, p.rain_field[id] * p.scale32 * dt);  // sources.py:104-121
+        kahan_add(h, comp, p.rain_field[id] * scale32 * dt);  // sources.py:104-121
       p.h_comp[id] = comp;
     } else if (p.rain_field != nullptr) {
-      h = h + p.rain_field[id] * p.scale32 * dt;  // local_inertial.py:154-167
+      h = h + p.rain_field[id] * scale32 * dt;  // local_inertial.py:154-167
     }
     if (p.infil != nullptr) {  // local_inertial.py:170-194
       const float avail = h;
@@ -248,25 +267,25 @@ __global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
     // boundaries.py:259-318, launched west, east, north, south.
     if (p.bc[RB_EDGE_WEST] == RB_BC_OPEN && nx > 1 && gj == 0) {
       const float avail = h;
-      h = drain(avail, rmax(-qxr, 0.0f), p.dxdt);
+      h = drain(avail, rmax(-qxr, 0.0f), dxdt);
       loss += (double)avail - (double)h;
     }
     if (p.bc[RB_EDGE_EAST] == RB_BC_OPEN && nx > 1 && gj == nx - 1) {
       const float avail = h;
-      h = drain(avail, rmax(qxl, 0.0f), p.dxdt);
+      h = drain(avail, rmax(qxl, 0.0f), dxdt);
       loss += (double)avail - (double)h;
     }
     if (p.bc[RB_EDGE_NORTH] == RB_BC_OPEN && ny > 1 && gi == 0) {
       const float avail = h;
-      h = drain(avail, rmax(-qyb, 0.0f), p.dxdt);
+      h = drain(avail, rmax(-qyb, 0.0f), dxdt);
       loss += (double)avail - (double)h;
     }
     if (p.bc[RB_EDGE_SOUTH] == RB_BC_OPEN && ny > 1 && gi == ny - 1) {
       const float avail = h;
-      h = drain(avail, rmax(qyt, 0.0f), p.dxdt);
+      h = drain(avail, rmax(qyt, 0.0f), dxdt);
       loss += (double)avail - (double)h;
     }
-    p.h_out[id] = h;
+    h_out[id] = h;
     hmax = h > hmax ? h : hmax;
     bad |= !(fabsf(h) <= FLT_MAX);
   }

@@ -11,6 +11,36 @@ namespace rb {
 constexpr int LI_TX = 32, LI_TY = 16, LI_NT = 256;
 constexpr int HLLC_TX = 32, HLLC_TY = 16, HLLC_NT = 256;
 
+// The device-resident clock (solver/scheduler.py:171-246 + compute_dt + the run
+// loop's rain gating and source ledger, run.py:369-388), one per workspace. The
+// plan kernel fills the per-step fields below from the state-derived reduction;
+// step kernels given a clock read their dt, forcing and buffer index from it.
+struct DevClock {
+  double t;          // simulated time at the start of the next step
+  double t1;         // end of the planned step
+  double dt;         // the planned step (float64, as the host scheduler has it)
+  double t_target;   // the span ends when t >= t_target - EPS_T
+  double alpha, dt_max, dx;
+  double rain_rate, rain_until, rain_field_sum, cell_area;
+  double n_cells;
+  double rain_in[2];    // Kahan (total, compensation) of areal rain volume, m^3
+  double inflow_in[2];  // Kahan of point-source volume, m^3
+  double wt;            // 0.5 * dt / dx (HLLC banking weight)
+  const double* sync;   // ascending sync times (device memory owned by the caller)
+  int nsync, sync_pos;
+  int scheme;           // 0 local inertial, 1 HLLC
+  int rain_is_field;
+  int cur;              // buffer holding the current state
+  int active;           // the planned step runs
+  int pending;          // a planned step awaits commit by the next plan
+  int steps;            // committed steps since the clock was set
+  int max_steps;        // step budget of the current span
+  unsigned int red_key; // state-derived max for the next dt (filled by the step kernel)
+  unsigned int err;
+  float dt32, dxdt32, rain32, scale32;
+  int limit;
+};
+
 struct LiParams {
   int ny, nx;
   float dx32, dt32;
@@ -20,8 +50,10 @@ struct LiParams {
   float dxdt;        // float32(dt / dx) in float64, the open-edge drain factor
   int limit;
   int bc[4];
-  const float *h, *z, *n, *qx, *qy;  // buffer [cur]
-  float *h_out, *qx_out, *qy_out;    // buffer [cur ^ 1]
+  float *hb[2], *qxb[2], *qyb[2];   // double buffers; the step reads [cur], writes [cur ^ 1]
+  int cur;
+  const float *z, *n;
+  const DevClock* clk;               // when set: dt, forcing and cur come from the device clock
   float *h_comp;
   const float *rain_field, *infil;
   const float *d50;
@@ -34,11 +66,11 @@ struct LiParams {
 struct HllcParams {
   int ny, nx;
   float dx32, dt32;
-  const float *h_s, *hu_s, *hv_s;  // the stage's input state (U^n, then U1)
+  float *hb[2], *hub[2], *hvb[2];  // double-buffered U: U^n = [cur], U^{n+1} = [cur ^ 1]
+  int cur;
   const float *z, *n;
-  float *h1, *hu1, *hv1;           // stage-1 output (workspace)
-  const float *h_n, *hu_n, *hv_n;  // U^n for the stage-2 convex combination
-  float *h_out, *hu_out, *hv_out;  // U^{n+1}
+  float *h1, *hu1, *hv1;           // stage-1 output U1 (workspace)
+  const DevClock* clk;
   float *h_comp;
   const float *rain_field, *infil;
   float rain32, scale32;
@@ -52,6 +84,9 @@ struct HllcParams {
 };
 
 cudaError_t li_step_launch(const LiParams& p, cudaStream_t s);
+cudaError_t clock_plan_launch(DevClock* clk, cudaStream_t s);
+cudaError_t clock_commit_launch(DevClock* clk, cudaStream_t s);
+cudaError_t clock_target_launch(DevClock* clk, double t_target, int max_steps, cudaStream_t s);
 cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s);
 int li_tiles(int ny, int nx);
 int hllc_tiles(int ny, int nx);
@@ -62,7 +97,10 @@ struct WsHeader {
   unsigned int err;      // device error bits
   unsigned int pad[2];
   double sum;            // f64 reduction result
+  double pad2[5];
+  DevClock clock;        // the device-resident clock (offset 64)
 };
+static_assert(sizeof(WsHeader) <= 1024, "workspace header overflows its reserved block");
 constexpr size_t WS_HEADER = 1024;
 constexpr int WS_SUM_BLOCKS = 1184;  // 8 x 148 SMs: fixed so the f64 sum order is fixed
 constexpr size_t WS_PARTIALS = WS_HEADER;                             // WS_SUM_BLOCKS doubles

@@ -53,6 +53,22 @@ class StepArgs(ctypes.Structure):
     ]  # fmt: skip
 
 
+class ClockConfig(ctypes.Structure):
+    _fields_ = [
+        ("alpha", ctypes.c_double), ("dt_max", ctypes.c_double), ("t0", ctypes.c_double), ("sync", _P),
+        ("nsync", ctypes.c_int32), ("rain_is_field", ctypes.c_int32), ("rain_rate", ctypes.c_double),
+        ("rain_until", ctypes.c_double), ("rain_field_sum", ctypes.c_double), ("limit", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]  # fmt: skip
+
+
+class ClockState(ctypes.Structure):
+    _fields_ = [
+        ("t", ctypes.c_double), ("dt", ctypes.c_double), ("rain_volume", ctypes.c_double),
+        ("cur", ctypes.c_int32), ("steps", ctypes.c_int32), ("err", ctypes.c_uint32), ("reserved", ctypes.c_int32),
+    ]  # fmt: skip
+
+
 # name -> (restype, argtypes) for every exported entry point of include/rbsim.h
 SIGNATURES = {
     "rb_li_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
@@ -72,6 +88,17 @@ SIGNATURES = {
     "rb_ledger_loss": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _P, ctypes.POINTER(ctypes.c_double)]),
     "rb_sum_f64": (ctypes.c_int, [_P, ctypes.c_int64, _P, ctypes.c_size_t, _P, ctypes.POINTER(ctypes.c_double)]),
     "rb_read_device_error": (ctypes.c_int, [_P, _P, ctypes.POINTER(ctypes.c_uint32)]),
+    "rb_li_clock_start": (ctypes.c_int, [ctypes.POINTER(LiFields), ctypes.c_int32, ctypes.POINTER(ClockConfig),
+                                         _P, _P]),
+    "rb_hllc_clock_start": (ctypes.c_int, [ctypes.POINTER(HllcFields), ctypes.c_int32,
+                                           ctypes.POINTER(ClockConfig), _P, _P]),
+    "rb_clock_set_target": (ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int32, _P]),
+    "rb_clock_plan": (ctypes.c_int, [_P, _P]),
+    "rb_li_step_clocked": (ctypes.c_int, [ctypes.POINTER(LiFields), _P, _P]),
+    "rb_hllc_stage_clocked": (ctypes.c_int, [ctypes.POINTER(HllcFields), ctypes.c_int32, _P, _P]),
+    "rb_li_enqueue_steps": (ctypes.c_int, [ctypes.POINTER(LiFields), ctypes.c_int32, _P, _P]),
+    "rb_hllc_enqueue_steps": (ctypes.c_int, [ctypes.POINTER(HllcFields), ctypes.c_int32, _P, _P]),
+    "rb_clock_read": (ctypes.c_int, [_P, _P, ctypes.POINTER(ClockState)]),
     "rb_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
     "rb_version": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)] * 3),
 }  # fmt: skip

@@ -1,0 +1,117 @@
+"""Device-resident stepping: the run loop's clock on the GPU, replayed as CUDA graphs.
+
+The reference run loop (solver/run.py:369-388) reads a float back from the device
+every step (``compute_dt``) and clamps it on the host (solver/scheduler.py). Here
+the same float64 arithmetic runs in a one-thread plan kernel on the device
+(librbsim ``rb_clock_plan``), the step kernels read their dt from it, and a span of
+``graph_steps`` steps is captured once into a CUDA graph and replayed. The host only
+looks at the clock between replays, and only to ask "has the span's target been
+reached?". The result is bit-identical to stepping through ``compute_dt`` /
+``step``: same state-derived dt, same fill_span clamp, same rain gating.
+
+Sync times must include every time a step may not cross (outputs, forcing
+breakpoints, slow-process activations, the end time), exactly as they are given
+to ``MultiRateScheduler``; ``run_until`` is then called with a sync time as target.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+import torch
+
+from . import _lib
+from .scheduler import EPS_T
+from .state import State
+
+
+class DeviceClock:
+    def __init__(self, state: State, scheme: str, *, alpha: float, dt_max: float, sync_times, t0: float = 0.0,
+                 rain_rate: float = 0.0, rain_until: float = 0.0, limit: bool = True, graph_steps: int = 32,
+                 use_graph: bool = True):  # fmt: skip
+        if scheme not in ("local_inertial", "hllc_fv"):
+            raise ValueError(f"unknown scheme {scheme!r}")
+        self.state = state
+        self.scheme = scheme
+        self.graph_steps = int(graph_steps)
+        self.use_graph = use_graph
+        self._L = _lib.lib()
+        sync = np.sort(np.asarray(list(sync_times), dtype=np.float64))
+        self._sync = torch.from_numpy(sync).to(state.device)
+        field = state.rain is not None
+        rain_sum = float(state.rain.double().sum().item()) if field else 0.0
+        self._cfg = _lib.ClockConfig(float(alpha), float(dt_max), float(t0), self._sync.data_ptr(), len(sync),
+                                     1 if field else 0, float(rain_rate), float(rain_until), rain_sum,
+                                     1 if limit else 0, 0)  # fmt: skip
+        if scheme == "hllc_fv":
+            state.arm_hllc_fields()
+            self._fields = state.hllc_fields()
+            _lib.check(self._L.rb_hllc_clock_start(ctypes.byref(self._fields), state.cur, ctypes.byref(self._cfg),
+                                                   state.workspace.data_ptr(), state.stream))  # fmt: skip
+        else:
+            self._fields = state.li_fields()
+            _lib.check(self._L.rb_li_clock_start(ctypes.byref(self._fields), state.cur, ctypes.byref(self._cfg),
+                                                 state.workspace.data_ptr(), state.stream))  # fmt: skip
+        self._graph: torch.cuda.CUDAGraph | None = None
+        self.t = float(t0)
+        self.steps = 0
+        self.rain_volume = 0.0
+
+    # -- enqueue ------------------------------------------------------------------ #
+    def _enqueue(self, n: int, stream: int) -> None:
+        ws = self.state.workspace.data_ptr()
+        if self.scheme == "hllc_fv":
+            _lib.check(self._L.rb_hllc_enqueue_steps(ctypes.byref(self._fields), n, ws, stream))
+        else:
+            _lib.check(self._L.rb_li_enqueue_steps(ctypes.byref(self._fields), n, ws, stream))
+
+    def _replay(self) -> None:
+        if not self.use_graph:
+            self._enqueue(self.graph_steps, self.state.stream)
+            return
+        if self._graph is None:
+            g = torch.cuda.CUDAGraph()
+            s = torch.cuda.Stream(self.state.device)
+            s.wait_stream(torch.cuda.current_stream(self.state.device))
+            with torch.cuda.graph(g, stream=s):
+                self._enqueue(self.graph_steps, s.cuda_stream)
+            torch.cuda.current_stream(self.state.device).wait_stream(s)
+            self._graph = g
+        self._graph.replay()
+
+    def set_target(self, t_target: float, max_steps: int = 2**31 - 1) -> None:
+        _lib.check(self._L.rb_clock_set_target(self.state.workspace.data_ptr(), float(t_target), int(max_steps),
+                                               self.state.stream))  # fmt: skip
+
+    def read(self) -> _lib.ClockState:
+        out = _lib.ClockState()
+        _lib.check(self._L.rb_clock_read(self.state.workspace.data_ptr(), self.state.stream, ctypes.byref(out)))
+        self.state.cur = out.cur
+        self.t, self.steps, self.rain_volume = out.t, out.steps, out.rain_volume
+        if out.err & _lib.RB_DEVERR_NONFINITE:
+            raise _lib.DeviceError(f"a step produced a non-finite depth (t = {out.t})")
+        if out.err & _lib.RB_DEVERR_CLOCK:
+            raise RuntimeError(f"non-positive timestep at t={out.t}")
+        return out
+
+    def run_until(self, t_target: float, max_steps: int = 2**31 - 1) -> int:
+        """Step until the state reaches ``t_target`` (a sync time) or ``max_steps`` steps; returns steps taken."""
+        start = self.steps
+        self.set_target(t_target, max_steps)
+        while True:
+            self._replay()
+            st = self.read()
+            taken = st.steps - start
+            if st.t >= t_target - EPS_T or taken >= max_steps:
+                return taken
+
+    def enqueue_span(self, max_steps: int) -> None:
+        """Enqueue (without waiting) replays covering at most ``max_steps`` more steps."""
+        self.set_target(math.inf, max_steps)
+        for _ in range(-(-max_steps // self.graph_steps)):
+            self._replay()
+
+    def close(self) -> None:
+        self._graph = None
