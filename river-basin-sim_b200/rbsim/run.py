@@ -1,0 +1,225 @@
+"""Run a scenario on the B200 and stream results to the Zarr store (solver/run.py:140-584).
+
+Same arming order and hot-loop semantics as the reference ``run_simulation``:
+fields -> morphology (z0 captured after the bed is final) -> infiltration ->
+rain field -> areal-source compensation -> inflow injector -> boundaries ->
+ledgers -> writer + frame 0 -> the scheduler's ticks: inject, step, bank rain,
+advance due slow processes, record + write at output ticks.
+
+Two ways through the ticks, with identical results:
+
+* the **device clock** (default when the scenario has no point inflows and no
+  fixed_stage edges): the scheduler's sync times are uploaded once and the GPU
+  plans and takes every step between host events (outputs, slow-process
+  activations, the end) in CUDA-graph replays; the host wakes only for those.
+* the **host loop**: one ``compute_dt`` + ``step`` per tick exactly as the
+  reference's run loop, used for inflows and stage curves.
+
+    python -m rbsim.run --config scenario.toml --out results.zarr [--status status.json]
+"""
+
+from __future__ import annotations
+
+import argparse
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from .config import Scenario, load_config
+from .grid import H_DRY
+from .io.status import StatusWriter
+from .io.zarr_writer import AsyncFrameWriter, ZarrWriter
+from .massbalance import MassLedger, SedimentLedger
+from .processes.inflow import InflowInjector
+from .processes.morphology import MorphologyProcess, bed_change_bounds
+from .scheduler import EPS_T, MultiRateScheduler
+from .schemes import get_scheme, hllc
+from .sediment import arm_sediment
+from .state import State
+
+
+def _cell_velocities(st: State):
+    """state.py:232-256 on the device: (u, v) cell-centred, 0 where h < H_DRY."""
+    h = st.h
+    wet = h >= H_DRY
+    if st.hu is not None:
+        qx_c, qy_c = st.hu, st.hv
+    else:
+        qx_c = 0.5 * (st.qx[:, :-1] + st.qx[:, 1:])
+        qy_c = 0.5 * (st.qy[:-1, :] + st.qy[1:, :])
+    zero = torch.zeros_like(h)
+    return torch.where(wet, qx_c / h, zero), torch.where(wet, qy_c / h, zero)
+
+
+def run_simulation(scenario: Scenario, bed=None, out_path="results.zarr", *, device="cuda", verbose: bool = True,
+                   status: StatusWriter | None = None, use_device_clock: bool = True,
+                   graph_steps: int = 32) -> MassLedger:  # fmt: skip
+    sc = scenario
+    bed = sc.bed if bed is None else bed
+    if bed is None:
+        raise ValueError("no bed: pass an array or set [grid] dem")
+    if sc.dx is None:
+        raise ValueError("scenario.dx is unresolved")
+    scheme = get_scheme(sc.scheme)
+    st = State.from_bed(bed, sc.dx, depth=sc.initial_depth, manning=sc.manning, device=device)
+    grid = st.grid
+    if sc.scheme == "hllc_fv":
+        hllc.arm_hllc(st)
+
+    morphology = None
+    if sc.has_sediment:
+        arm_sediment(st, sc.sediment_d50, sc.sediment_porosity)
+        dz_lo, dz_hi = bed_change_bounds(grid.shape, alluvium_thickness=sc.alluvium_thickness)
+        morphology = MorphologyProcess(st, sc.sediment_interval_s, dz_lo=dz_lo, dz_hi=dz_hi)
+        if verbose:
+            print(f"  morphology    : {morphology.summary()}")
+
+    infil = np.broadcast_to(np.asarray(sc.infiltration_mm_hr, np.float32), grid.shape)
+    infil_m_s = infil / 1000.0 / 3600.0
+    if not np.isscalar(sc.infiltration_mm_hr) or float(infil_m_s.max()) > 0.0:
+        st.set_infiltration(infil_m_s)
+    rain_is_field = sc.rain_type == "field"
+    rain_field_sum = 0.0
+    if rain_is_field:
+        rf = (np.asarray(sc.rain_field, np.float32) / 1000.0 / 3600.0).astype(np.float32)
+        st.set_rain_field(rf)
+        rain_field_sum = float(rf.astype(np.float64).sum())
+    if rain_is_field or (sc.rain_m_s > 0.0 and sc.rain_duration > 0.0):
+        st.arm_source_compensation()
+    injector = InflowInjector(sc.inflows, grid, st.device) if sc.inflows else None
+    st.set_open_boundaries(sc.boundaries, sc.stage_curves)
+
+    ledger = MassLedger.from_state(st)
+    sed_ledger = SedimentLedger.from_state(st) if morphology is not None else None
+    n_frames = int(round(sc.end_time / sc.output_every)) + 1
+    attrs = {
+        "scheme": sc.scheme, "dx": grid.dx, "coarsen": 1,
+        "units": {"depth": "m", "u": "m/s", "v": "m/s", "time": "s", "bed": "m"},
+        "scenario": sc.name, "rain_type": sc.rain_type, "rain_mm_hr": sc.rain_mm_hr,
+        "rain_duration_s": sc.rain_duration, "end_time_s": sc.end_time, "output_every_s": sc.output_every,
+        "datum_shift_m": 0.0, "solver": "rbsim (B200 CUDA)",
+    }  # fmt: skip
+    if morphology is not None:
+        attrs["sediment"] = {"law": "mpm", **morphology.as_attrs()}
+    writer = ZarrWriter(out_path, grid, n_frames, attrs, bed_change=morphology is not None)
+    writer.write_bed(np.asarray(bed, np.float32))
+    frames = AsyncFrameWriter(writer, st.device)
+
+    def emit(t_out: float) -> None:
+        u, v = _cell_velocities(st)
+        frames.submit(t_out, st.h, u, v, st.sediment.dz_cum if morphology is not None else None)
+
+    emit(0.0)
+    inflow_events = injector.breakpoints() if injector else []
+    sched = MultiRateScheduler(
+        end_time=sc.end_time, output_every=sc.output_every,
+        events=[sc.rain_duration, *inflow_events, *sc.stage_events],
+        processes=[morphology.as_slow_process()] if morphology is not None else [],
+    )  # fmt: skip
+
+    def on_output(t1: float) -> None:
+        rec = ledger.record(st, t1)
+        emit(t1)
+        h_max = float(st.h.max().item())
+        line = f"  t={t1:8.1f}s  h_max={h_max:6.3f}m  mass_rel_err={rec.rel_error:.2e}"
+        if sed_ledger is not None:
+            line += f"  bed_moved={sed_ledger.record(st, t1).gross_volume:9.1f}m3"
+        if verbose:
+            print(line)
+        if status is not None:
+            status.write("running", sim_time=t1,
+                         message=f"t={t1:.0f}s  h_max={h_max:.3f}m  mass_rel_err={rec.rel_error:.1e}")  # fmt: skip
+
+    device_path = use_device_clock and injector is None and not sc.stage_curves
+    if device_path:
+        from .device_clock import DeviceClock
+
+        clock = DeviceClock(st, sc.scheme, alpha=sc.alpha, dt_max=sc.dt_max, sync_times=sched.sync_times,
+                            rain_rate=0.0 if rain_is_field else sc.rain_m_s, rain_until=sc.rain_duration,
+                            graph_steps=graph_steps)  # fmt: skip
+        procs = [p for p in sched.processes]
+        pending = {p.name: list(p.activations(sc.end_time)) for p in procs}
+        last_ran = {p.name: 0.0 for p in procs}
+        outputs = list(sched.output_times)
+        targets = sorted({*outputs, *[t for ts in pending.values() for t in ts], sc.end_time})
+        banked_rain = 0.0
+        next_output = sc.output_every
+        for target in targets:
+            if target <= clock.t + EPS_T:
+                continue
+            clock.run_until(target)
+            t1 = clock.t
+            ledger.add_inflow(clock.rain_volume - banked_rain)
+            banked_rain = clock.rain_volume
+            for p in procs:  # scheduler.py:234-242, on the step that landed here
+                times, fired = pending[p.name], False
+                while times and t1 >= times[0] - EPS_T:
+                    times.pop(0)
+                    fired = True
+                if fired:
+                    p.advance(t1, t1 - last_ran[p.name])
+                    last_ran[p.name] = t1
+            if t1 >= next_output - EPS_T and next_output <= sc.end_time + EPS_T:
+                next_output += sc.output_every
+                on_output(t1)
+        clock.close()
+    else:
+        for tick in sched.ticks(lambda: scheme.compute_dt(st, alpha=sc.alpha, dt_max=sc.dt_max)):
+            t, dt = tick.t0, tick.dt
+            if injector is not None:
+                ledger.add_inflow(injector.apply(st, t, dt))
+            raining = t < sc.rain_duration - EPS_T
+            if rain_is_field:
+                scheme.step(st, dt=dt, rain_scale=(1.0 if raining else 0.0), t=t)
+                if raining:
+                    ledger.add_inflow(rain_field_sum * dt * grid.cell_area)
+            else:
+                rain = sc.rain_m_s if raining else 0.0
+                scheme.step(st, dt=dt, rain=rain, t=t)
+                if rain > 0.0:
+                    ledger.add_rain_step(rain, dt, grid.n_cells)
+            for proc, elapsed in tick.due:
+                proc.advance(tick.t1, elapsed)
+            if tick.is_output:
+                on_output(tick.t1)
+    st.check_device_errors()
+    frames.close()
+    final = dict(ledger.as_attrs())
+    if morphology is not None:
+        final["morphology"] = morphology.series
+        final.update(sed_ledger.as_attrs())
+    writer.finalize(final)
+    if verbose and ledger.max_rel_error >= 1e-6:
+        print(f"  warning: mass balance {ledger.max_rel_error:.2e} exceeds the 1e-6 gate")
+    return ledger
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(prog="python -m rbsim.run")
+    ap.add_argument("--config", required=True)
+    ap.add_argument("--out", default=None)
+    ap.add_argument("--status", default=None)
+    ap.add_argument("--host-loop", action="store_true", help="step through compute_dt/step on the host")
+    args = ap.parse_args(argv)
+    sc = load_config(args.config)
+    out = args.out or str(Path(args.config).with_suffix(".zarr").name)
+    status = StatusWriter(args.status, sc.end_time) if args.status else None
+    try:
+        if status:
+            status.write("starting")
+        t0 = time.time()
+        run_simulation(sc, None, out, status=status, use_device_clock=not args.host_loop)
+        if status:
+            status.write("done", sim_time=sc.end_time, message=f"wall {time.time() - t0:.1f}s")
+    except Exception as e:
+        if status:
+            status.write("error", message=str(e))
+        raise
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -106,6 +106,48 @@ class ReferenceAPI:
         return out
 
 
+SCHEDULER_CASES = {
+    # name: (end_time, output_every, events, [(process name, interval)], dt recipe)
+    "plain": (3600.0, 600.0, [], [], ("const", 7.3)),
+    "rain_and_knots": (7200.0, 900.0, [1800.0, 2.5, 3333.3], [], ("wave", 11.0)),
+    "slow_processes": (5400.0, 1000.0, [1234.5], [("reservoir", 900.0), ("morphology", 600.0)], ("wave", 37.0)),
+    "coarse_dt": (100.0, 30.0, [10.0], [("morphology", 25.0)], ("const", 1000.0)),
+    "near_integer": (10.0, 1.0, [], [], ("const", 0.1)),
+}
+
+
+def _dt_fn(recipe):
+    import math
+
+    kind, base = recipe
+    k = [0]
+
+    def fn():
+        k[0] += 1
+        if kind == "const":
+            return base
+        return base * (1.0 + 0.35 * math.sin(0.37 * k[0]))
+
+    return fn
+
+
+def make_scheduler_fixture(out_path):
+    """Record the reference scheduler's ticks for stub dt sequences (solver/scheduler.py)."""
+    import json
+
+    from solver.scheduler import MultiRateScheduler, SlowProcess
+
+    out = {}
+    for name, (end, every, events, procs, recipe) in SCHEDULER_CASES.items():
+        sp = [SlowProcess(name=n, interval=iv, advance=lambda t, e: None) for n, iv in procs]
+        sched = MultiRateScheduler(end_time=end, output_every=every, events=events, processes=sp)
+        ticks = [[t.index, t.t0, t.dt, t.t1, t.is_output, [[p.name, el] for p, el in t.due]]
+                 for t in sched.ticks(_dt_fn(recipe))]
+        out[name] = {"n_frames": sched.n_frames, "sync": sched.sync_times, "ticks": ticks}
+    with open(out_path, "w") as f:
+        json.dump(out, f)
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True, help="root of the reference source tree")
@@ -119,6 +161,7 @@ def main(argv=None):
     sys.path.insert(0, os.path.abspath(args.reference))
     from cases import CASES, run_case
 
+    make_scheduler_fixture(os.path.join(HERE, "scheduler_ticks.json"))
     api = ReferenceAPI()
     names = args.cases or list(CASES)
     for name in names:

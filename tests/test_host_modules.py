@@ -1,0 +1,127 @@
+"""Host-side modules of the package: scheduler, Zarr store, status.json, config.
+
+The scheduler is pinned tick for tick to fixtures recorded from the reference's own
+``MultiRateScheduler`` (tests/golden/scheduler_ticks.json, made by
+tests/golden/make_golden.py) for the same stub dt sequences.
+"""
+
+from __future__ import annotations
+
+import json
+import os
+
+import numpy as np
+import pytest
+
+from make_golden import SCHEDULER_CASES, _dt_fn
+from rbsim.scheduler import EPS_T, MultiRateScheduler, SlowProcess, fill_span
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "scheduler_ticks.json")
+
+
+@pytest.mark.parametrize("name", sorted(SCHEDULER_CASES))
+def test_scheduler_replays_reference_ticks_exactly(name):
+    want = json.load(open(GOLDEN))[name]
+    end, every, events, procs, recipe = SCHEDULER_CASES[name]
+    sp = [SlowProcess(name=n, interval=iv, advance=lambda t, e: None) for n, iv in procs]
+    sched = MultiRateScheduler(end_time=end, output_every=every, events=events, processes=sp)
+    assert sched.n_frames == want["n_frames"]
+    assert sched.sync_times == want["sync"]
+    got = [[t.index, t.t0, t.dt, t.t1, t.is_output, [[p.name, el] for p, el in t.due]]
+           for t in sched.ticks(_dt_fn(recipe))]  # fmt: skip
+    assert got == want["ticks"]
+
+
+def test_fill_span_invariants():
+    for span in (1.0, 7.3, 599.999999, 1e4, 3.0):
+        for dt_raw in (0.1, 0.7, 2.0, 7.3, 1e5):
+            dt = fill_span(span, dt_raw)
+            assert dt <= dt_raw
+            n = round(span / dt)
+            assert abs(n * dt - span) < 1e-9 * max(span, 1.0)
+    assert fill_span(float("inf"), 3.0) == 3.0
+
+
+def test_scheduler_rejects_bad_inputs():
+    with pytest.raises(ValueError):
+        MultiRateScheduler(end_time=0.0, output_every=1.0)
+    with pytest.raises(ValueError):
+        MultiRateScheduler(end_time=10.0, output_every=0.0)
+    with pytest.raises(ValueError):
+        SlowProcess("p", 0.0, lambda t, e: None)
+    sched = MultiRateScheduler(end_time=10.0, output_every=5.0)
+    with pytest.raises(RuntimeError, match="non-positive timestep"):
+        next(iter(sched.ticks(lambda: 0.0)))
+
+
+def test_zarr_store_layout_and_roundtrip(tmp_path):
+    from rbsim.grid import Grid
+    from rbsim.io.zarr_writer import ZarrWriter, read_array, read_attrs
+
+    g = Grid(3, 4, 10.0)
+    w = ZarrWriter(tmp_path / "r.zarr", g, 3, {"scheme": "local_inertial", "dx": 10.0}, bed_change=True)
+    bed = np.arange(12, dtype=np.float32).reshape(3, 4)
+    w.write_bed(bed)
+    rng = np.random.default_rng(0)
+    frames = [rng.random((4, 3, 4)).astype(np.float32) for _ in range(2)]
+    for k, f in enumerate(frames):
+        w.append(10.0 * k, f[0], f[1], f[2], f[3].astype(np.float64))
+    with pytest.raises(ValueError, match="bed_change"):
+        w.append(20.0, frames[0][0], frames[0][1], frames[0][2])
+    w.finalize({"mass_gate": 1e-6, "series": [{"t": 1.0}]})
+    store = tmp_path / "r.zarr"
+    meta = json.loads((store / "depth" / "zarr.json").read_text())
+    assert meta["zarr_format"] == 3 and meta["dimension_names"] == ["time", "y", "x"]
+    assert meta["chunk_grid"]["configuration"]["chunk_shape"] == [1, 3, 4]
+    assert (store / "depth" / "c" / "1" / "0" / "0").exists()
+    depth = read_array(store, "depth")
+    np.testing.assert_array_equal(depth[:2], np.stack([f[0] for f in frames]))
+    np.testing.assert_array_equal(depth[2], 0.0)
+    np.testing.assert_array_equal(read_array(store, "bed"), bed)
+    np.testing.assert_array_equal(read_array(store, "time"), [0.0, 10.0, 0.0])
+    attrs = read_attrs(store)
+    assert attrs["n_frames"] == 2 and attrs["n_frames_allocated"] == 3 and attrs["mass_gate"] == 1e-6
+
+
+def test_status_writer_states(tmp_path):
+    from rbsim.io.status import StatusWriter
+
+    s = StatusWriter(tmp_path / "status.json", end_time=100.0)
+    s.write("starting")
+    s.write("running", sim_time=25.0, message="t=25s")
+    rec = json.loads((tmp_path / "status.json").read_text())
+    assert rec["state"] == "running" and rec["progress"] == 0.25 and rec["message"] == "t=25s"
+    s.write("done", sim_time=50.0)
+    assert json.loads((tmp_path / "status.json").read_text())["progress"] == 1.0
+    with pytest.raises(ValueError):
+        s.write("paused")
+    assert not (tmp_path / "status.json.tmp").exists()
+
+
+def test_config_loader(tmp_path):
+    from rbsim.config import ConfigError, load_config
+
+    (tmp_path / "n.r32").write_bytes(np.full((4, 5), 0.04, "<f4").tobytes())
+    toml = tmp_path / "s.toml"
+    toml.write_text(
+        '[meta]\nname = "t"\nscheme = "local_inertial"\n[grid]\ndx = 10.0\nshape = [4, 5]\n'
+        '[run]\nend_time = 600.0\noutput_every = 60.0\ncfl = 0.7\n'
+        '[rainfall]\ntype = "uniform"\nrate_mm_hr = 36.0\nduration_s = 300.0\n'
+        '[parameters]\nmanning_n = "n.r32"\ninfiltration = 2.0\n'
+        '[sediment]\nd50 = 0.002\nporosity = 0.4\ninterval_s = 120.0\n'
+        '[[inflow]]\ncell = [1, 2]\nhydrograph = [[0.0, 1.0], [600.0, 2.0]]\n'
+        '[boundaries]\ndefault = "closed"\neast = "open"\n'
+    )
+    sc = load_config(toml)
+    assert sc.rain_m_s == pytest.approx(1e-5) and sc.boundaries["east"] == "open"
+    assert sc.manning.shape == (4, 5) and sc.has_sediment and sc.inflows[0].cell == (1, 2)
+    bad = tmp_path / "b.toml"
+    bad.write_text('[meta]\nscheme = "hllc_fv"\n[sediment]\nd50 = 0.002\n')
+    with pytest.raises(ConfigError, match="local-inertial-only"):
+        load_config(bad)
+    bad.write_text('[meta]\nscheme = "local_inertial"\n[boundaries]\neast = { type = "fixed_stage", level = 1.0 }\n')
+    with pytest.raises(ConfigError, match="hllc_fv"):
+        load_config(bad)
+    bad.write_text("[channels]\nwidth = 3.0\n")
+    with pytest.raises(ConfigError, match="outside"):
+        load_config(bad)
