@@ -252,7 +252,7 @@ def main(argv=None) -> int:
     stream.wait_stream(side)
     for _ in range(args.warmup):  # W untimed warm-up steps
         clk.set_target(T_END, 1)
-        _lib.check(L.rb_hllc_enqueue_steps(ctypes.byref(f), 1, ws, stream.cuda_stream))
+        _lib.check(L.rb_hllc_enqueue_steps(ctypes.byref(f), 1, 0, ws, stream.cuda_stream))
     clk.set_target(T_END, K)
     barrier()
     start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -159,7 +159,8 @@ int rb_read_device_error(void *ws, void *stream, uint32_t *err_out);
  * clamps it with fill_span to the next sync time, gates the rain and banks its
  * volume, all in float64 in the reference's operation order, so K steps run
  * without host round trips and can be captured in a CUDA graph. The clock lives
- * in the workspace. Fixed_stage edges and point sources stay on the host loop. */
+ * in the workspace. Point sources (inflow.py:167-200) and fixed_stage curves
+ * (boundaries.py:199-220) are sampled on the device from tables in device memory. */
 typedef struct rb_clock_config {
   double alpha, dt_max;      /* compute_dt arguments */
   double t0;                 /* simulated time of the current state */
@@ -172,13 +173,23 @@ typedef struct rb_clock_config {
   double rain_until;         /* rain duration, s */
   double rain_field_sum;     /* float64 sum of the rain field, m/s (run.py:276) */
   int32_t limit;             /* LI donor limiter */
+  int32_t nsrc;              /* point sources (0: none) */
+  const int32_t *src_cell;   /* device, nsrc: row * nx + col, distinct cells */
+  const int32_t *knot_off;   /* device, nsrc + 1: source k's hydrograph knots are [off[k], off[k+1]) */
+  const double *knot_t;      /* device: knot times (s), non-decreasing per source */
+  const double *knot_q;      /* device: knot discharges (m^3/s) */
+  float *src_comp;           /* device, nsrc: Kahan residue per source, or NULL for the plain add */
+  int32_t stage_off[5];      /* fixed_stage curve of edge e: stage_t/v[off[e] .. off[e+1]) (empty: none) */
   int32_t reserved;
+  const double *stage_t;     /* device: curve knot times */
+  const double *stage_v;     /* device: curve levels (m, stepping datum) */
 } rb_clock_config;
 
 typedef struct rb_clock_state {
   double t;            /* simulated time of the committed state */
   double dt;           /* the last planned step */
   double rain_volume;  /* areal rain banked since start, m^3 (ledger add_rain_step) */
+  double inflow_volume; /* point-source volume requested since start, m^3 (InflowInjector.apply) */
   int32_t cur;         /* the buffer holding the state */
   int32_t steps;       /* steps taken since start */
   uint32_t err;        /* RB_DEVERR_* bits raised by the clock or the steps */
@@ -196,9 +207,11 @@ int rb_clock_plan(void *ws, void *stream);
 /* One clocked launch: a no-op when the plan stopped the clock. Capturable. */
 int rb_li_step_clocked(const rb_li_fields *f, void *ws, void *stream);
 int rb_hllc_stage_clocked(const rb_hllc_fields *f, int32_t stage, void *ws, void *stream);
-/* nsteps x (plan, step). Capturable. */
-int rb_li_enqueue_steps(const rb_li_fields *f, int32_t nsteps, void *ws, void *stream);
-int rb_hllc_enqueue_steps(const rb_hllc_fields *f, int32_t nsteps, void *ws, void *stream);
+/* The planned step's point-source injection into buffer [cur] of (h0, h1). Capturable. */
+int rb_clock_inflow(const float *h0, const float *h1, void *ws, void *stream);
+/* nsteps x (plan, [point sources when with_sources], step). Capturable. */
+int rb_li_enqueue_steps(const rb_li_fields *f, int32_t nsteps, int32_t with_sources, void *ws, void *stream);
+int rb_hllc_enqueue_steps(const rb_hllc_fields *f, int32_t nsteps, int32_t with_sources, void *ws, void *stream);
 /* Commit the last planned step and read the clock. Synchronising. */
 int rb_clock_read(void *ws, void *stream, rb_clock_state *out);
 

@@ -351,6 +351,22 @@ static int clock_start(int scheme, int ny, int nx, double dx, int32_t cur, const
   c.rain_is_field = cfg->rain_is_field ? 1 : 0;
   c.cur = cur;
   c.limit = cfg->limit ? 1 : 0;
+  if (cfg->nsrc < 0 || (cfg->nsrc > 0 && (!cfg->src_cell || !cfg->knot_off || !cfg->knot_t || !cfg->knot_q)))
+    return fail(RB_ERR_ARG, "clock start: point sources need device cell, offset and knot arrays");
+  c.nsrc = cfg->nsrc;
+  c.src_cell = cfg->src_cell;
+  c.knot_off = cfg->knot_off;
+  c.knot_t = cfg->knot_t;
+  c.knot_q = cfg->knot_q;
+  c.src_comp = cfg->src_comp;
+  for (int e = 0; e < 5; e++) {
+    c.stage_off[e] = cfg->stage_off[e];
+    if (e > 0 && cfg->stage_off[e] < cfg->stage_off[e - 1]) return fail(RB_ERR_ARG, "clock start: stage_off must be ascending");
+  }
+  if (c.stage_off[4] > c.stage_off[0] && (!cfg->stage_t || !cfg->stage_v))
+    return fail(RB_ERR_ARG, "clock start: stage curves need device knot arrays");
+  c.stage_t = cfg->stage_t;
+  c.stage_v = cfg->stage_v;
   rb::DevClock* dc = &header(ws)->clock;
   RB_CUDA(cudaMemcpyAsync(dc, &c, sizeof c, cudaMemcpyHostToDevice, s), "clock start copy");
   RB_CUDA(cudaStreamSynchronize(s), "clock start sync");  // the source is a stack object
@@ -371,8 +387,9 @@ int rb_hllc_clock_start(const rb_hllc_fields* f, int32_t cur, const rb_clock_con
   rb::HllcParams p;
   int rc = hllc_params(f, ws, p, "rb_hllc_clock_start");
   if (rc) return rc;
-  if (any_bc(f->bc, RB_BC_STAGE))
-    return fail(RB_ERR_ARG, "rb_hllc_clock_start: fixed_stage edges are stepped by the host loop (rb_hllc_step)");
+  for (int e = 0; e < 4; e++)
+    if (f->bc[e] == RB_BC_STAGE && cfg->stage_off[e + 1] <= cfg->stage_off[e])
+      return fail(RB_ERR_ARG, "rb_hllc_clock_start: fixed_stage edge %d has no stage curve", e);
   cudaStream_t s = (cudaStream_t)stream;
   if ((rc = clock_start(1, f->ny, f->nx, f->dx, cur, cfg, ws, s))) return rc;
   RB_CUDA(rb::reduce_wavespeed(f->h[cur], f->hu[cur], f->hv[cur], (size_t)f->ny * f->nx, &header(ws)->clock.red_key,
@@ -387,6 +404,13 @@ int rb_clock_set_target(void* ws, double t_target, int32_t max_steps, void* stre
   return RB_OK;
 }
 
+int rb_clock_inflow(const float* h0, const float* h1, void* ws, void* stream) {
+  if (ws == nullptr || h0 == nullptr || h1 == nullptr) return fail(RB_ERR_ARG, "rb_clock_inflow: null argument");
+  float* hb[2] = {const_cast<float*>(h0), const_cast<float*>(h1)};
+  RB_CUDA(rb::clock_inflow_launch(&header(ws)->clock, hb, (cudaStream_t)stream), "rb_clock_inflow");
+  return RB_OK;
+}
+
 int rb_clock_plan(void* ws, void* stream) {
   if (ws == nullptr) return fail(RB_ERR_ARG, "rb_clock_plan: null workspace");
   RB_CUDA(rb::clock_plan_launch(&header(ws)->clock, (cudaStream_t)stream), "rb_clock_plan");
@@ -398,15 +422,13 @@ int rb_hllc_stage_clocked(const rb_hllc_fields* f, int32_t stage, void* ws, void
   rb::HllcParams p;
   int rc = hllc_params(f, ws, p, "rb_hllc_stage_clocked");
   if (rc) return rc;
-  if (any_bc(f->bc, RB_BC_STAGE))
-    return fail(RB_ERR_ARG, "rb_hllc_stage_clocked: fixed_stage edges are stepped by the host loop");
   p.clk = &header(ws)->clock;
   p.smax_key = &header(ws)->clock.red_key;
   RB_CUDA(rb::hllc_stage_launch(p, stage, (cudaStream_t)stream), "rb_hllc_stage_clocked");
   return RB_OK;
 }
 
-int rb_li_enqueue_steps(const rb_li_fields* f, int32_t nsteps, void* ws, void* stream) {
+int rb_li_enqueue_steps(const rb_li_fields* f, int32_t nsteps, int32_t with_sources, void* ws, void* stream) {
   if (nsteps < 0) return fail(RB_ERR_ARG, "rb_li_enqueue_steps: nsteps < 0");
   rb::LiParams p;
   int rc = li_params(f, ws, p, "rb_li_enqueue_steps");
@@ -416,23 +438,23 @@ int rb_li_enqueue_steps(const rb_li_fields* f, int32_t nsteps, void* ws, void* s
   cudaStream_t s = (cudaStream_t)stream;
   for (int k = 0; k < nsteps; k++) {
     RB_CUDA(rb::clock_plan_launch(&header(ws)->clock, s), "rb_li_enqueue_steps plan");
+    if (with_sources) RB_CUDA(rb::clock_inflow_launch(&header(ws)->clock, p.hb, s), "rb_li_enqueue_steps inflow");
     RB_CUDA(rb::li_step_launch(p, s), "rb_li_enqueue_steps step");
   }
   return RB_OK;
 }
 
-int rb_hllc_enqueue_steps(const rb_hllc_fields* f, int32_t nsteps, void* ws, void* stream) {
+int rb_hllc_enqueue_steps(const rb_hllc_fields* f, int32_t nsteps, int32_t with_sources, void* ws, void* stream) {
   if (nsteps < 0) return fail(RB_ERR_ARG, "rb_hllc_enqueue_steps: nsteps < 0");
   rb::HllcParams p;
   int rc = hllc_params(f, ws, p, "rb_hllc_enqueue_steps");
   if (rc) return rc;
-  if (any_bc(f->bc, RB_BC_STAGE))
-    return fail(RB_ERR_ARG, "rb_hllc_enqueue_steps: fixed_stage edges are stepped by the host loop");
   p.clk = &header(ws)->clock;
   p.smax_key = &header(ws)->clock.red_key;
   cudaStream_t s = (cudaStream_t)stream;
   for (int k = 0; k < nsteps; k++) {
     RB_CUDA(rb::clock_plan_launch(&header(ws)->clock, s), "rb_hllc_enqueue_steps plan");
+    if (with_sources) RB_CUDA(rb::clock_inflow_launch(&header(ws)->clock, p.hb, s), "rb_hllc_enqueue_steps inflow");
     RB_CUDA(rb::hllc_stage_launch(p, 1, s), "rb_hllc_enqueue_steps stage 1");
     RB_CUDA(rb::hllc_stage_launch(p, 2, s), "rb_hllc_enqueue_steps stage 2");
   }
@@ -452,6 +474,7 @@ int rb_clock_read(void* ws, void* stream, rb_clock_state* out) {
   out->t = c.t;
   out->dt = c.dt;
   out->rain_volume = c.rain_in[0];
+  out->inflow_volume = c.inflow_in[0];
   out->cur = c.cur;
   out->steps = c.steps;
   out->err = c.err | err;

@@ -34,6 +34,31 @@ __device__ __forceinline__ double fill_span(double span, double dt_raw) {
   return dt;
 }
 
+// boundaries.py:199-220 stage_at: piecewise linear, held (not zeroed) outside.
+__device__ double stage_at(const double* tk, const double* vk, int n, double t) {
+  if (t <= tk[0]) return vk[0];
+  if (t >= tk[n - 1]) return vk[n - 1];
+  for (int i = 0; i + 1 < n; i++) {
+    if (tk[i] <= t && t <= tk[i + 1]) {
+      if (tk[i + 1] == tk[i]) return vk[i + 1];
+      return vk[i] + (vk[i + 1] - vk[i]) * (t - tk[i]) / (tk[i + 1] - tk[i]);
+    }
+  }
+  return vk[n - 1];
+}
+
+// config.py:111-122 Inflow.discharge_at: piecewise linear, zero outside.
+__device__ double discharge_at(const double* tk, const double* qk, int n, double t) {
+  if (n == 0 || t < tk[0] || t > tk[n - 1]) return 0.0;
+  for (int i = 0; i + 1 < n; i++) {
+    if (tk[i] <= t && t <= tk[i + 1]) {
+      if (tk[i + 1] == tk[i]) return qk[i + 1];
+      return qk[i] + (qk[i + 1] - qk[i]) * (t - tk[i]) / (tk[i + 1] - tk[i]);
+    }
+  }
+  return qk[n - 1];
+}
+
 __device__ __forceinline__ void kahan64(double* acc, double x) {
   const double y = x - acc[1];
   const double t = acc[0] + y;
@@ -105,6 +130,10 @@ __global__ void clock_plan_kernel(DevClock* c) {
   c->wt = 0.5 * dt / c->dx;         // hllc.py:1320
   c->rain32 = (float)rain;
   c->scale32 = scale;
+  for (int e = 0; e < 4; e++) {  // hllc.py:1308-1312, once per step at the midpoint
+    const int a = c->stage_off[e], b = c->stage_off[e + 1];
+    c->stage32[e] = b > a ? (float)stage_at(c->stage_t + a, c->stage_v + a, b - a, t + 0.5 * dt) : 0.0f;
+  }
   c->red_key = 0u;  // the step kernel folds max(h) / max wave speed of its output here
   c->active = 1;
   c->pending = 1;
@@ -120,6 +149,49 @@ __global__ void clock_target_kernel(DevClock* c, double t_target, int max_steps)
   c->active = 0;
   c->t_target = t_target;
   c->max_steps = c->steps + max_steps;
+}
+
+// inflow.py:167-200 InflowInjector.apply for the planned step: midpoint discharge,
+// float32 depth request Q*dt/A per source, Kahan add into the cell (sources are
+// distinct cells), and the float64 sum of the requests banked into the ledger.
+constexpr int INFLOW_NT = 256;
+__global__ void __launch_bounds__(INFLOW_NT) clock_inflow_kernel(DevClock* c, float* h0, float* h1) {
+  if (!c->active) return;
+  __shared__ float s_add[INFLOW_NT];
+  const double t_mid = c->t + 0.5 * c->dt;
+  float* h = c->cur ? h1 : h0;
+  double total = 0.0;
+  for (int base = 0; base < c->nsrc; base += INFLOW_NT) {
+    const int k = base + threadIdx.x;
+    float add = 0.0f;
+    if (k < c->nsrc) {
+      const int a = c->knot_off[k], b = c->knot_off[k + 1];
+      const double vol = discharge_at(c->knot_t + a, c->knot_q + a, b - a, t_mid) * c->dt;
+      add = (float)(vol / c->cell_area);
+      const int cell = c->src_cell[k];
+      if (c->src_comp != nullptr) {
+        float tot = h[cell], cp = c->src_comp[k];
+        kahan_add(tot, cp, add);
+        h[cell] = tot;
+        c->src_comp[k] = cp;
+      } else {
+        h[cell] = h[cell] + add;
+      }
+    }
+    s_add[threadIdx.x] = add;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      const int m = min(INFLOW_NT, c->nsrc - base);
+      for (int i = 0; i < m; i++) total += (double)s_add[i];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) kahan64(c->inflow_in, total * c->cell_area);
+}
+
+cudaError_t clock_inflow_launch(DevClock* clk, float* const* hb, cudaStream_t s) {
+  clock_inflow_kernel<<<1, INFLOW_NT, 0, s>>>(clk, hb[0], hb[1]);
+  return cudaGetLastError();
 }
 
 cudaError_t clock_plan_launch(DevClock* clk, cudaStream_t s) {

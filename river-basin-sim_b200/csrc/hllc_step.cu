@@ -144,6 +144,8 @@ __global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
   const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
   int cur = p.cur, rain_mode = p.rain_mode;
   float dt = p.dt32, rain32 = p.rain32, scale32 = p.scale32;
+  float stage_w = p.stage[RB_EDGE_WEST], stage_e = p.stage[RB_EDGE_EAST];
+  float stage_n = p.stage[RB_EDGE_NORTH], stage_s = p.stage[RB_EDGE_SOUTH];
   double wt = p.wt;
   if (p.clk != nullptr) {  // device-resident clock: this step's dt and forcing
     const DevClock* c = p.clk;
@@ -154,6 +156,10 @@ __global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
     rain32 = c->rain32;
     scale32 = c->scale32;
     rain_mode = (p.h_comp != nullptr && p.rain_field == nullptr) ? 1 : (rain32 != 0.0f ? 2 : 0);
+    stage_w = c->stage32[RB_EDGE_WEST];
+    stage_e = c->stage32[RB_EDGE_EAST];
+    stage_n = c->stage32[RB_EDGE_NORTH];
+    stage_s = c->stage32[RB_EDGE_SOUTH];
   }
   // Stage input U_s (U^n for stage 1, U1 for stage 2) and U^n.
   const float* __restrict__ h_s = STAGE == 1 ? p.hb[cur] : p.h1;
@@ -209,7 +215,7 @@ __global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
         else
           hllc_flux(h0, u0, v0, h0, -u0, v0, fh, f1, ft);
       } else {  // prescribed surface, hllc.py:537-581
-        const float stage = gj == 0 ? p.stage[RB_EDGE_WEST] : p.stage[RB_EDGE_EAST];
+        const float stage = gj == 0 ? stage_w : stage_e;
         const float h_g = rmax(stage - s_z[r][ce], 0.0f);
         if (gj == 0)
           hllc_flux(h_g, u0, v0, h0, u0, v0, fh, f1, ft);
@@ -254,7 +260,7 @@ __global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
         else
           hllc_flux(h0, v0, u0, h0, -v0, u0, fh, f1, ft);
       } else {  // hllc.py:584-628
-        const float stage = gi == 0 ? p.stage[RB_EDGE_NORTH] : p.stage[RB_EDGE_SOUTH];
+        const float stage = gi == 0 ? stage_n : stage_s;
         const float h_g = rmax(stage - s_z[re][c], 0.0f);
         if (gi == 0)
           hllc_flux(h_g, v0, u0, h0, v0, u0, fh, f1, ft);

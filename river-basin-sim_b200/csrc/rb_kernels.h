@@ -39,6 +39,18 @@ struct DevClock {
   unsigned int err;
   float dt32, dxdt32, rain32, scale32;
   int limit;
+  // point sources sampled on the device (solver/processes/inflow.py:167-200)
+  int nsrc;
+  const int* src_cell;   // row * nx + col
+  const int* knot_off;   // nsrc + 1 offsets into knot_t / knot_q
+  const double* knot_t;
+  const double* knot_q;
+  float* src_comp;       // per-source Kahan residue, or null for the plain add
+  // fixed_stage curves per edge (boundaries.py:199-220), evaluated at t + dt/2
+  int stage_off[5];      // edge e's knots are stage_t/v[stage_off[e] .. stage_off[e+1])
+  const double* stage_t;
+  const double* stage_v;
+  float stage32[4];
 };
 
 struct LiParams {
@@ -87,6 +99,7 @@ cudaError_t li_step_launch(const LiParams& p, cudaStream_t s);
 cudaError_t clock_plan_launch(DevClock* clk, cudaStream_t s);
 cudaError_t clock_commit_launch(DevClock* clk, cudaStream_t s);
 cudaError_t clock_target_launch(DevClock* clk, double t_target, int max_steps, cudaStream_t s);
+cudaError_t clock_inflow_launch(DevClock* clk, float* const* hb, cudaStream_t s);
 cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s);
 int li_tiles(int ny, int nx);
 int hllc_tiles(int ny, int nx);

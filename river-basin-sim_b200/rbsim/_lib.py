@@ -58,13 +58,16 @@ class ClockConfig(ctypes.Structure):
         ("alpha", ctypes.c_double), ("dt_max", ctypes.c_double), ("t0", ctypes.c_double), ("sync", _P),
         ("nsync", ctypes.c_int32), ("rain_is_field", ctypes.c_int32), ("rain_rate", ctypes.c_double),
         ("rain_until", ctypes.c_double), ("rain_field_sum", ctypes.c_double), ("limit", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("nsrc", ctypes.c_int32), ("src_cell", _P), ("knot_off", _P), ("knot_t", _P), ("knot_q", _P),
+        ("src_comp", _P), ("stage_off", ctypes.c_int32 * 5), ("reserved", ctypes.c_int32), ("stage_t", _P),
+        ("stage_v", _P),
     ]  # fmt: skip
 
 
 class ClockState(ctypes.Structure):
     _fields_ = [
         ("t", ctypes.c_double), ("dt", ctypes.c_double), ("rain_volume", ctypes.c_double),
+        ("inflow_volume", ctypes.c_double),
         ("cur", ctypes.c_int32), ("steps", ctypes.c_int32), ("err", ctypes.c_uint32), ("reserved", ctypes.c_int32),
     ]  # fmt: skip
 
@@ -96,8 +99,9 @@ SIGNATURES = {
     "rb_clock_plan": (ctypes.c_int, [_P, _P]),
     "rb_li_step_clocked": (ctypes.c_int, [ctypes.POINTER(LiFields), _P, _P]),
     "rb_hllc_stage_clocked": (ctypes.c_int, [ctypes.POINTER(HllcFields), ctypes.c_int32, _P, _P]),
-    "rb_li_enqueue_steps": (ctypes.c_int, [ctypes.POINTER(LiFields), ctypes.c_int32, _P, _P]),
-    "rb_hllc_enqueue_steps": (ctypes.c_int, [ctypes.POINTER(HllcFields), ctypes.c_int32, _P, _P]),
+    "rb_clock_inflow": (ctypes.c_int, [_P, _P, _P, _P]),
+    "rb_li_enqueue_steps": (ctypes.c_int, [ctypes.POINTER(LiFields), ctypes.c_int32, ctypes.c_int32, _P, _P]),
+    "rb_hllc_enqueue_steps": (ctypes.c_int, [ctypes.POINTER(HllcFields), ctypes.c_int32, ctypes.c_int32, _P, _P]),
     "rb_clock_read": (ctypes.c_int, [_P, _P, ctypes.POINTER(ClockState)]),
     "rb_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
     "rb_version": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)] * 3),

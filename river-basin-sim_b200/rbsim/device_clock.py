@@ -9,6 +9,9 @@ looks at the clock between replays, and only to ask "has the span's target been
 reached?". The result is bit-identical to stepping through ``compute_dt`` /
 ``step``: same state-derived dt, same fill_span clamp, same rain gating.
 
+Point inflows (an ``InflowInjector``) and fixed_stage curves are sampled on the
+device at the step midpoint, as the host loop samples them.
+
 Sync times must include every time a step may not cross (outputs, forcing
 breakpoints, slow-process activations, the end time), exactly as they are given
 to ``MultiRateScheduler``; ``run_until`` is then called with a sync time as target.
@@ -30,7 +33,7 @@ from .state import State
 class DeviceClock:
     def __init__(self, state: State, scheme: str, *, alpha: float, dt_max: float, sync_times, t0: float = 0.0,
                  rain_rate: float = 0.0, rain_until: float = 0.0, limit: bool = True, graph_steps: int = 32,
-                 use_graph: bool = True):  # fmt: skip
+                 use_graph: bool = True, injector=None):  # fmt: skip
         if scheme not in ("local_inertial", "hllc_fv"):
             raise ValueError(f"unknown scheme {scheme!r}")
         self.state = state
@@ -44,7 +47,41 @@ class DeviceClock:
         rain_sum = float(state.rain.double().sum().item()) if field else 0.0
         self._cfg = _lib.ClockConfig(float(alpha), float(dt_max), float(t0), self._sync.data_ptr(), len(sync),
                                      1 if field else 0, float(rain_rate), float(rain_until), rain_sum,
-                                     1 if limit else 0, 0)  # fmt: skip
+                                     1 if limit else 0)  # fmt: skip
+        self._keep = []  # device tables the clock points at
+        self.injector = injector
+        if injector is not None and injector.inflows:
+            nx = state.grid.nx
+            cells = [int(i) * nx + int(j) for i, j in (inf.cell for inf in injector.inflows)]
+            offs, kt, kq = [0], [], []
+            for inf in injector.inflows:
+                kt += [float(t) for t, _ in inf.hydrograph]
+                kq += [float(q) for _, q in inf.hydrograph]
+                offs.append(len(kt))
+            dev = state.device
+            tabs = [torch.tensor(cells, dtype=torch.int32, device=dev), torch.tensor(offs, dtype=torch.int32, device=dev),
+                    torch.tensor(kt or [0.0], dtype=torch.float64, device=dev),
+                    torch.tensor(kq or [0.0], dtype=torch.float64, device=dev)]  # fmt: skip
+            self._keep += tabs
+            self._cfg.nsrc = len(cells)
+            self._cfg.src_cell, self._cfg.knot_off, self._cfg.knot_t, self._cfg.knot_q = [t.data_ptr() for t in tabs]
+            self._cfg.src_comp = injector._comp.data_ptr() if injector._comp is not None else None
+        curves = state.stage_curves
+        if curves:
+            from .state import EDGES
+
+            st_t, st_v, off = [], [], [0]
+            for e in EDGES:
+                for tk, lv in curves.get(e, []):
+                    st_t.append(float(tk))
+                    st_v.append(float(lv))
+                off.append(len(st_t))
+            tabs = [torch.tensor(st_t, dtype=torch.float64, device=state.device),
+                    torch.tensor(st_v, dtype=torch.float64, device=state.device)]  # fmt: skip
+            self._keep += tabs
+            for k in range(5):
+                self._cfg.stage_off[k] = off[k]
+            self._cfg.stage_t, self._cfg.stage_v = tabs[0].data_ptr(), tabs[1].data_ptr()
         if scheme == "hllc_fv":
             state.arm_hllc_fields()
             self._fields = state.hllc_fields()
@@ -58,14 +95,16 @@ class DeviceClock:
         self.t = float(t0)
         self.steps = 0
         self.rain_volume = 0.0
+        self.inflow_volume = 0.0
 
     # -- enqueue ------------------------------------------------------------------ #
     def _enqueue(self, n: int, stream: int) -> None:
         ws = self.state.workspace.data_ptr()
+        src = 1 if self._cfg.nsrc > 0 else 0
         if self.scheme == "hllc_fv":
-            _lib.check(self._L.rb_hllc_enqueue_steps(ctypes.byref(self._fields), n, ws, stream))
+            _lib.check(self._L.rb_hllc_enqueue_steps(ctypes.byref(self._fields), n, src, ws, stream))
         else:
-            _lib.check(self._L.rb_li_enqueue_steps(ctypes.byref(self._fields), n, ws, stream))
+            _lib.check(self._L.rb_li_enqueue_steps(ctypes.byref(self._fields), n, src, ws, stream))
 
     def _replay(self) -> None:
         if not self.use_graph:
@@ -90,6 +129,7 @@ class DeviceClock:
         _lib.check(self._L.rb_clock_read(self.state.workspace.data_ptr(), self.state.stream, ctypes.byref(out)))
         self.state.cur = out.cur
         self.t, self.steps, self.rain_volume = out.t, out.steps, out.rain_volume
+        self.inflow_volume = out.inflow_volume
         if out.err & _lib.RB_DEVERR_NONFINITE:
             raise _lib.DeviceError(f"a step produced a non-finite depth (t = {out.t})")
         if out.err & _lib.RB_DEVERR_CLOCK:

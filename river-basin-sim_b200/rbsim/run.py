@@ -8,12 +8,12 @@ advance due slow processes, record + write at output ticks.
 
 Two ways through the ticks, with identical results:
 
-* the **device clock** (default when the scenario has no point inflows and no
-  fixed_stage edges): the scheduler's sync times are uploaded once and the GPU
-  plans and takes every step between host events (outputs, slow-process
-  activations, the end) in CUDA-graph replays; the host wakes only for those.
-* the **host loop**: one ``compute_dt`` + ``step`` per tick exactly as the
-  reference's run loop, used for inflows and stage curves.
+* the **device clock** (default): the scheduler's sync times, the hydrograph
+  knots and the stage curves are uploaded once and the GPU plans and takes every
+  step between host events (outputs, slow-process activations, the end) in
+  CUDA-graph replays; the host wakes only for those.
+* the **host loop** (``use_device_clock=False``): one ``compute_dt`` + ``step`` per
+  tick exactly as the reference's run loop.
 
     python -m rbsim.run --config scenario.toml --out results.zarr [--status status.json]
 """
@@ -133,27 +133,27 @@ def run_simulation(scenario: Scenario, bed=None, out_path="results.zarr", *, dev
             status.write("running", sim_time=t1,
                          message=f"t={t1:.0f}s  h_max={h_max:.3f}m  mass_rel_err={rec.rel_error:.1e}")  # fmt: skip
 
-    device_path = use_device_clock and injector is None and not sc.stage_curves
-    if device_path:
+    if use_device_clock:
         from .device_clock import DeviceClock
 
         clock = DeviceClock(st, sc.scheme, alpha=sc.alpha, dt_max=sc.dt_max, sync_times=sched.sync_times,
                             rain_rate=0.0 if rain_is_field else sc.rain_m_s, rain_until=sc.rain_duration,
-                            graph_steps=graph_steps)  # fmt: skip
+                            graph_steps=graph_steps, injector=injector)  # fmt: skip
         procs = [p for p in sched.processes]
         pending = {p.name: list(p.activations(sc.end_time)) for p in procs}
         last_ran = {p.name: 0.0 for p in procs}
         outputs = list(sched.output_times)
         targets = sorted({*outputs, *[t for ts in pending.values() for t in ts], sc.end_time})
-        banked_rain = 0.0
+        banked_rain = banked_inflow = 0.0
         next_output = sc.output_every
         for target in targets:
             if target <= clock.t + EPS_T:
                 continue
             clock.run_until(target)
             t1 = clock.t
+            ledger.add_inflow(clock.inflow_volume - banked_inflow)
             ledger.add_inflow(clock.rain_volume - banked_rain)
-            banked_rain = clock.rain_volume
+            banked_rain, banked_inflow = clock.rain_volume, clock.inflow_volume
             for p in procs:  # scheduler.py:234-242, on the step that landed here
                 times, fired = pending[p.name], False
                 while times and t1 >= times[0] - EPS_T:
