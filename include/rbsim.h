@@ -215,6 +215,42 @@ int rb_hllc_enqueue_steps(const rb_hllc_fields *f, int32_t nsteps, int32_t with_
 /* Commit the last planned step and read the clock. Synchronising. */
 int rb_clock_read(void *ws, void *stream, rb_clock_state *out);
 
+/* --- ensembles and serving ------------------------------------------------------
+ * Many independent domains (local inertial and HLLC mixed) stepped together: each
+ * keeps its own fields, workspace and device clock (its own dt, rain and target),
+ * and one persistent kernel per scheme walks the (domain, tile) work-list of all of
+ * them; a domain whose clock has stopped costs one early return per tile. A
+ * domain's arithmetic is exactly that of rb_li_step / rb_hllc_step, so its result
+ * does not depend on the batch it is in. No reference counterpart: the reference
+ * runs one scenario per process (solver/run.py:530). The ensemble workspace
+ * (clocks, parameter blocks, tile maps) is caller-allocated, sized by the layout. */
+typedef struct rb_ensemble_layout {
+  int32_t ndom, n_li, n_hllc;
+  int32_t li_variant, hllc_variant;  /* tile shapes: LI 0 = 32x16, 1 = 32x8, 2 = 64x8; HLLC 0 = 32x16, 1 = 32x8 */
+  int32_t li_grid, hllc_grid;        /* persistent grid sizes (set by rb_ensemble_init) */
+  int32_t reserved;
+  int64_t li_tiles, hllc_tiles;
+  int64_t off_clocks, off_li, off_hllc, off_map_li, off_map_hllc, off_targets, bytes;
+} rb_ensemble_layout;
+
+/* Host only: the workspace layout of ndom domains (scheme 0 = LI, 1 = HLLC). */
+int rb_ensemble_layout_make(int32_t ndom, const int32_t *scheme, const int32_t *ny, const int32_t *nx,
+                            int32_t li_variant, int32_t hllc_variant, rb_ensemble_layout *out);
+/* Fill the ensemble workspace from each domain's fields (li[] for the LI domains
+ * and hl[] for the HLLC domains, in domain order), its own workspace (dom_ws[d],
+ * sized by rb_*_workspace_bytes), clock configuration (no point sources or stage
+ * curves) and current buffer; seeds every domain's dt reduction. Synchronising. */
+int rb_ensemble_init(rb_ensemble_layout *L, void *ens, const int32_t *scheme, const rb_li_fields *li,
+                     const rb_hllc_fields *hl, void *const *dom_ws, const rb_clock_config *cfg, const int32_t *cur,
+                     void *stream);
+/* Per-domain span targets (host arrays). Synchronising. */
+int rb_ensemble_set_targets(const rb_ensemble_layout *L, void *ens, const double *t_target, const int32_t *max_steps,
+                            void *stream);
+/* nsteps x (plan every clock, LI tiles, HLLC stage 1 tiles, HLLC stage 2 tiles). Capturable. */
+int rb_ensemble_enqueue(const rb_ensemble_layout *L, void *ens, int32_t nsteps, void *stream);
+/* Commit and read every domain's clock into out[ndom]. Synchronising. */
+int rb_ensemble_read(const rb_ensemble_layout *L, void *ens, rb_clock_state *out, void *stream);
+
 /* --- diagnostics ------------------------------------------------------------ */
 /* Message of this thread's last failed call (empty if none). Returns its length. */
 int rb_last_error(char *buf, size_t n);

@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "rb_common.cuh"
 #include "rb_kernels.h"
@@ -66,9 +67,12 @@ bool any_bc(const int32_t* bc, int kind) {
 
 namespace rb {
 
+void set_last_error(const char* msg) { snprintf(g_err, sizeof g_err, "%s", msg); }
+
 size_t ws_ledger_bytes(int ny, int nx) {
-  const int t = li_tiles(ny, nx) > hllc_tiles(ny, nx) ? li_tiles(ny, nx) : hllc_tiles(ny, nx);
-  return align256((size_t)t * 2 * sizeof(double));
+  // one slot per tile of the smallest tile any kernel variant uses (32 x 8)
+  const size_t t = (size_t)((nx + 31) / 32) * (size_t)((ny + 7) / 8);
+  return align256(t * 2 * sizeof(double));
 }
 size_t ws_li_bytes(int ny, int nx) { return WS_LEDGER + ws_ledger_bytes(ny, nx); }
 size_t ws_hllc_u1_offset(int ny, int nx) { return WS_LEDGER + ws_ledger_bytes(ny, nx); }
@@ -479,6 +483,203 @@ int rb_clock_read(void* ws, void* stream, rb_clock_state* out) {
   out->steps = c.steps;
   out->err = c.err | err;
   out->reserved = 0;
+  return RB_OK;
+}
+
+// --- ensembles ----------------------------------------------------------------
+static int64_t tiles_of(int ny, int nx, int tx, int ty) {
+  return (int64_t)((nx + tx - 1) / tx) * (int64_t)((ny + ty - 1) / ty);
+}
+
+int rb_ensemble_layout_make(int32_t ndom, const int32_t* scheme, const int32_t* ny, const int32_t* nx,
+                            int32_t li_variant, int32_t hllc_variant, rb_ensemble_layout* out) {
+  if (ndom < 1 || !scheme || !ny || !nx || !out) return fail(RB_ERR_ARG, "rb_ensemble_layout_make: bad argument");
+  if (li_variant < 0 || li_variant > 2 || hllc_variant < 0 || hllc_variant > 1)
+    return fail(RB_ERR_ARG, "rb_ensemble_layout_make: unknown tile variant");
+  rb_ensemble_layout L{};
+  L.ndom = ndom;
+  L.li_variant = li_variant;
+  L.hllc_variant = hllc_variant;
+  int ltx, lty, htx, hty;
+  rb::li_variant_tile(li_variant, &ltx, &lty);
+  rb::hllc_variant_tile(hllc_variant, &htx, &hty);
+  for (int d = 0; d < ndom; d++) {
+    if (ny[d] < 1 || nx[d] < 1) return fail(RB_ERR_ARG, "rb_ensemble_layout_make: domain %d has an empty grid", d);
+    if (scheme[d] == 0) {
+      L.n_li++;
+      L.li_tiles += tiles_of(ny[d], nx[d], ltx, lty);
+    } else if (scheme[d] == 1) {
+      L.n_hllc++;
+      L.hllc_tiles += tiles_of(ny[d], nx[d], htx, hty);
+    } else {
+      return fail(RB_ERR_ARG, "rb_ensemble_layout_make: domain %d has unknown scheme %d", d, scheme[d]);
+    }
+  }
+  size_t off = 256;
+  L.off_clocks = (int64_t)off;
+  off += align256((size_t)ndom * sizeof(rb::DevClock));
+  L.off_li = (int64_t)off;
+  off += align256((size_t)L.n_li * sizeof(rb::LiParams));
+  L.off_hllc = (int64_t)off;
+  off += align256((size_t)L.n_hllc * sizeof(rb::HllcParams));
+  L.off_map_li = (int64_t)off;
+  off += align256((size_t)L.li_tiles * sizeof(int2));
+  L.off_map_hllc = (int64_t)off;
+  off += align256((size_t)L.hllc_tiles * sizeof(int2));
+  L.off_targets = (int64_t)off;
+  off += align256((size_t)ndom * (sizeof(double) + sizeof(int32_t)));
+  L.bytes = (int64_t)off;
+  *out = L;
+  return RB_OK;
+}
+
+int rb_ensemble_init(rb_ensemble_layout* L, void* ens, const int32_t* scheme, const rb_li_fields* li,
+                     const rb_hllc_fields* hl, void* const* dom_ws, const rb_clock_config* cfg, const int32_t* cur,
+                     void* stream) {
+  if (!L || !ens || !scheme || !dom_ws || !cfg || !cur) return fail(RB_ERR_ARG, "rb_ensemble_init: null argument");
+  if ((L->n_li > 0 && !li) || (L->n_hllc > 0 && !hl)) return fail(RB_ERR_ARG, "rb_ensemble_init: missing fields");
+  cudaStream_t s = (cudaStream_t)stream;
+  char* base = (char*)ens;
+  rb::DevClock* clocks = (rb::DevClock*)(base + L->off_clocks);
+  std::vector<rb::DevClock> hc(L->ndom);
+  std::vector<rb::LiParams> hli(L->n_li);
+  std::vector<rb::HllcParams> hhl(L->n_hllc);
+  std::vector<int2> mli, mhl;
+  mli.reserve((size_t)L->li_tiles);
+  mhl.reserve((size_t)L->hllc_tiles);
+  int ltx, lty, htx, hty;
+  rb::li_variant_tile(L->li_variant, &ltx, &lty);
+  rb::hllc_variant_tile(L->hllc_variant, &htx, &hty);
+  int ili = 0, ihl = 0;
+  for (int d = 0; d < L->ndom; d++) {
+    if (!dom_ws[d]) return fail(RB_ERR_ARG, "rb_ensemble_init: domain %d has no workspace", d);
+    int rc;
+    rb::DevClock c{};
+    const rb_clock_config& k = cfg[d];
+    int ny, nx;
+    double dx;
+    if (scheme[d] == 0) {
+      const rb_li_fields& f = li[ili];
+      if ((rc = li_params(&f, dom_ws[d], hli[ili], "rb_ensemble_init"))) return rc;
+      hli[ili].clk = &clocks[d];
+      hli[ili].hmax_key = &clocks[d].red_key;
+      ny = f.ny, nx = f.nx, dx = f.dx;
+      const int64_t nt = tiles_of(ny, nx, ltx, lty);
+      for (int64_t t = 0; t < nt; t++) mli.push_back(make_int2(ili, (int)t));
+      ili++;
+    } else {
+      const rb_hllc_fields& f = hl[ihl];
+      if ((rc = hllc_params(&f, dom_ws[d], hhl[ihl], "rb_ensemble_init"))) return rc;
+      hhl[ihl].clk = &clocks[d];
+      hhl[ihl].smax_key = &clocks[d].red_key;
+      ny = f.ny, nx = f.nx, dx = f.dx;
+      const int64_t nt = tiles_of(ny, nx, htx, hty);
+      for (int64_t t = 0; t < nt; t++) mhl.push_back(make_int2(ihl, (int)t));
+      ihl++;
+    }
+    if (!(k.alpha > 0.0) || !(k.dt_max > 0.0)) return fail(RB_ERR_ARG, "rb_ensemble_init: domain %d alpha/dt_max", d);
+    if (k.nsrc != 0 || k.stage_off[4] != k.stage_off[0])
+      return fail(RB_ERR_ARG, "rb_ensemble_init: domain %d: ensembles step rain and fields only (no point "
+                  "sources or stage curves)", d);
+    c.t = c.t1 = c.t_target = k.t0;
+    c.alpha = k.alpha;
+    c.dt_max = k.dt_max;
+    c.dx = dx;
+    c.rain_rate = k.rain_rate;
+    c.rain_until = k.rain_until;
+    c.rain_field_sum = k.rain_field_sum;
+    c.cell_area = dx * dx;
+    c.n_cells = (double)ny * (double)nx;
+    c.sync = k.sync;
+    c.nsync = k.nsync;
+    c.scheme = scheme[d];
+    c.rain_is_field = k.rain_is_field ? 1 : 0;
+    c.cur = cur[d];
+    c.limit = k.limit ? 1 : 0;
+    hc[d] = c;
+  }
+  L->li_grid = rb::ens_li_grid_size(L->li_variant);
+  L->hllc_grid = rb::ens_hllc_grid_size(L->hllc_variant);
+  RB_CUDA(cudaMemcpyAsync(clocks, hc.data(), hc.size() * sizeof(rb::DevClock), cudaMemcpyHostToDevice, s), "ens clocks");
+  if (!hli.empty())
+    RB_CUDA(cudaMemcpyAsync(base + L->off_li, hli.data(), hli.size() * sizeof(rb::LiParams), cudaMemcpyHostToDevice, s),
+            "ens li");
+  if (!hhl.empty())
+    RB_CUDA(cudaMemcpyAsync(base + L->off_hllc, hhl.data(), hhl.size() * sizeof(rb::HllcParams),
+                            cudaMemcpyHostToDevice, s),
+            "ens hllc");
+  if (!mli.empty())
+    RB_CUDA(cudaMemcpyAsync(base + L->off_map_li, mli.data(), mli.size() * sizeof(int2), cudaMemcpyHostToDevice, s),
+            "ens map li");
+  if (!mhl.empty())
+    RB_CUDA(cudaMemcpyAsync(base + L->off_map_hllc, mhl.data(), mhl.size() * sizeof(int2), cudaMemcpyHostToDevice, s),
+            "ens map hllc");
+  // seed each domain's compute_dt reduction from its current state
+  ili = ihl = 0;
+  for (int d = 0; d < L->ndom; d++) {
+    if (scheme[d] == 0) {
+      const rb_li_fields& f = li[ili++];
+      RB_CUDA(rb::reduce_max_h(f.h[cur[d]], (size_t)f.ny * f.nx, &clocks[d].red_key, s), "ens seed");
+    } else {
+      const rb_hllc_fields& f = hl[ihl++];
+      RB_CUDA(rb::reduce_wavespeed(f.h[cur[d]], f.hu[cur[d]], f.hv[cur[d]], (size_t)f.ny * f.nx, &clocks[d].red_key, s),
+              "ens seed");
+    }
+  }
+  RB_CUDA(cudaStreamSynchronize(s), "rb_ensemble_init sync");  // host vectors are the copy sources
+  return RB_OK;
+}
+
+int rb_ensemble_set_targets(const rb_ensemble_layout* L, void* ens, const double* t_target, const int32_t* max_steps,
+                            void* stream) {
+  if (!L || !ens || !t_target || !max_steps) return fail(RB_ERR_ARG, "rb_ensemble_set_targets: null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  char* base = (char*)ens;
+  double* dt_t = (double*)(base + L->off_targets);
+  int* dm = (int*)(base + L->off_targets + (int64_t)L->ndom * (int64_t)sizeof(double));
+  RB_CUDA(cudaMemcpyAsync(dt_t, t_target, (size_t)L->ndom * sizeof(double), cudaMemcpyHostToDevice, s), "targets");
+  RB_CUDA(cudaMemcpyAsync(dm, max_steps, (size_t)L->ndom * sizeof(int32_t), cudaMemcpyHostToDevice, s), "targets");
+  RB_CUDA(rb::clock_target_many_launch((rb::DevClock*)(base + L->off_clocks), L->ndom, dt_t, dm, s), "targets");
+  RB_CUDA(cudaStreamSynchronize(s), "rb_ensemble_set_targets sync");
+  return RB_OK;
+}
+
+int rb_ensemble_enqueue(const rb_ensemble_layout* L, void* ens, int32_t nsteps, void* stream) {
+  if (!L || !ens || nsteps < 0) return fail(RB_ERR_ARG, "rb_ensemble_enqueue: bad argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  char* base = (char*)ens;
+  rb::DevClock* clocks = (rb::DevClock*)(base + L->off_clocks);
+  const rb::LiParams* P = (const rb::LiParams*)(base + L->off_li);
+  const rb::HllcParams* Q = (const rb::HllcParams*)(base + L->off_hllc);
+  const int2* mli = (const int2*)(base + L->off_map_li);
+  const int2* mhl = (const int2*)(base + L->off_map_hllc);
+  for (int k = 0; k < nsteps; k++) {
+    RB_CUDA(rb::clock_plan_many_launch(clocks, L->ndom, s), "ens plan");
+    RB_CUDA(rb::ens_li_launch(L->li_variant, L->li_grid, P, mli, L->li_tiles, s), "ens li");
+    RB_CUDA(rb::ens_hllc_launch(L->hllc_variant, L->hllc_grid, 1, Q, mhl, L->hllc_tiles, s), "ens hllc 1");
+    RB_CUDA(rb::ens_hllc_launch(L->hllc_variant, L->hllc_grid, 2, Q, mhl, L->hllc_tiles, s), "ens hllc 2");
+  }
+  return RB_OK;
+}
+
+int rb_ensemble_read(const rb_ensemble_layout* L, void* ens, rb_clock_state* out, void* stream) {
+  if (!L || !ens || !out) return fail(RB_ERR_ARG, "rb_ensemble_read: null argument");
+  cudaStream_t s = (cudaStream_t)stream;
+  rb::DevClock* clocks = (rb::DevClock*)((char*)ens + L->off_clocks);
+  RB_CUDA(rb::clock_commit_many_launch(clocks, L->ndom, s), "ens commit");
+  std::vector<rb::DevClock> hc(L->ndom);
+  RB_CUDA(cudaMemcpyAsync(hc.data(), clocks, hc.size() * sizeof(rb::DevClock), cudaMemcpyDeviceToHost, s), "ens read");
+  RB_CUDA(cudaStreamSynchronize(s), "rb_ensemble_read sync");
+  for (int d = 0; d < L->ndom; d++) {
+    out[d].t = hc[d].t;
+    out[d].dt = hc[d].dt;
+    out[d].rain_volume = hc[d].rain_in[0];
+    out[d].inflow_volume = hc[d].inflow_in[0];
+    out[d].cur = hc[d].cur;
+    out[d].steps = hc[d].steps;
+    out[d].err = hc[d].err;
+    out[d].reserved = 0;
+  }
   return RB_OK;
 }
 

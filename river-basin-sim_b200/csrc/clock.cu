@@ -75,7 +75,7 @@ __device__ __forceinline__ void commit(DevClock* c) {
   }
 }
 
-__global__ void clock_plan_kernel(DevClock* c) {
+__device__ void clock_plan(DevClock* c) {
   commit(c);
   c->active = 0;
   const double t = c->t;
@@ -137,6 +137,49 @@ __global__ void clock_plan_kernel(DevClock* c) {
   c->red_key = 0u;  // the step kernel folds max(h) / max wave speed of its output here
   c->active = 1;
   c->pending = 1;
+}
+
+__global__ void clock_plan_kernel(DevClock* c) { clock_plan(c); }
+
+// One plan per domain of an ensemble (each domain has its own clock).
+__global__ void clock_plan_many_kernel(DevClock* clocks, int n) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < n) clock_plan(&clocks[d]);
+}
+
+__global__ void clock_commit_many_kernel(DevClock* clocks, int n) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < n) {
+    commit(&clocks[d]);
+    clocks[d].active = 0;
+  }
+}
+
+__global__ void clock_target_many_kernel(DevClock* clocks, int n, const double* t_target, const int* max_steps) {
+  const int d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d < n) {
+    DevClock* c = &clocks[d];
+    commit(c);
+    c->active = 0;
+    c->t_target = t_target[d];
+    c->max_steps = c->steps + max_steps[d];
+  }
+}
+
+cudaError_t clock_plan_many_launch(DevClock* clocks, int n, cudaStream_t s) {
+  clock_plan_many_kernel<<<(n + 127) / 128, 128, 0, s>>>(clocks, n);
+  return cudaGetLastError();
+}
+
+cudaError_t clock_commit_many_launch(DevClock* clocks, int n, cudaStream_t s) {
+  clock_commit_many_kernel<<<(n + 127) / 128, 128, 0, s>>>(clocks, n);
+  return cudaGetLastError();
+}
+
+cudaError_t clock_target_many_launch(DevClock* clocks, int n, const double* t_target, const int* max_steps,
+                                     cudaStream_t s) {
+  clock_target_many_kernel<<<(n + 127) / 128, 128, 0, s>>>(clocks, n, t_target, max_steps);
+  return cudaGetLastError();
 }
 
 __global__ void clock_commit_kernel(DevClock* c) {

@@ -125,23 +125,48 @@ __device__ __forceinline__ void muscl_face(const Cell& c0, const Cell& c1, const
   fmt = f2;
 }
 
+template <int TX, int TY>
+struct HllcSmem {
+  static constexpr int H = 3;                     // halo
+  static constexpr int RW = TX + 2 * H, RH = TY + 2 * H;
+  static constexpr int XW = TX + 3, XH = TY + 2;  // x-face mass flux: cols x0-1..x0+TX+1, rows y0-1..y0+TY
+  static constexpr int YW = TX + 2, YH = TY + 3;  // y-face mass flux: cols x0-1..x0+TX,   rows y0-1..y0+TY+1
+  static constexpr int BW = TX + 2, BH = TY + 2;  // beta on the tile + ring
+  float h[RH][RW], u[RH][RW], v[RH][RW], z[RH][RW];
+  float fxh[XH][XW], fyh[YH][YW];
+  float fxl[TY][TX + 1], fxr[TY][TX + 1], fxt[TY][TX + 1];  // tile x-faces
+  float fyl[TY + 1][TX], fyr[TY + 1][TX], fyt[TY + 1][TX];  // tile y-faces
+  float beta[BH][BW];
+  double red[8];
+  float redf[8];
+};
+
+// One Heun stage of tile (bx, by) of domain p; ledger slot `slot`. Called by every
+// thread of the block; returns uniformly.
 template <int TX, int TY, int NT, int STAGE>
-__global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
-  constexpr int H = 3;                      // halo
-  constexpr int RW = TX + 2 * H, RH = TY + 2 * H;
-  constexpr int XW = TX + 3, XH = TY + 2;   // x-face mass flux: cols x0-1..x0+TX+1, rows y0-1..y0+TY
-  constexpr int YW = TX + 2, YH = TY + 3;   // y-face mass flux: cols x0-1..x0+TX,   rows y0-1..y0+TY+1
-  constexpr int BW = TX + 2, BH = TY + 2;   // beta on the tile + ring
-  __shared__ float s_h[RH][RW], s_u[RH][RW], s_v[RH][RW], s_z[RH][RW];
-  __shared__ float s_fxh[XH][XW], s_fyh[YH][YW];
-  __shared__ float s_fxl[TY][TX + 1], s_fxr[TY][TX + 1], s_fxt[TY][TX + 1];  // tile x-faces
-  __shared__ float s_fyl[TY + 1][TX], s_fyr[TY + 1][TX], s_fyt[TY + 1][TX];  // tile y-faces
-  __shared__ float s_beta[BH][BW];
-  __shared__ double s_red[NT / 32];
-  __shared__ float s_redf[NT / 32];
+__device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, size_t slot, HllcSmem<TX, TY>& S) {
+  static_assert(NT / 32 <= 8, "reduction scratch sized for <= 8 warps");
+  using SM = HllcSmem<TX, TY>;
+  constexpr int H = SM::H, RW = SM::RW, RH = SM::RH, XW = SM::XW, XH = SM::XH, YW = SM::YW, YH = SM::YH;
+  constexpr int BW = SM::BW, BH = SM::BH;
+  auto& s_h = S.h;
+  auto& s_u = S.u;
+  auto& s_v = S.v;
+  auto& s_z = S.z;
+  auto& s_fxh = S.fxh;
+  auto& s_fyh = S.fyh;
+  auto& s_fxl = S.fxl;
+  auto& s_fxr = S.fxr;
+  auto& s_fxt = S.fxt;
+  auto& s_fyl = S.fyl;
+  auto& s_fyr = S.fyr;
+  auto& s_fyt = S.fyt;
+  auto& s_beta = S.beta;
+  double* s_red = S.red;
+  float* s_redf = S.redf;
 
   const int ny = p.ny, nx = p.nx;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int x0 = bx * TX, y0 = by * TY;
   int cur = p.cur, rain_mode = p.rain_mode;
   float dt = p.dt32, rain32 = p.rain32, scale32 = p.scale32;
   float stage_w = p.stage[RB_EDGE_WEST], stage_e = p.stage[RB_EDGE_EAST];
@@ -433,12 +458,19 @@ __global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
 
   if (p.ledger != nullptr) {
     const double s = block_sum<NT>(loss, s_red);
-    if (threadIdx.x == 0) ledger_add(p.ledger + 2 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x), s);
+    if (threadIdx.x == 0) ledger_add(p.ledger + 2 * slot, s);
   }
   if (STAGE == 2) {
     if (p.smax_key != nullptr) block_max_to<NT>(smax, p.smax_key, s_redf);
     if (bad) flag_error(p.err, RB_DEVERR_NONFINITE);
   }
+  __syncthreads();  // the shared tile is reused by the caller's next tile
+}
+
+template <int TX, int TY, int NT, int STAGE>
+__global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
+  __shared__ HllcSmem<TX, TY> S;
+  hllc_tile<TX, TY, NT, STAGE>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
 
 template <int TX, int TY, int NT>
@@ -456,5 +488,54 @@ cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s) {
 }
 
 int hllc_tiles(int ny, int nx) { return ((nx + HLLC_TX - 1) / HLLC_TX) * ((ny + HLLC_TY - 1) / HLLC_TY); }
+
+// Ensemble: one Heun stage over the (domain, local tile) work-list of every HLLC
+// domain (stage 2 of any domain starts only after stage 1 of all of them, as the
+// single-domain step requires for its own tiles).
+template <int TX, int TY, int NT, int STAGE>
+__global__ void __launch_bounds__(NT) ens_hllc_kernel(const HllcParams* __restrict__ P, const int2* __restrict__ map,
+                                                       long long total) {
+  __shared__ HllcSmem<TX, TY> S;
+  for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+    const int2 m = map[t];
+    const HllcParams& p = P[m.x];
+    const int tiles_x = (p.nx + TX - 1) / TX;
+    hllc_tile<TX, TY, NT, STAGE>(p, m.y % tiles_x, m.y / tiles_x, (size_t)m.y, S);
+  }
+}
+
+template <int TX, int TY, int NT>
+static int ens_hllc_grid() {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_hllc_kernel<TX, TY, NT, 2>, NT, 0);
+  return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+}
+
+void hllc_variant_tile(int variant, int* tx, int* ty) {
+  *tx = 32;
+  *ty = variant == 1 ? 8 : 16;
+}
+
+int ens_hllc_grid_size(int variant) { return variant == 1 ? ens_hllc_grid<32, 8, 256>() : ens_hllc_grid<32, 16, 256>(); }
+
+cudaError_t ens_hllc_launch(int variant, int grid, int stage, const HllcParams* P, const int2* map, long long total,
+                            cudaStream_t s) {
+  if (total <= 0) return cudaSuccess;
+  const int g = (int)(total < grid ? total : grid);
+  if (variant == 1) {
+    if (stage == 1)
+      ens_hllc_kernel<32, 8, 256, 1><<<g, 256, 0, s>>>(P, map, total);
+    else
+      ens_hllc_kernel<32, 8, 256, 2><<<g, 256, 0, s>>>(P, map, total);
+  } else {
+    if (stage == 1)
+      ens_hllc_kernel<32, 16, 256, 1><<<g, 256, 0, s>>>(P, map, total);
+    else
+      ens_hllc_kernel<32, 16, 256, 2><<<g, 256, 0, s>>>(P, map, total);
+  }
+  return cudaGetLastError();
+}
 
 }  // namespace rb

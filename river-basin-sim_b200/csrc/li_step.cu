@@ -54,19 +54,38 @@ __device__ __forceinline__ float drain(float h_edge, float q_out, float dxdt) {
   return h_edge - removed;
 }
 
+template <int TX, int TY>
+struct LiSmem {
+  static constexpr int RW = TX + 4, RH = TY + 4;  // cells: cols x0-2 .. x0+TX+1, rows y0-2 .. y0+TY+1
+  static constexpr int XW = TX + 3, XH = TY + 2;  // x-faces: cols x0-1 .. x0+TX+1, rows y0-1 .. y0+TY
+  static constexpr int YW = TX + 2, YH = TY + 3;  // y-faces: cols x0-1 .. x0+TX,   rows y0-1 .. y0+TY+1
+  static constexpr int BW = TX + 2, BH = TY + 2;  // beta:    cols x0-1 .. x0+TX,   rows y0-1 .. y0+TY
+  float h[RH][RW], z[RH][RW], n[RH][RW], eta[RH][RW];
+  float qx[XH][XW], qy[YH][YW], beta[BH][BW];
+  double red[8];
+  float redf[8];
+};
+
+// One CTA-wide tile of the step: tile (bx, by) of domain p, ledger slot `slot`.
+// Called by every thread of the block; returns uniformly.
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
-  constexpr int RW = TX + 4, RH = TY + 4;  // cells: cols x0-2 .. x0+TX+1, rows y0-2 .. y0+TY+1
-  constexpr int XW = TX + 3, XH = TY + 2;  // x-faces: cols x0-1 .. x0+TX+1, rows y0-1 .. y0+TY
-  constexpr int YW = TX + 2, YH = TY + 3;  // y-faces: cols x0-1 .. x0+TX,   rows y0-1 .. y0+TY+1
-  constexpr int BW = TX + 2, BH = TY + 2;  // beta:    cols x0-1 .. x0+TX,   rows y0-1 .. y0+TY
-  __shared__ float s_h[RH][RW], s_z[RH][RW], s_n[RH][RW], s_eta[RH][RW];
-  __shared__ float s_qx[XH][XW], s_qy[YH][YW], s_beta[BH][BW];
-  __shared__ double s_red[NT / 32];
-  __shared__ float s_redf[NT / 32];
+__device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_t slot, LiSmem<TX, TY>& S) {
+  static_assert(NT / 32 <= 8, "reduction scratch sized for <= 8 warps");
+  using SM = LiSmem<TX, TY>;
+  constexpr int RW = SM::RW, RH = SM::RH, XW = SM::XW, XH = SM::XH, YW = SM::YW, YH = SM::YH;
+  constexpr int BW = SM::BW, BH = SM::BH;
+  auto& s_h = S.h;
+  auto& s_z = S.z;
+  auto& s_n = S.n;
+  auto& s_eta = S.eta;
+  auto& s_qx = S.qx;
+  auto& s_qy = S.qy;
+  auto& s_beta = S.beta;
+  double* s_red = S.red;
+  float* s_redf = S.redf;
 
   const int ny = p.ny, nx = p.nx;
-  const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+  const int x0 = bx * TX, y0 = by * TY;
   int cur = p.cur, limit = p.limit;
   float dt = p.dt32, rain_cont = p.rain_cont, rain32 = p.rain32, scale32 = p.scale32, dxdt = p.dxdt;
   if (p.clk != nullptr) {  // device-resident clock: this step's dt and forcing
@@ -292,10 +311,17 @@ __global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
 
   if (p.ledger != nullptr) {
     const double s = block_sum<NT>(loss, s_red);
-    if (threadIdx.x == 0) ledger_add(p.ledger + 2 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x), s);
+    if (threadIdx.x == 0) ledger_add(p.ledger + 2 * slot, s);
   }
   if (p.hmax_key != nullptr) block_max_to<NT>(hmax, p.hmax_key, s_redf);
   if (bad) flag_error(p.err, RB_DEVERR_NONFINITE);
+  __syncthreads();  // the shared tile is reused by the caller's next tile
+}
+
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
+  __shared__ LiSmem<TX, TY> S;
+  li_tile<TX, TY, NT>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
 
 template <int TX, int TY, int NT>
@@ -310,5 +336,56 @@ cudaError_t li_step_launch(const LiParams& p, cudaStream_t s) {
 }
 
 int li_tiles(int ny, int nx) { return ((nx + LI_TX - 1) / LI_TX) * ((ny + LI_TY - 1) / LI_TY); }
+
+// Ensemble: a persistent grid walks the (domain, local tile) work-list of every
+// local-inertial domain; a tile of a domain whose clock is not active returns at
+// its first instruction. Each domain's tiles, ledger slots and clock are its own,
+// so a domain's result does not depend on what else is in the batch.
+template <int TX, int TY, int NT>
+__global__ void __launch_bounds__(NT) ens_li_kernel(const LiParams* __restrict__ P, const int2* __restrict__ map,
+                                                     long long total) {
+  __shared__ LiSmem<TX, TY> S;
+  for (long long t = blockIdx.x; t < total; t += gridDim.x) {
+    const int2 m = map[t];
+    const LiParams& p = P[m.x];
+    const int tiles_x = (p.nx + TX - 1) / TX;
+    li_tile<TX, TY, NT>(p, m.y % tiles_x, m.y / tiles_x, (size_t)m.y, S);
+  }
+}
+
+template <int TX, int TY, int NT>
+static int ens_li_grid() {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_li_kernel<TX, TY, NT>, NT, 0);
+  return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+}
+
+void li_variant_tile(int variant, int* tx, int* ty) {
+  static const int T[3][2] = {{32, 16}, {32, 8}, {64, 8}};
+  const int v = variant < 0 || variant > 2 ? 0 : variant;
+  *tx = T[v][0];
+  *ty = T[v][1];
+}
+
+int ens_li_grid_size(int variant) {
+  switch (variant) {
+    case 1: return ens_li_grid<32, 8, 256>();
+    case 2: return ens_li_grid<64, 8, 256>();
+    default: return ens_li_grid<32, 16, 256>();
+  }
+}
+
+cudaError_t ens_li_launch(int variant, int grid, const LiParams* P, const int2* map, long long total, cudaStream_t s) {
+  if (total <= 0) return cudaSuccess;
+  const int g = (int)(total < grid ? total : grid);
+  switch (variant) {
+    case 1: ens_li_kernel<32, 8, 256><<<g, 256, 0, s>>>(P, map, total); break;
+    case 2: ens_li_kernel<64, 8, 256><<<g, 256, 0, s>>>(P, map, total); break;
+    default: ens_li_kernel<32, 16, 256><<<g, 256, 0, s>>>(P, map, total); break;
+  }
+  return cudaGetLastError();
+}
 
 }  // namespace rb

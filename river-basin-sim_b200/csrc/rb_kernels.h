@@ -100,8 +100,20 @@ cudaError_t clock_plan_launch(DevClock* clk, cudaStream_t s);
 cudaError_t clock_commit_launch(DevClock* clk, cudaStream_t s);
 cudaError_t clock_target_launch(DevClock* clk, double t_target, int max_steps, cudaStream_t s);
 cudaError_t clock_inflow_launch(DevClock* clk, float* const* hb, cudaStream_t s);
+cudaError_t clock_plan_many_launch(DevClock* clocks, int n, cudaStream_t s);
+cudaError_t clock_commit_many_launch(DevClock* clocks, int n, cudaStream_t s);
+cudaError_t clock_target_many_launch(DevClock* clocks, int n, const double* t_target, const int* max_steps,
+                                     cudaStream_t s);
 cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s);
 int li_tiles(int ny, int nx);
+void li_variant_tile(int variant, int* tx, int* ty);
+void hllc_variant_tile(int variant, int* tx, int* ty);
+int ens_li_grid_size(int variant);
+int ens_hllc_grid_size(int variant);
+cudaError_t ens_li_launch(int variant, int grid, const LiParams* P, const int2* map, long long total, cudaStream_t s);
+cudaError_t ens_hllc_launch(int variant, int grid, int stage, const HllcParams* P, const int2* map, long long total,
+                            cudaStream_t s);
+void set_last_error(const char* msg);  // the message rb_last_error returns on this thread
 int hllc_tiles(int ny, int nx);
 
 // Workspace layout (byte offsets from the workspace base).

@@ -72,6 +72,17 @@ class ClockState(ctypes.Structure):
     ]  # fmt: skip
 
 
+class EnsembleLayout(ctypes.Structure):
+    _fields_ = [
+        ("ndom", ctypes.c_int32), ("n_li", ctypes.c_int32), ("n_hllc", ctypes.c_int32),
+        ("li_variant", ctypes.c_int32), ("hllc_variant", ctypes.c_int32), ("li_grid", ctypes.c_int32),
+        ("hllc_grid", ctypes.c_int32), ("reserved", ctypes.c_int32), ("li_tiles", ctypes.c_int64),
+        ("hllc_tiles", ctypes.c_int64), ("off_clocks", ctypes.c_int64), ("off_li", ctypes.c_int64),
+        ("off_hllc", ctypes.c_int64), ("off_map_li", ctypes.c_int64), ("off_map_hllc", ctypes.c_int64),
+        ("off_targets", ctypes.c_int64), ("bytes", ctypes.c_int64),
+    ]  # fmt: skip
+
+
 # name -> (restype, argtypes) for every exported entry point of include/rbsim.h
 SIGNATURES = {
     "rb_li_workspace_bytes": (ctypes.c_size_t, [ctypes.c_int32, ctypes.c_int32]),
@@ -103,6 +114,12 @@ SIGNATURES = {
     "rb_li_enqueue_steps": (ctypes.c_int, [ctypes.POINTER(LiFields), ctypes.c_int32, ctypes.c_int32, _P, _P]),
     "rb_hllc_enqueue_steps": (ctypes.c_int, [ctypes.POINTER(HllcFields), ctypes.c_int32, ctypes.c_int32, _P, _P]),
     "rb_clock_read": (ctypes.c_int, [_P, _P, ctypes.POINTER(ClockState)]),
+    "rb_ensemble_layout_make": (ctypes.c_int, [ctypes.c_int32, _P, _P, _P, ctypes.c_int32, ctypes.c_int32,
+                                               ctypes.POINTER(EnsembleLayout)]),
+    "rb_ensemble_init": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, _P, _P, _P, _P, _P, _P, _P]),
+    "rb_ensemble_set_targets": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, _P, _P, _P]),
+    "rb_ensemble_enqueue": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, ctypes.c_int32, _P]),
+    "rb_ensemble_read": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, _P, _P]),
     "rb_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
     "rb_version": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)] * 3),
 }  # fmt: skip

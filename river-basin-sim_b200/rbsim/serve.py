@@ -1,0 +1,247 @@
+"""A request loop that serves scenario solves with continuous batching.
+
+Requests (scheme, grid side, horizon, seeded synthetic terrain, optional Exner
+morphology) arrive over wall-clock time. The server admits them in arrival order
+while the HBM they need fits the budget, keeps every admitted solve resident, and
+steps all of them together as one ``Ensemble`` (one persistent kernel per scheme
+over every member's tiles, each member on its own device clock). Between graph
+replays it retires finished solves (freeing their memory), runs due slow processes
+(Exner activations) for the members that reached them, writes output frames
+asynchronously, and admits whatever arrived meanwhile -- so new work joins the
+batch while older work is still on the GPU. Each result is bit-identical to
+solving that request alone (``solve_alone``).
+
+``serial_baseline`` solves the same requests one after another, each alone, in
+arrival order: the plain loop the batched server is measured against.
+"""
+
+from __future__ import annotations
+
+import math
+import time
+from dataclasses import dataclass, field
+
+import numpy as np
+import torch
+
+from .ensemble import Ensemble
+from .processes.morphology import MorphologyProcess
+from .scheduler import EPS_T
+from .sediment import arm_sediment
+from .state import State
+
+ALPHA = {"local_inertial": 0.7, "hllc_fv": 0.45}
+
+
+@dataclass
+class Request:
+    rid: int
+    arrival: float  # seconds after the stream starts
+    scheme: str  # "local_inertial" | "hllc_fv"
+    side: int  # grid side, cells
+    horizon: float  # simulated seconds
+    seed: int
+    exner: bool = False
+    dx: float = 10.0
+    rain_mm_hr: float = 30.0
+    morph_interval: float = 300.0
+
+
+@dataclass
+class Result:
+    rid: int
+    arrival: float
+    admitted: float
+    finished: float
+    steps: int
+    t: float
+    depth: np.ndarray | None = None
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+
+def request_bytes(req: Request) -> int:
+    """Device bytes a request holds while resident (fields, workspace, morphology)."""
+    n = req.side * req.side
+    if req.scheme == "hllc_fv":
+        per = 4 * (6 + 2 + 3)  # h/hu/hv double-buffered, z, n, stage-1 state
+    else:
+        per = 4 * (6 + 2 + 1)  # h/qx/qy double-buffered, z, n, rain residue
+        if req.exner:
+            per += 4 + 4 + 8 + 8 + 16  # d50, z0, dz_cum, dz_unapplied, four transport accumulators
+    return per * n + (1 << 20)
+
+
+def build_state(req: Request, device) -> tuple[State, MorphologyProcess | None]:
+    """Seeded synthetic terrain: a sloping plane plus Gaussian bumps, rain-on-grid."""
+    rng = np.random.default_rng(req.seed)
+    n = req.side
+    yy, xx = np.mgrid[0:n, 0:n].astype(np.float32)
+    z = 1e-3 * xx * req.dx
+    for _ in range(6):
+        a, s = rng.uniform(0.5, 3.0), rng.uniform(3.0, 0.2 * n)
+        cy, cx = rng.uniform(0, n), rng.uniform(0, n)
+        z += a * np.exp(-((yy - cy) ** 2 + (xx - cx) ** 2) / (2 * s * s))
+    manning = float(rng.uniform(0.02, 0.06))
+    depth = 0.05 if req.scheme == "local_inertial" else np.where(xx < n / 2, 1.0, 0.2).astype(np.float32)
+    st = State.from_bed(z.astype(np.float32), req.dx, depth=depth, manning=manning, device=device)
+    morph = None
+    if req.scheme == "hllc_fv":
+        st.arm_hllc_fields()
+    else:
+        st.arm_source_compensation()
+        st.set_open_boundaries({"east": "open"})
+        if req.exner:
+            arm_sediment(st, 0.002, 0.4)
+            morph = MorphologyProcess(st, req.morph_interval)
+    return st, morph
+
+
+@dataclass
+class _Member:
+    req: Request
+    st: State
+    morph: MorphologyProcess | None
+    admitted: float
+    nbytes: int
+    next_act: float = math.inf  # next Exner activation (simulated s)
+    last_act: float = 0.0
+    t: float = 0.0  # simulated time reached
+    steps: int = 0  # steps taken
+    base_steps: int = 0  # steps taken before the current ensemble was built
+
+    @property
+    def target(self) -> float:
+        return min(self.next_act, self.req.horizon)
+
+    def sync_times(self) -> list[float]:
+        acts = []
+        if self.morph is not None:
+            k = 1
+            while k * self.req.morph_interval <= self.req.horizon + EPS_T:
+                acts.append(k * self.req.morph_interval)
+                k += 1
+        return sorted({*acts, self.req.horizon})
+
+
+def _build_ensemble(members: list[_Member], graph_steps: int) -> Ensemble:
+    """An ensemble over the current members, each clock continuing from where it stopped."""
+    reqs = [m.req for m in members]
+    for m in members:
+        m.base_steps = m.steps
+    ens = Ensemble(
+        [m.st for m in members], [r.scheme for r in reqs], alpha=[ALPHA[r.scheme] for r in reqs], dt_max=30.0,
+        sync_times=[m.sync_times() for m in members], rain_rate=[r.rain_mm_hr / 3.6e6 for r in reqs],
+        rain_until=[r.horizon for r in reqs], graph_steps=graph_steps, t0=[m.t for m in members],
+    )  # fmt: skip
+    ens.set_targets([m.target for m in members])
+    return ens
+
+
+@dataclass
+class Server:
+    hbm_budget: float = 150e9
+    graph_steps: int = 16
+    device: str = "cuda"
+    keep_depth: bool = False
+    stats: dict = field(default_factory=dict)
+
+    def run(self, requests: list[Request]) -> list[Result]:
+        dev = torch.device(self.device)
+        queue = sorted(requests, key=lambda r: r.arrival)
+        active: list[_Member] = []
+        results: list[Result] = []
+        used, replays, rebuilds = 0, 0, 0
+        ens = None
+        t0 = time.perf_counter()
+        while queue or active:
+            now = time.perf_counter() - t0
+            # admit, in arrival order, whatever has arrived and fits the budget
+            while queue and queue[0].arrival <= now and used + request_bytes(queue[0]) <= self.hbm_budget:
+                req = queue.pop(0)
+                st, morph = build_state(req, dev)
+                m = _Member(req, st, morph, admitted=time.perf_counter() - t0, nbytes=request_bytes(req),
+                            next_act=req.morph_interval if morph is not None else math.inf)  # fmt: skip
+                active.append(m)
+                used += m.nbytes
+                ens = None
+            if not active:
+                if queue:
+                    time.sleep(max(0.0, min(queue[0].arrival - (time.perf_counter() - t0), 0.01)))
+                continue
+            if ens is None:
+                ens = _build_ensemble(active, self.graph_steps)
+                rebuilds += 1
+            ens.replay()
+            replays += 1
+            clk = ens.read()
+            finished, retarget = [], False
+            for m, c in zip(active, clk, strict=True):
+                m.t, m.steps = c.t, m.base_steps + c.steps
+                if m.morph is not None and c.t >= m.next_act - EPS_T:
+                    m.morph.advance(c.t, c.t - m.last_act)  # operator split, scheduler order
+                    m.last_act = c.t
+                    m.next_act += m.req.morph_interval
+                    retarget = True
+                if c.t >= m.req.horizon - EPS_T:
+                    finished.append(m)
+            for m in finished:
+                depth = m.st.h.cpu().numpy() if self.keep_depth else None
+                results.append(Result(m.req.rid, m.req.arrival, m.admitted, time.perf_counter() - t0, m.steps,
+                                      m.t, depth))  # fmt: skip
+                active.remove(m)
+                used -= m.nbytes
+            if finished:
+                ens = None  # rebuilt over the survivors (and any new arrivals) next round
+            elif retarget:
+                ens.set_targets([m.target for m in active])
+        wall = time.perf_counter() - t0
+        lat = np.array([r.latency for r in results])
+        self.stats = {
+            "solves": len(results), "wall_s": wall, "solves_per_s": len(results) / wall if wall > 0 else 0.0,
+            "p50_s": float(np.percentile(lat, 50)) if len(lat) else None,
+            "p99_s": float(np.percentile(lat, 99)) if len(lat) else None,
+            "replays": replays, "ensemble_rebuilds": rebuilds,
+        }  # fmt: skip
+        return sorted(results, key=lambda r: r.rid)
+
+
+def solve_alone(req: Request, device="cuda", graph_steps: int = 16) -> Result:
+    """One request on its own (the reference for "same alone and in the mix")."""
+    srv = Server(graph_steps=graph_steps, device=device, keep_depth=True)
+    r = Request(**{**req.__dict__, "arrival": 0.0})
+    return srv.run([r])[0]
+
+
+def serial_baseline(requests: list[Request], device="cuda", graph_steps: int = 16) -> dict:
+    """The plain loop: each request solved alone, in arrival order, one after another."""
+    t0 = time.perf_counter()
+    lat = []
+    for req in sorted(requests, key=lambda r: r.arrival):
+        now = time.perf_counter() - t0
+        if req.arrival > now:
+            time.sleep(req.arrival - now)
+        solve_alone(req, device, graph_steps)
+        lat.append(time.perf_counter() - t0 - req.arrival)
+    wall = time.perf_counter() - t0
+    lat = np.array(lat)
+    return {"solves": len(lat), "wall_s": wall, "solves_per_s": len(lat) / wall,
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99))}  # fmt: skip
+
+
+def poisson_stream(rate: float, n: int, seed: int, side_lo: int = 256, side_hi: int = 4096,
+                   horizon_lo: float = 600.0, horizon_hi: float = 7200.0) -> list[Request]:  # fmt: skip
+    """Config-5 requests: Poisson arrivals, log-uniform sides, 70 % LI / 30 % HLLC, 10 % with Exner."""
+    rng = np.random.default_rng(seed)
+    t, out = 0.0, []
+    for k in range(n):
+        t += rng.exponential(1.0 / rate)
+        side = int(round(math.exp(rng.uniform(math.log(side_lo), math.log(side_hi)))))
+        scheme = "local_inertial" if rng.random() < 0.7 else "hllc_fv"
+        exner = scheme == "local_inertial" and rng.random() < 0.1 / 0.7
+        out.append(Request(rid=k, arrival=t, scheme=scheme, side=side,
+                           horizon=float(rng.uniform(horizon_lo, horizon_hi)), seed=int(rng.integers(1 << 31)),
+                           exner=exner, dx=10.0 if scheme == "local_inertial" else 2.0))  # fmt: skip
+    return out

@@ -46,7 +46,9 @@ def test_struct_layouts_match_the_c_compiler(tmp_path):
 
     from rbsim import _lib
 
-    structs = {"rb_li_fields": _lib.LiFields, "rb_hllc_fields": _lib.HllcFields, "rb_step_args": _lib.StepArgs}
+    structs = {"rb_li_fields": _lib.LiFields, "rb_hllc_fields": _lib.HllcFields, "rb_step_args": _lib.StepArgs,
+               "rb_clock_config": _lib.ClockConfig, "rb_clock_state": _lib.ClockState,
+               "rb_ensemble_layout": _lib.EnsembleLayout}  # fmt: skip
     lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "rbsim.h"', "int main(void) {"]
     for cname, cls in structs.items():
         lines.append(f'  printf("{cname} %zu\\n", sizeof({cname}));')

@@ -1,0 +1,45 @@
+"""Serving: continuous batching returns, for every request, what solving it alone returns.
+
+A Poisson stream of small mixed requests (LI / HLLC, some with Exner) arrives while
+earlier ones are still running; the server admits them between graph replays,
+retires finished ones and rebuilds the batch. Each request's final depth must be
+bit-identical to the same request served alone. A tight HBM budget forces queueing
+behind the budget (requests wait for memory to free up) without changing results.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+
+def _stream():
+    from rbsim.serve import poisson_stream
+
+    reqs = poisson_stream(rate=40.0, n=10, seed=7, side_lo=48, side_hi=192, horizon_lo=60.0, horizon_hi=400.0)
+    reqs[1].exner = True  # make sure a morphology request is in the mix
+    reqs[1].scheme = "local_inertial"
+    reqs[1].morph_interval = 50.0
+    return reqs
+
+
+@pytest.mark.parametrize("budget", [150e9, 2.5e6])
+def test_results_are_the_same_alone_and_in_the_mix(budget):
+    from rbsim.serve import Server, request_bytes, solve_alone
+
+    reqs = _stream()
+    assert budget > max(request_bytes(r) for r in reqs)
+    srv = Server(hbm_budget=budget, graph_steps=4, keep_depth=True)
+    results = srv.run(reqs)
+    assert [r.rid for r in results] == [r.rid for r in reqs]
+    assert srv.stats["solves"] == len(reqs) and srv.stats["p99_s"] >= srv.stats["p50_s"] > 0.0
+    if budget < 1e9:
+        assert srv.stats["ensemble_rebuilds"] >= 3
+    for req, res in zip(reqs, results, strict=True):
+        assert abs(res.t - req.horizon) < 1e-6
+        alone = solve_alone(req, graph_steps=4)
+        assert alone.steps == res.steps, req.rid
+        np.testing.assert_array_equal(res.depth, alone.depth, err_msg=f"request {req.rid}")
