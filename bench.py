@@ -193,7 +193,17 @@ def main(argv=None) -> int:
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="rbsim", choices=["rbsim", "reference"])
+    ap.add_argument("--workload", default="hllc_dambreak",
+                    choices=["hllc_dambreak", "li_rain_512", "li_reach_8192", "ensemble_256", "serve"],
+                    help="hllc_dambreak is the headline; the others measure the remaining configurations")
+    ap.add_argument("--rates", default="1,2,5,10,20,50", help="serve: arrival rates, requests/s")
+    ap.add_argument("--requests", type=int, default=48, help="serve: requests per rate")
     args = ap.parse_args(argv)
+    if args.workload != "hllc_dambreak" and args.impl == "rbsim":
+        import bench_workloads
+
+        print(json.dumps(bench_workloads.run(args)))
+        return 0
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     if args.impl == "reference":

@@ -1,0 +1,248 @@
+"""The non-headline configurations, measured for ``bench.py --workload ...``.
+
+* ``li_rain_512``: local inertial, 512 x 512, dx 10 m, sloping plane + 20 seeded
+  Gaussian bumps, n 0.03, uniform rain 50 mm/h for 3600 s (compensated), all edges
+  open, alpha 0.7, the full 3600 s through run_simulation (device clock), plus the
+  fused step kernel's roofline at the 40 B/cell-step it must move.
+* ``li_reach_8192``: local inertial, 8192 x 8192, dx 5 m: a V-shaped valley with a
+  down-valley slope and a meandering 3 m x 40 m channel, lognormal Manning
+  (median 0.035, sigma 0.3), infiltration U(0, 20) mm/h, a triangular 500 m3/s
+  hydrograph split over the 8 inlet channel cells, MPM bedload (d50 2 mm), open
+  downstream edge; the first K steps (the full 12 h is ~10^5 steps), fused step
+  roofline at 72 B/cell-step.
+* ``ensemble_256``: 256 local-inertial domains, sides log-uniform in [128, 2048],
+  each with its own rain U(10, 100) mm/h and Manning U(0.02, 0.06), to 1800 s:
+  the batched ensemble (autotuned tiles) against the plain per-domain loop
+  (``compute_dt`` + ``step`` per step, one domain after another).
+* ``serve``: Poisson request streams at each rate (sides 256-4096, horizons
+  600-7200 s, 70 % LI / 30 % HLLC, 10 % Exner, 150 GB budget): solves/s and
+  p50/p99 latency of the continuous-batching server against the serial loop.
+All inputs are synthetic and seeded.
+"""
+
+from __future__ import annotations
+
+import math
+import statistics
+import time
+
+import numpy as np
+import torch
+
+import rbsim
+from rbsim import _lib
+from rbsim.config import Scenario
+from rbsim.device_clock import DeviceClock
+from rbsim.ensemble import Ensemble, autotune, log_uniform_sides
+from rbsim.processes.inflow import Inflow, InflowInjector
+from rbsim.sediment import arm_sediment
+
+
+def _peak():
+    import bench
+
+    return bench.peaks()
+
+
+def _bumps(ny, nx, dx, rng, n, amp, sigma, slope=1e-3):
+    yy, xx = np.mgrid[0:ny, 0:nx].astype(np.float32)
+    z = slope * xx * dx
+    for _ in range(n):
+        a, s = rng.uniform(*amp), rng.uniform(*sigma)
+        cy, cx = rng.uniform(0, ny), rng.uniform(0, nx)
+        z += a * np.exp(-((yy - cy) ** 2 + (xx - cx) ** 2) * dx * dx / (2 * s * s))
+    return z.astype(np.float32)
+
+
+def _kernel_roofline(state, scheme, steps, bytes_per_cell, injector=None):
+    """Per-launch CUDA-event time of the step kernel(s) over a timed span of device-clock steps."""
+    import ctypes
+
+    L = _lib.lib()
+    clk = DeviceClock(state, scheme, alpha=0.7, dt_max=30.0, sync_times=[1e9], graph_steps=steps,
+                      injector=injector)  # fmt: skip
+    f = state.li_fields()
+    ws = state.workspace.data_ptr()
+    stream = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    clk.set_target(1e9, steps)
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for k in range(steps):
+        _lib.check(L.rb_clock_plan(ws, stream.cuda_stream))
+        if injector is not None:
+            _lib.check(L.rb_clock_inflow(state._h.bufs[0].data_ptr(), state._h.bufs[1].data_ptr(), ws,
+                                         stream.cuda_stream))  # fmt: skip
+        ev[k][0].record()
+        _lib.check(L.rb_li_step_clocked(ctypes.byref(f), ws, stream.cuda_stream))
+        ev[k][1].record()
+    stop.record()
+    torch.cuda.synchronize()
+    clk.read()
+    cells = state.grid.n_cells
+    kms = statistics.mean(a.elapsed_time(b) for a, b in ev)
+    achieved = bytes_per_cell * cells / (kms / 1e3) / 1e9
+    pk = _peak()
+    return {
+        "bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+        "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk["source"],
+        "kernel": "li_step_kernel", "kernel_ms_mean": kms, "bytes_per_cell_step": bytes_per_cell,
+        "gcell_per_s_kernel": cells / (kms / 1e3) / 1e9,
+        "gcell_per_s_step": cells * steps / (start.elapsed_time(stop) / 1e3) / 1e9,
+    }  # fmt: skip
+
+
+def li_rain_512(args):
+    from rbsim.run import run_simulation
+
+    n, dx = 512, 10.0
+    rng = np.random.default_rng(1)
+    bed = _bumps(n, n, dx, rng, 20, (0.5, 5.0), (50.0, 300.0))
+    sc = Scenario(name="li_rain_512", scheme="local_inertial", dx=dx, end_time=3600.0, output_every=600.0,
+                  alpha=0.7, dt_max=30.0, rain_mm_hr=50.0, rain_duration=3600.0, manning=0.03,
+                  boundaries={e: "open" for e in ("north", "south", "east", "west")}, bed=bed)  # fmt: skip
+    import tempfile
+
+    with tempfile.TemporaryDirectory() as tmp:
+        run_simulation(sc, None, f"{tmp}/warm.zarr", verbose=False)  # build + warm
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ledger = run_simulation(sc, None, f"{tmp}/r.zarr", verbose=False)
+        torch.cuda.synchronize()
+        wall = time.perf_counter() - t0
+    st = rbsim.State.from_bed(bed, dx, depth=0.05, manning=0.03)
+    st.arm_source_compensation()
+    st.set_open_boundaries({e: "open" for e in ("north", "south", "east", "west")})
+    roof = _kernel_roofline(st, "local_inertial", 200, 40)
+    return {"workload": "li_rain_512", "metric": "Gcell-updates/s", "full_run_wall_s": wall,
+            "mass_max_rel_error": ledger.max_rel_error, "roofline": roof}  # fmt: skip
+
+
+def reach_inputs(n=8192, dx=5.0, seed=3):
+    rng = np.random.default_rng(seed)
+    yy, xx = np.mgrid[0:n, 0:n].astype(np.float32)
+    centre = n / 2 + (400.0 / dx) * np.sin(2 * np.pi * xx * dx / 3000.0)
+    dist = np.abs(yy - centre) * dx
+    z = 0.05 * dist + 1e-3 * (n - 1 - xx) * dx
+    chan = dist <= 20.0
+    z = np.where(chan, z - 3.0, z).astype(np.float32)
+    manning = np.exp(np.log(0.035) + 0.3 * rng.standard_normal((n, n))).astype(np.float32)
+    infil = (rng.uniform(0.0, 20.0, (n, n)) / 1000.0 / 3600.0).astype(np.float32)
+    inlet_rows = np.nonzero(chan[:, 0])[0][:8]
+    hydro = [(0.0, 0.0), (7200.0, 500.0 / len(inlet_rows)), (14400.0, 0.0)]
+    inflows = [Inflow((int(r), 0), hydro) for r in inlet_rows]
+    depth = np.where(chan, 2.0, 0.05).astype(np.float32)  # a wet valley: every face path is exercised
+    return z, manning, infil, inflows, depth
+
+
+def li_reach_8192(args):
+    n, dx = 8192, 5.0
+    z, manning, infil, inflows, depth = reach_inputs(n, dx)
+    st = rbsim.State.from_bed(z, dx, depth=depth, manning=manning)
+    st.set_infiltration(infil)
+    st.set_open_boundaries({"east": "open"})
+    arm_sediment(st, 0.002, 0.4)
+    inj = InflowInjector(inflows, st.grid, st.device)
+    # warm up on the first steps of the flood so transport is active, then time
+    clk = DeviceClock(st, "local_inertial", alpha=0.7, dt_max=30.0, sync_times=[43200.0], graph_steps=20,
+                      injector=inj)  # fmt: skip
+    clk.run_until(43200.0, max_steps=20)
+    roof = _kernel_roofline(st, "local_inertial", args.steps, 72, injector=inj)
+    return {"workload": "li_reach_8192", "metric": "Gcell-updates/s", "value": roof["gcell_per_s_step"],
+            "steps": args.steps, "roofline": roof}  # fmt: skip
+
+
+def _ensemble_members(n=256, seed=5):
+    rng = np.random.default_rng(seed)
+    sides = log_uniform_sides(n, 128, 2048, seed)
+    out = []
+    for k, side in enumerate(sides):
+        bed = _bumps(side, side, 10.0, np.random.default_rng(1000 + k), 8, (0.5, 3.0), (30.0, 0.15 * side * 10.0))
+        out.append((bed, float(rng.uniform(10.0, 100.0)) / 3.6e6, float(rng.uniform(0.02, 0.06))))
+    return out
+
+
+def ensemble_256(args):
+    horizon = 1800.0
+    spec = _ensemble_members()
+    cells = sum(b.size for b, _, _ in spec)
+
+    def fresh():
+        sts = []
+        for bed, _, n_ in spec:
+            st = rbsim.State.from_bed(bed, 10.0, depth=0.0, manning=n_)
+            st.arm_source_compensation()
+            sts.append(st)
+        return sts
+
+    # plain loop: each domain to the horizon through compute_dt + step, one after another
+    from rbsim.scheduler import MultiRateScheduler
+    from rbsim.schemes import local_inertial as li
+
+    sts = fresh()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plain_steps = 0
+    for st, (_, rain, _) in zip(sts, spec, strict=True):
+        sched = MultiRateScheduler(end_time=horizon, output_every=horizon)
+        for tick in sched.ticks(lambda st=st: li.compute_dt(st, 0.7, 30.0)):
+            li.step(st, tick.dt, rain=rain)
+            plain_steps += 1
+    torch.cuda.synchronize()
+    plain_wall = time.perf_counter() - t0
+    plain_h = [st.h.cpu().numpy() for st in sts[:8]]
+    del sts
+    torch.cuda.empty_cache()
+
+    sts = fresh()
+    rains = [r for _, r, _ in spec]
+
+    def make(li_v, hl_v):
+        e = Ensemble(sts, ["local_inertial"] * len(sts), alpha=0.7, dt_max=30.0, sync_times=[[horizon]] * len(sts),
+                     rain_rate=rains, rain_until=[horizon] * len(sts), li_variant=li_v, hllc_variant=hl_v,
+                     graph_steps=8)  # fmt: skip
+        e.set_targets(horizon)
+        return e
+
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    best, timings = autotune(make, probe_replays=1, candidates=[(0, 0), (1, 0), (2, 0)])
+    ens = make(*best)
+    ens.graph_steps = 32
+    replays = ens.run_until(horizon)
+    torch.cuda.synchronize()
+    batched_wall = time.perf_counter() - t0
+    steps = sum(c.steps for c in ens.clock)
+    same = all(np.array_equal(sts[k].h.cpu().numpy(), plain_h[k]) for k in range(len(plain_h)))
+    return {
+        "workload": "ensemble_256", "metric": "ensemble solves/s", "domains": len(spec), "cells": cells,
+        "batched": {"wall_s": batched_wall, "solves_per_s": len(spec) / batched_wall, "replays": replays,
+                    "tiles": {"li_variant": best[0]}, "autotune_ms_per_replay": {str(k): v for k, v in timings.items()},
+                    "gcell_per_s": cells * 0 + sum(c.steps * b.size for c, (b, _, _) in zip(ens.clock, spec)) /
+                    batched_wall / 1e9, "steps": steps},
+        "plain_loop": {"wall_s": plain_wall, "solves_per_s": len(spec) / plain_wall, "steps": plain_steps},
+        "speedup": plain_wall / batched_wall, "first_8_domains_bitwise_equal_to_plain": same,
+    }  # fmt: skip
+
+
+def serve(args):
+    from rbsim.serve import Server, poisson_stream, serial_baseline
+
+    out = {"workload": "serve", "metric": "solves/s, p50/p99 latency", "rates": {}}
+    for rate in [float(r) for r in args.rates.split(",")]:
+        reqs = poisson_stream(rate, args.requests, seed=int(rate * 100))
+        srv = Server(hbm_budget=150e9, graph_steps=16)
+        srv.run(reqs)
+        torch.cuda.empty_cache()
+        serial = serial_baseline(reqs)
+        out["rates"][str(rate)] = {"batched": srv.stats, "serial": serial,
+                                   "throughput_ratio": srv.stats["solves_per_s"] / serial["solves_per_s"]}  # fmt: skip
+        torch.cuda.empty_cache()
+    return out
+
+
+def run(args):
+    torch.cuda.set_device(0)
+    fn = {"li_rain_512": li_rain_512, "li_reach_8192": li_reach_8192, "ensemble_256": ensemble_256,
+          "serve": serve}[args.workload]  # fmt: skip
+    return fn(args)
