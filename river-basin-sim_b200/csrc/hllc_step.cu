@@ -92,33 +92,85 @@ __device__ __forceinline__ void hllc_flux(float hl, float ul, float vtl, float h
   f2 = fh * vt;
 }
 
-// One face of the MUSCL + Audusse reconstruction (hllc.py:306-354 / :378-424):
-// four cells along the normal (m2, m1 | p0, p1), the face between m1 and p0.
+// A cell of the stencil, in the face's frame: depth, normal and transverse
+// velocity, bed.
 struct Cell {
-  float h, un, ut, z;  // depth, normal velocity, transverse velocity, bed
+  float h, un, ut, z;
 };
 
-__device__ __forceinline__ void muscl_face(const Cell& c0, const Cell& c1, const Cell& c2, const Cell& c3, float& fh,
-                                           float& fmn_l, float& fmn_r, float& fmt) {
+// MUSCL-minmod reconstruction of one cell to its two faces along the normal
+// (hllc.py:325-342): the east ("E", +1/2) and west ("W", -1/2) values of the water
+// surface, bed, normal and transverse velocity, first order at a dry-adjacent cell.
+struct Rec {
+  float eE, zE, nE, tE, eW, zW, nW, tW;
+};
+
+__device__ __forceinline__ Rec recon(const Cell& m, const Cell& c, const Cell& p) {
+  const float em = m.h + m.z, ec = c.h + c.z, ep = p.h + p.z;
+  const float hw = 0.5f * dryfactor(c.h, m.h, p.h);
+  const float me = minmod(ec - em, ep - ec);
+  const float mz = minmod(c.z - m.z, p.z - c.z);
+  const float mn = minmod(c.un - m.un, p.un - c.un);
+  const float mt = minmod(c.ut - m.ut, p.ut - c.ut);
+  Rec r;
+  r.eE = ec + hw * me;
+  r.eW = ec - hw * me;
+  r.zE = c.z + hw * mz;
+  r.zW = c.z - hw * mz;
+  r.nE = c.un + hw * mn;
+  r.nW = c.un - hw * mn;
+  r.tE = c.ut + hw * mt;
+  r.tW = c.ut - hw * mt;
+  return r;
+}
+
+// hllc.py:191-247, the mass component only (identical arithmetic to hllc_flux's fh).
+__device__ __forceinline__ float hllc_mass(float hl, float ul, float hr, float ur) {
   const float g = kG;
-  const float e0 = c0.h + c0.z, e1 = c1.h + c1.z, e2 = c2.h + c2.z, e3 = c3.h + c3.z;
-  const float wl = dryfactor(c1.h, c0.h, c2.h);
-  const float wr = dryfactor(c2.h, c1.h, c3.h);
-  const float eta_l = e1 + 0.5f * wl * minmod(e1 - e0, e2 - e1);
-  const float eta_r = e2 - 0.5f * wr * minmod(e2 - e1, e3 - e2);
-  const float zf_l = c1.z + 0.5f * wl * minmod(c1.z - c0.z, c2.z - c1.z);
-  const float zf_r = c2.z - 0.5f * wr * minmod(c2.z - c1.z, c3.z - c2.z);
-  const float un_l = c1.un + 0.5f * wl * minmod(c1.un - c0.un, c2.un - c1.un);
-  const float un_r = c2.un - 0.5f * wr * minmod(c2.un - c1.un, c3.un - c2.un);
-  const float ut_l = c1.ut + 0.5f * wl * minmod(c1.ut - c0.ut, c2.ut - c1.ut);
-  const float ut_r = c2.ut - 0.5f * wr * minmod(c2.ut - c1.ut, c3.ut - c2.ut);
-  const float h_l = rmax(eta_l - zf_l, 0.0f);
-  const float h_r = rmax(eta_r - zf_r, 0.0f);
-  const float z_star = rmax(zf_l, zf_r);
-  const float hl_star = rmax(eta_l - z_star, 0.0f);
-  const float hr_star = rmax(eta_r - z_star, 0.0f);
+  const float cl = sqrtf(g * rmax(hl, 0.0f));
+  const float cr = sqrtf(g * rmax(hr, 0.0f));
+  const bool dry_l = hl <= kHDry, dry_r = hr <= kHDry;
+  if (dry_l && dry_r) return 0.0f;
+  float sl, sr;
+  if (dry_l) {
+    sl = ur - 2.0f * cr;
+    sr = ur + cr;
+  } else if (dry_r) {
+    sl = ul - cl;
+    sr = ul + 2.0f * cl;
+  } else {
+    const float hs = 0.5f * (cl + cr) + 0.25f * (ul - ur);
+    const float h_star = rmax(hs * hs / g, 0.0f);
+    const float c_star = sqrtf(g * h_star);
+    const float u_star = 0.5f * (ul + ur) + cl - cr;
+    sl = rmin(ul - cl, u_star - c_star);
+    sr = rmax(ur + cr, u_star + c_star);
+  }
+  const float fh_l = hl * ul;
+  const float fh_r = hr * ur;
+  if (sl >= 0.0f) return fh_l;
+  if (sr <= 0.0f) return fh_r;
+  const float inv = 1.0f / (sr - sl);
+  return (sr * fh_l - sl * fh_r + sl * sr * (hr - hl)) * inv;
+}
+
+// The face between a left cell's east values and a right cell's west values:
+// Audusse hydrostatic reconstruction and HLLC (hllc.py:344-354), with the left and
+// right bed-slope corrections of the normal momentum flux.
+__device__ __forceinline__ void face_flux(const Rec& L, const Rec& R, bool full, float& fh, float& fmn_l,
+                                          float& fmn_r, float& fmt) {
+  const float g = kG;
+  const float h_l = rmax(L.eE - L.zE, 0.0f);
+  const float h_r = rmax(R.eW - R.zW, 0.0f);
+  const float z_star = rmax(L.zE, R.zW);
+  const float hl_star = rmax(L.eE - z_star, 0.0f);
+  const float hr_star = rmax(R.eW - z_star, 0.0f);
+  if (!full) {
+    fh = hllc_mass(hl_star, L.nE, hr_star, R.nW);
+    return;
+  }
   float f0, f1, f2;
-  hllc_flux(hl_star, un_l, ut_l, hr_star, un_r, ut_r, f0, f1, f2);
+  hllc_flux(hl_star, L.nE, L.tE, hr_star, R.nW, R.tW, f0, f1, f2);
   fh = f0;
   fmn_l = f1 + 0.5f * g * (h_l * h_l - hl_star * hl_star);
   fmn_r = f1 + 0.5f * g * (h_r * h_r - hr_star * hr_star);
@@ -213,95 +265,122 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
   }
   __syncthreads();
 
-  // 2. x-face fluxes (hllc.py:285-354), boundary corrections (:993-1109).
-  for (int k = threadIdx.x; k < XH * XW; k += NT) {
-    const int a = k / XW, b = k - a * XW;
-    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-    if (gi < 0 || gi >= ny || gj < 0 || gj > nx) continue;
-    const int r = a + 2;  // cell row; stencil columns c = b .. b+3 (cells gj-2 .. gj+1)
-    float fh, fl, fr, ft;
-    const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
-    if (kind == RB_BC_OPEN) {
-      const Cell c0{s_h[r][b], s_u[r][b], s_v[r][b], s_z[r][b]};
-      const Cell c1{s_h[r][b + 1], s_u[r][b + 1], s_v[r][b + 1], s_z[r][b + 1]};
-      const Cell c2{s_h[r][b + 2], s_u[r][b + 2], s_v[r][b + 2], s_z[r][b + 2]};
-      const Cell c3{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
-      muscl_face(c0, c1, c2, c3, fh, fl, fr, ft);
-    } else {
-      // The edge cell is column 0 (west) or nx-1 (east): region column b+2 or b+1.
-      const int ce = gj == 0 ? b + 2 : b + 1;
-      const float h0 = s_h[r][ce], u0 = s_u[r][ce], v0 = s_v[r][ce];
-      fl = 0.0f;
-      fr = 0.0f;
-      float f1;
-      if (kind == RB_BC_CLOSED) {  // reflective wall, hllc.py:442-481
-        if (gj == 0)
-          hllc_flux(h0, -u0, v0, h0, u0, v0, fh, f1, ft);
-        else
-          hllc_flux(h0, u0, v0, h0, -u0, v0, fh, f1, ft);
-      } else {  // prescribed surface, hllc.py:537-581
-        const float stage = gj == 0 ? stage_w : stage_e;
-        const float h_g = rmax(stage - s_z[r][ce], 0.0f);
-        if (gj == 0)
-          hllc_flux(h_g, u0, v0, h0, u0, v0, fh, f1, ft);
-        else
-          hllc_flux(h0, u0, v0, h_g, u0, v0, fh, f1, ft);
+  // 2. face fluxes (hllc.py:285-424) with boundary corrections (:993-1109).
+  // A thread takes FU consecutive faces along the normal and reconstructs each cell
+  // once in a rolling window of three cells: the reference's face-local eta_l /
+  // eta_r are exactly the left cell's east and the right cell's west values.
+  // The faces of the 1-cell ring around the tile only feed the limiter's beta, so
+  // they get the mass flux alone.
+  constexpr int FU = 3;
+  constexpr int GX = (XW + FU - 1) / FU, GY = (YH + FU - 1) / FU;
+  for (int k = threadIdx.x; k < XH * GX; k += NT) {
+    const int a = k / GX, g = k - a * GX;
+    const int gi = y0 - 1 + a;
+    if (gi < 0 || gi >= ny) continue;
+    const int r = a + 2;
+    const int b0 = g * FU;
+    Cell c0{s_h[r][b0 + 1], s_u[r][b0 + 1], s_v[r][b0 + 1], s_z[r][b0 + 1]};
+    Cell cp{s_h[r][b0 + 2], s_u[r][b0 + 2], s_v[r][b0 + 2], s_z[r][b0 + 2]};
+    Rec left = recon(Cell{s_h[r][b0], s_u[r][b0], s_v[r][b0], s_z[r][b0]}, c0, cp);
+#pragma unroll
+    for (int f = 0; f < FU; f++) {
+      const int b = b0 + f;
+      if (b >= XW) break;
+      const Cell cn{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
+      const Rec right = recon(c0, cp, cn);
+      const int gj = x0 - 1 + b;
+      if (gj >= 0 && gj <= nx) {
+        const bool inner = a >= 1 && a <= TY && b >= 1 && b <= TX + 1;
+        float fh, fl = 0.0f, fr = 0.0f, ft = 0.0f;
+        const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
+        if (kind == RB_BC_OPEN) {
+          face_flux(left, right, inner, fh, fl, fr, ft);
+        } else {
+          // edge cell: column 0 (west, region column b+2) or nx-1 (east, b+1)
+          const Cell& e = gj == 0 ? cp : c0;
+          float f1;
+          if (kind == RB_BC_CLOSED) {  // reflective wall, hllc.py:442-481
+            if (gj == 0)
+              hllc_flux(e.h, -e.un, e.ut, e.h, e.un, e.ut, fh, f1, ft);
+            else
+              hllc_flux(e.h, e.un, e.ut, e.h, -e.un, e.ut, fh, f1, ft);
+          } else {  // prescribed surface, hllc.py:537-581
+            const float h_g = rmax((gj == 0 ? stage_w : stage_e) - e.z, 0.0f);
+            if (gj == 0)
+              hllc_flux(h_g, e.un, e.ut, e.h, e.un, e.ut, fh, f1, ft);
+            else
+              hllc_flux(e.h, e.un, e.ut, h_g, e.un, e.ut, fh, f1, ft);
+          }
+          if (gj == 0)
+            fr = f1;  // only the inward slot is read (hllc.py:439-440)
+          else
+            fl = f1;
+        }
+        s_fxh[a][b] = fh;
+        if (inner) {
+          s_fxl[a - 1][b - 1] = fl;
+          s_fxr[a - 1][b - 1] = fr;
+          s_fxt[a - 1][b - 1] = ft;
+        }
       }
-      if (gj == 0)
-        fr = f1;  // only the inward slot is read (hllc.py:439-440)
-      else
-        fl = f1;
-    }
-    s_fxh[a][b] = fh;
-    if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
-      s_fxl[a - 1][b - 1] = fl;
-      s_fxr[a - 1][b - 1] = fr;
-      s_fxt[a - 1][b - 1] = ft;
+      left = right;
+      c0 = cp;
+      cp = cn;
     }
   }
-  // y-face fluxes (hllc.py:357-424): normal velocity v, transverse u.
-  for (int k = threadIdx.x; k < YH * YW; k += NT) {
-    const int a = k / YW, b = k - a * YW;
-    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-    if (gj < 0 || gj >= nx || gi < 0 || gi > ny) continue;
-    const int c = b + 2;  // cell column; stencil rows r = a .. a+3 (cells gi-2 .. gi+1)
-    float fh, fl, fr, ft;
-    const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
-    if (kind == RB_BC_OPEN) {
-      const Cell c0{s_h[a][c], s_v[a][c], s_u[a][c], s_z[a][c]};
-      const Cell c1{s_h[a + 1][c], s_v[a + 1][c], s_u[a + 1][c], s_z[a + 1][c]};
-      const Cell c2{s_h[a + 2][c], s_v[a + 2][c], s_u[a + 2][c], s_z[a + 2][c]};
-      const Cell c3{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
-      muscl_face(c0, c1, c2, c3, fh, fl, fr, ft);
-    } else {
-      const int re = gi == 0 ? a + 2 : a + 1;
-      const float h0 = s_h[re][c], u0 = s_u[re][c], v0 = s_v[re][c];
-      fl = 0.0f;
-      fr = 0.0f;
-      float f1;
-      if (kind == RB_BC_CLOSED) {  // hllc.py:483-521
-        if (gi == 0)
-          hllc_flux(h0, -v0, u0, h0, v0, u0, fh, f1, ft);
-        else
-          hllc_flux(h0, v0, u0, h0, -v0, u0, fh, f1, ft);
-      } else {  // hllc.py:584-628
-        const float stage = gi == 0 ? stage_n : stage_s;
-        const float h_g = rmax(stage - s_z[re][c], 0.0f);
-        if (gi == 0)
-          hllc_flux(h_g, v0, u0, h0, v0, u0, fh, f1, ft);
-        else
-          hllc_flux(h0, v0, u0, h_g, v0, u0, fh, f1, ft);
+  // y-faces: normal velocity v, transverse u (hllc.py:357-424).
+  for (int k = threadIdx.x; k < GY * YW; k += NT) {
+    const int g = k / YW, b = k - g * YW;
+    const int gj = x0 - 1 + b;
+    if (gj < 0 || gj >= nx) continue;
+    const int c = b + 2;
+    const int a0 = g * FU;
+    Cell c0{s_h[a0 + 1][c], s_v[a0 + 1][c], s_u[a0 + 1][c], s_z[a0 + 1][c]};
+    Cell cp{s_h[a0 + 2][c], s_v[a0 + 2][c], s_u[a0 + 2][c], s_z[a0 + 2][c]};
+    Rec left = recon(Cell{s_h[a0][c], s_v[a0][c], s_u[a0][c], s_z[a0][c]}, c0, cp);
+#pragma unroll
+    for (int f = 0; f < FU; f++) {
+      const int a = a0 + f;
+      if (a >= YH) break;
+      const Cell cn{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
+      const Rec right = recon(c0, cp, cn);
+      const int gi = y0 - 1 + a;
+      if (gi >= 0 && gi <= ny) {
+        const bool inner = a >= 1 && a <= TY + 1 && b >= 1 && b <= TX;
+        float fh, fl = 0.0f, fr = 0.0f, ft = 0.0f;
+        const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
+        if (kind == RB_BC_OPEN) {
+          face_flux(left, right, inner, fh, fl, fr, ft);
+        } else {
+          const Cell& e = gi == 0 ? cp : c0;  // edge cell row 0 (north) or ny-1 (south)
+          float f1;
+          if (kind == RB_BC_CLOSED) {  // hllc.py:483-521
+            if (gi == 0)
+              hllc_flux(e.h, -e.un, e.ut, e.h, e.un, e.ut, fh, f1, ft);
+            else
+              hllc_flux(e.h, e.un, e.ut, e.h, -e.un, e.ut, fh, f1, ft);
+          } else {  // hllc.py:584-628
+            const float h_g = rmax((gi == 0 ? stage_n : stage_s) - e.z, 0.0f);
+            if (gi == 0)
+              hllc_flux(h_g, e.un, e.ut, e.h, e.un, e.ut, fh, f1, ft);
+            else
+              hllc_flux(e.h, e.un, e.ut, h_g, e.un, e.ut, fh, f1, ft);
+          }
+          if (gi == 0)
+            fr = f1;
+          else
+            fl = f1;
+        }
+        s_fyh[a][b] = fh;
+        if (inner) {
+          s_fyl[a - 1][b - 1] = fl;
+          s_fyr[a - 1][b - 1] = fr;
+          s_fyt[a - 1][b - 1] = ft;
+        }
       }
-      if (gi == 0)
-        fr = f1;
-      else
-        fl = f1;
-    }
-    s_fyh[a][b] = fh;
-    if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
-      s_fyl[a - 1][b - 1] = fl;
-      s_fyr[a - 1][b - 1] = fr;
-      s_fyt[a - 1][b - 1] = ft;
+      left = right;
+      c0 = cp;
+      cp = cn;
     }
   }
   __syncthreads();
