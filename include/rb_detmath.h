@@ -1,11 +1,13 @@
 /*
  * rb_detmath.h -- deterministic float32 power functions for the river-basin solver path.
  *
- * The reference evaluates three fractional powers in float32 through the platform
+ * The reference evaluates four fractional powers in float32 through the platform
  * libm (`wp.pow`), each with a float32 exponent:
  *   - h_flow ^ float32(7/3) in the semi-implicit Manning denominator
  *     (solver/core/friction.py:30, used by local_inertial.py:98,128 and hllc.py:937);
  *   - R ^ float32(1/3) in the Manning bed shear (solver/core/sediment.py:168);
+ *   - R ^ float32(4/3) in the sub-grid channel's Manning denominator
+ *     (solver/core/friction.py:56-58, used by local_inertial.py:310);
  *   - (theta - theta_c) ^ 1.5 in the Meyer-Peter-Mueller capacity (sediment.py:192).
  * Note the exponents: float32(7/3) = 2.3333332538604736, so the reference computes
  * x^2.33333325..., not x^(7/3) (a difference of up to ~10 ulp for large x).
@@ -45,9 +47,10 @@
 #define RB_HD static inline
 #endif
 
-/* p - float32(p) for p = 7/3 and p = 1/3 (double arithmetic). */
+/* p - float32(p) for p = 7/3, 1/3 and 4/3. */
 #define RB_DELTA_73 7.947285984855057e-08
 #define RB_DELTA_13 (-9.934107481068821e-09)
+#define RB_DELTA_43 (-3.9736429850260414e-08)
 
 RB_HD uint64_t rb_bits_of(double d) {
 #if defined(__CUDA_ARCH__)
@@ -124,6 +127,14 @@ RB_HD float rb_pow13f(float x) {
   if (x > 3.4028234663852886e38f) return x;
   const double d = (double)x;
   return (float)(rb_cbrt_pos(d) * rb_offset_factor(d, RB_DELTA_13));
+}
+
+/* x ^ float32(4/3) as a float; same special cases as rb_pow73f. */
+RB_HD float rb_pow43f(float x) {
+  if (!(x > 0.0f)) return x == 0.0f ? 0.0f : (x - x) / (x - x);
+  if (x > 3.4028234663852886e38f) return x;
+  const double d = (double)x;
+  return (float)((d * rb_cbrt_pos(d)) * rb_offset_factor(d, RB_DELTA_43));
 }
 
 /* x ^ 1.5 as a float for x >= 0 (NaN below 0 or for NaN). */

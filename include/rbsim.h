@@ -71,6 +71,13 @@ typedef struct rb_li_fields {
   const float *d50;
   float *qs_int_x, *qs_comp_x; /* (ny, nx+1) transport integral + Kahan residue */
   float *qs_int_y, *qs_comp_y; /* (ny+1, nx) */
+  /* Sub-grid channels (solver/core/channels.py:182-312); chan_w == NULL: unarmed.
+   * Geometry per cell (w = d = 0 where there is no channel; callers validate as
+   * channels.py:214-262 does); the split face discharges are double buffered
+   * like qx / qy: the step reads [cur] and writes [cur ^ 1]. */
+  const float *chan_w, *chan_d, *chan_n; /* (ny, nx) width m, bank-full depth m, roughness */
+  float *qx_ch[2], *qx_fp[2];            /* (ny, nx+1) channel / floodplain x-face discharge */
+  float *qy_ch[2], *qy_fp[2];            /* (ny+1, nx) */
 } rb_li_fields;
 
 /* HLLC state (state.py:52-57, hllc.py:96-152). */

@@ -14,11 +14,12 @@ points with ctypes, and restates the host-side Python of the reference path:
 * ``stage_at``                           -- solver/core/boundaries.py:199-220
 * ``Inflow.discharge_at``                -- solver/io/config.py:111-122
 * ``InflowInjector.apply``               -- solver/processes/inflow.py:116-200
+* ``arm_channels`` / storage curve       -- solver/core/channels.py:140-312
 * ``arm_sediment`` / Exner activation    -- solver/core/sediment.py:658-709,
                                             solver/processes/morphology.py:223-321
 * ``MassLedger``                         -- solver/core/massbalance.py:39-158
 
-``pow_mode`` selects how the three fractional powers are evaluated: 0 = libm
+``pow_mode`` selects how the four fractional powers are evaluated: 0 = libm
 ``powf`` (what the reference's CPU build calls), 1 = the deterministic functions
 of ``include/rb_detmath.h`` that the CUDA kernels use (bit-identical to them).
 """
@@ -85,6 +86,8 @@ def _li_struct(R):
                 ("h_comp", P), ("rain", P), ("infil", P), ("loss_cum", P),
                 ("bc", ctypes.c_int32 * 4),
                 ("d50", P), ("qs_int_x", P), ("qs_comp_x", P), ("qs_int_y", P), ("qs_comp_y", P),
+                ("chan_w", P), ("chan_d", P), ("chan_n", P),
+                ("qx_ch", P), ("qx_fp", P), ("qy_ch", P), ("qy_fp", P),
             ]
         },
     )  # fmt: skip
@@ -148,6 +151,19 @@ class Sediment:
 
 
 @dataclass
+class Channels:
+    """Sub-grid channel geometry and the split face discharges (channels.py:182-208)."""
+
+    w: np.ndarray
+    d: np.ndarray
+    n: np.ndarray
+    qx_ch: np.ndarray
+    qx_fp: np.ndarray
+    qy_ch: np.ndarray
+    qy_fp: np.ndarray
+
+
+@dataclass
 class State:
     """Host arrays of one domain, laid out as the reference State (state.py:38-96)."""
 
@@ -172,6 +188,7 @@ class State:
     boundaries: dict = field(default_factory=lambda: {e: "closed" for e in EDGES})
     stage_curves: dict = field(default_factory=dict)
     sediment: Sediment | None = None
+    channels: Channels | None = None
 
     # --- construction / arming (state.py:98-226) -------------------------- #
     @classmethod
@@ -247,6 +264,32 @@ class State:
         )  # fmt: skip
         return self.sediment
 
+    def arm_channels(self, width, depth, manning=None):
+        """channels.py:265-312 arm_channels, after the validation of :214-262 (the
+        oracle keeps the normalisation "no channel" -> w = d = 0 and the refusals that
+        change results; the CUDA path's host code restates the full validation)."""
+        c = (self.ny, self.nx)
+        w = np.ascontiguousarray(width, dtype=np.float32).copy()
+        d = np.ascontiguousarray(depth, dtype=np.float32).copy()
+        n = (self.n.astype(np.float32).copy() if manning is None
+             else np.ascontiguousarray(manning, dtype=np.float32).copy())  # fmt: skip
+        if w.shape != c or d.shape != c or n.shape != c:
+            raise ValueError("channel field shape does not match the grid")
+        if (w > self.dx).any() or (w < 0).any() or (d < 0).any():
+            raise ValueError("channel width must be in [0, dx] and depth >= 0")
+        has = (w > 0) & (d > 0)
+        if ((w > 0) != (d > 0)).any():
+            raise ValueError("a channel needs both a width and a bank-full depth")
+        w[~has] = 0.0
+        d[~has] = 0.0
+        dt = self.dtype
+        fx, fy = (self.ny, self.nx + 1), (self.ny + 1, self.nx)
+        self.channels = Channels(
+            w=w.astype(dt), d=d.astype(dt), n=n.astype(dt),
+            qx_ch=np.zeros(fx, dt), qx_fp=np.zeros(fx, dt), qy_ch=np.zeros(fy, dt), qy_fp=np.zeros(fy, dt),
+        )  # fmt: skip
+        return self.channels
+
     # --- diagnostics ------------------------------------------------------- #
     @property
     def cell_area(self) -> float:
@@ -289,20 +332,23 @@ def li_compute_dt(st: State, alpha: float = 0.7, dt_max: float = 30.0) -> float:
     L = lib(st.dtype)
     f = getattr(L, "rbo_li_compute_dt" + st._suffix())
     f.restype = ctypes.c_double
-    return float(f(st.ny, st.nx, _ptr(st.h), ctypes.c_double(st.dx), ctypes.c_double(alpha),
-                   ctypes.c_double(dt_max)))  # fmt: skip
+    ch = st.channels
+    return float(f(st.ny, st.nx, _ptr(st.h), _ptr(ch.w) if ch else None, _ptr(ch.d) if ch else None,
+                   ctypes.c_double(st.dx), ctypes.c_double(alpha), ctypes.c_double(dt_max)))  # fmt: skip
 
 
 def li_step(st: State, dt: float, rain: float = 0.0, limit: bool = True, rain_scale: float = 1.0,
             t: float = 0.0) -> None:  # fmt: skip
     L = lib(st.dtype)
     sed = st.sediment
+    ch = st.channels
+    chp = [_ptr(getattr(ch, k)) if ch else None for k in ("w", "d", "n", "qx_ch", "qx_fp", "qy_ch", "qy_fp")]
     s = _LI_STRUCT(
         st.ny, st.nx, st.dx, _ptr(st.h), _ptr(st.z), _ptr(st.n), _ptr(st.qx), _ptr(st.qy), _ptr(st.eta),
         _ptr(st.beta), _ptr(st.h_comp), _ptr(st.rain), _ptr(st.infil), _ptr(st.loss_cum), st._bc(),
         _ptr(sed.d50) if sed else None, _ptr(sed.qs_int_x) if sed else None,
         _ptr(sed.qs_comp_x) if sed else None, _ptr(sed.qs_int_y) if sed else None,
-        _ptr(sed.qs_comp_y) if sed else None,
+        _ptr(sed.qs_comp_y) if sed else None, *chp,
     )  # fmt: skip
     getattr(L, "rbo_li_step" + st._suffix())(
         ctypes.byref(s), ctypes.c_double(dt), ctypes.c_double(rain), ctypes.c_int(int(bool(limit))),

@@ -12,7 +12,7 @@
  *
  * Arithmetic model: one IEEE rounding per operation in the reference's expression
  * order (build with -ffp-contract=off, no fast-math), `wp.max(a,b)` = a > b ? a : b,
- * `wp.min(a,b)` = a < b ? a : b, `wp.clamp(x,lo,hi)` = min(max(lo,x),hi). The three
+ * `wp.min(a,b)` = a < b ? a : b, `wp.clamp(x,lo,hi)` = min(max(lo,x),hi). The four
  * fractional powers go through rbo_pow: mode 0 calls libm powf (how the
  * reference's CPU build evaluates `wp.pow`), mode 1 calls the deterministic
  * functions of include/rb_detmath.h that the CUDA kernels use.
@@ -59,18 +59,27 @@ static inline R rclamp(R x, R lo, R hi) { return rmin(rmax(lo, x), hi); }
 static inline R rabs(R x) { return (R)fabs((double)x); }
 static inline R r_sqrt(R x) { return (R)(sizeof(R) == 4 ? (double)sqrtf((float)x) : sqrt((double)x)); }
 
-/* which: 0 -> x^(7/3), 1 -> x^(1/3), 2 -> x^1.5, each with the reference's float32 exponent. */
+/* which: 0 -> x^(7/3), 1 -> x^(1/3), 2 -> x^1.5, 3 -> x^(4/3), each with the
+ * reference's float32 exponent. */
 static inline R rbo_pow(R x, int which) {
   if (sizeof(R) == 8) {
-    const double p = which == 0 ? 7.0 / 3.0 : (which == 1 ? 1.0 / 3.0 : 1.5);
-    return (R)pow((double)x, p);
+    static const double P[4] = {7.0 / 3.0, 1.0 / 3.0, 1.5, 4.0 / 3.0};
+    return (R)pow((double)x, P[which]);
   }
   if (g_pow_mode == 1) {
-    return which == 0 ? rb_pow73f((float)x) : (which == 1 ? rb_pow13f((float)x) : rb_pow15f((float)x));
+    switch (which) {
+      case 0: return rb_pow73f((float)x);
+      case 1: return rb_pow13f((float)x);
+      case 2: return rb_pow15f((float)x);
+      default: return rb_pow43f((float)x);
+    }
   }
-  const float p = which == 0 ? 7.0f / 3.0f : (which == 1 ? 1.0f / 3.0f : 1.5f);
-  return powf((float)x, p);
+  static const float PF[4] = {7.0f / 3.0f, 1.0f / 3.0f, 1.5f, 4.0f / 3.0f};
+  return powf((float)x, PF[which]);
 }
+
+/* The power functions themselves, for the accuracy tests. */
+float API(rbo_pow)(float x, int which) { return (float)rbo_pow((R)x, which); }
 
 #define IX(i, j) ((size_t)(i) * (size_t)nx + (size_t)(j))         /* cells (ny, nx)    */
 #define FX(i, j) ((size_t)(i) * (size_t)(nx + 1) + (size_t)(j))   /* x-faces (ny, nx+1) */
@@ -387,6 +396,196 @@ void API(rbo_rebuild_bed)(int ny, int nx, const R *z0, const double *dz_cum, R *
 }
 
 /* ========================================================================= */
+/* Sub-grid channels (solver/core/channels.py, local_inertial.py:275-500,     */
+/* friction.py:35-58, sediment.py:276-377)                                    */
+/* ========================================================================= */
+
+/* channels.py:58-70 eta_subgrid */
+static inline R eta_subgrid(R h, R z, R w, R d, R dx) {
+  R eta = h + z;
+  if (w > C(0.0) && d > C(0.0)) {
+    const R h_bf = w * d / dx;
+    if (h <= h_bf)
+      eta = z - d + h * dx / w;
+    else
+      eta = z + (h - h_bf);
+  }
+  return eta;
+}
+
+/* channels.py:73-83 column_depth */
+static inline R column_depth(R h, R w, R d, R dx) {
+  R col = h;
+  if (w > C(0.0) && d > C(0.0)) {
+    const R h_bf = w * d / dx;
+    if (h <= h_bf)
+      col = h * dx / w;
+    else
+      col = d + (h - h_bf);
+  }
+  return col;
+}
+
+/* local_inertial.py:278-291 compute_eta_channels */
+void API(rbo_compute_eta_channels)(int ny, int nx, const R *h, const R *z, const R *w, const R *d, R dx, R *eta) {
+#pragma omp parallel for schedule(static)
+  for (int i = 0; i < ny; i++)
+    for (int j = 0; j < nx; j++) eta[IX(i, j)] = eta_subgrid(h[IX(i, j)], z[IX(i, j)], w[IX(i, j)], d[IX(i, j)], dx);
+}
+
+/* friction.py:35-58 manning_denominator_radius */
+static inline R manning_denominator_radius(R q_prev, R h_flow, R radius, R n, R g, R dt) {
+  return C(1.0) + g * dt * n * n * rabs(q_prev) / (h_flow * rbo_pow(radius, 3));
+}
+
+/* local_inertial.py:294-320 _channel_flux, with channels.py:120-135 (flow depth, radius) */
+static inline R channel_flux(R q_prev, R eta_max, R slope, R w_face, R z_bank, R z_ch, R n_ch, R dt, R g) {
+  if (w_face <= C(0.0)) return C(0.0);
+  const R h_ch = rmin(eta_max, z_bank) - z_ch;
+  if (h_ch < H_DRY) return C(0.0);
+  const R radius = w_face * h_ch / (w_face + C(2.0) * h_ch);
+  const R num = q_prev - g * h_ch * dt * slope;
+  const R den = manning_denominator_radius(q_prev, h_ch, radius, n_ch, g, dt);
+  return num / den;
+}
+
+/* local_inertial.py:323-336 _floodplain_flux */
+static inline R floodplain_flux(R q_prev, R eta_max, R slope, R z_bank, R n_fp, R dt, R g) {
+  const R h_fp = eta_max - z_bank;
+  if (h_fp < H_DRY) return C(0.0);
+  const R num = q_prev - g * h_fp * dt * slope;
+  const R den = manning_denominator(q_prev, h_fp, n_fp, g, dt);
+  return num / den;
+}
+
+/* One two-component face between cell a (left / top) and cell b (right / bottom):
+ * local_inertial.py:355-383 (x) and :401-427 (y), channels.py:98-117 (face width, bed). */
+static inline void channel_face(R *q, R *q_ch, R *q_fp, R eta_a, R eta_b, R z_a, R z_b, R n_a, R n_b, R w_a, R w_b,
+                                R d_a, R d_b, R cn_a, R cn_b, R dx, R dt, R g) {
+  const R eta_max = rmax(eta_a, eta_b);
+  const R slope = (eta_b - eta_a) / dx;
+  const R z_bank = rmax(z_a, z_b);
+  const R f_fp = floodplain_flux(*q_fp, eta_max, slope, z_bank, C(0.5) * (n_a + n_b), dt, g);
+  const R w_face = rmin(w_a, w_b);
+  const R z_ch = rmax(z_a - d_a, z_b - d_b);
+  const R f_ch = channel_flux(*q_ch, eta_max, slope, w_face, z_bank, z_ch, C(0.5) * (cn_a + cn_b), dt, g);
+  *q_fp = f_fp;
+  *q_ch = f_ch;
+  const R frac = w_face / dx;
+  *q = f_fp * (C(1.0) - frac) + f_ch * frac;
+}
+
+/* local_inertial.py:338-427 update_qx_channels / update_qy_channels (interior faces) */
+void API(rbo_update_q_channels)(int ny, int nx, R *qx, R *qx_ch, R *qx_fp, R *qy, R *qy_ch, R *qy_fp, const R *eta,
+                                const R *z, const R *n, const R *w, const R *d, const R *cn, R dx, R dt, R g) {
+  if (nx > 1) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < ny; i++)
+      for (int j = 1; j <= nx - 1; j++) {
+        const size_t a = IX(i, j - 1), b = IX(i, j), f = FX(i, j);
+        channel_face(&qx[f], &qx_ch[f], &qx_fp[f], eta[a], eta[b], z[a], z[b], n[a], n[b], w[a], w[b], d[a], d[b],
+                     cn[a], cn[b], dx, dt, g);
+      }
+  }
+  if (ny > 1) {
+#pragma omp parallel for schedule(static)
+    for (int i = 1; i <= ny - 1; i++)
+      for (int j = 0; j < nx; j++) {
+        const size_t a = IX(i - 1, j), b = IX(i, j), f = FY(i, j);
+        channel_face(&qy[f], &qy_ch[f], &qy_fp[f], eta[a], eta[b], z[a], z[b], n[a], n[b], w[a], w[b], d[a], d[b],
+                     cn[a], cn[b], dx, dt, g);
+      }
+  }
+}
+
+/* local_inertial.py:430-472 limit_qx_channels / limit_qy_channels */
+void API(rbo_limit_q_channels)(int ny, int nx, R *qx, R *qx_ch, R *qx_fp, R *qy, R *qy_ch, R *qy_fp,
+                               const R *beta) {
+  if (nx > 1) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < ny; i++)
+      for (int j = 1; j <= nx - 1; j++) {
+        const size_t f = FX(i, j);
+        const R q = qx[f];
+        if (q == C(0.0)) continue;
+        R b = beta[IX(i, j - 1)];
+        if (q < C(0.0)) b = beta[IX(i, j)];
+        qx[f] = q * b;
+        qx_ch[f] = qx_ch[f] * b;
+        qx_fp[f] = qx_fp[f] * b;
+      }
+  }
+  if (ny > 1) {
+#pragma omp parallel for schedule(static)
+    for (int i = 1; i <= ny - 1; i++)
+      for (int j = 0; j < nx; j++) {
+        const size_t f = FY(i, j);
+        const R q = qy[f];
+        if (q == C(0.0)) continue;
+        R b = beta[IX(i - 1, j)];
+        if (q < C(0.0)) b = beta[IX(i, j)];
+        qy[f] = q * b;
+        qy_ch[f] = qy_ch[f] * b;
+        qy_fp[f] = qy_fp[f] * b;
+      }
+  }
+}
+
+/* local_inertial.py:475-489 reduce_column_max */
+R API(rbo_reduce_column_max)(int ny, int nx, const R *h, const R *w, const R *d, R dx) {
+  R m = C(0.0);
+  for (int i = 0; i < ny; i++)
+    for (int j = 0; j < nx; j++) {
+      const R c = column_depth(h[IX(i, j)], w[IX(i, j)], d[IX(i, j)], dx);
+      if (c > m) m = c;
+    }
+  return m;
+}
+
+/* sediment.py:276-305 _combined_capacity */
+static inline R combined_capacity(R q_ch, R q_fp, R eta_max, R z_bank, R z_ch, R w_face, R n_fp, R n_ch, R d50,
+                                  R dx) {
+  const R h_fp = eta_max - z_bank;
+  const R qs_fp = face_capacity(q_fp, h_fp, h_fp, n_fp, d50);
+  R qs_ch = C(0.0);
+  if (w_face > C(0.0)) {
+    const R h_ch = rmin(eta_max, z_bank) - z_ch;
+    if (h_ch >= H_DRY) qs_ch = face_capacity(q_ch, h_ch, w_face * h_ch / (w_face + C(2.0) * h_ch), n_ch, d50);
+  }
+  const R frac = w_face / dx;
+  return qs_fp * (C(1.0) - frac) + qs_ch * frac;
+}
+
+/* sediment.py:308-377 accumulate_qs_x_channels / accumulate_qs_y_channels */
+void API(rbo_accumulate_qs_channels)(int ny, int nx, const R *qx_ch, const R *qx_fp, const R *qy_ch, const R *qy_fp,
+                                     const R *eta, const R *z, const R *n, const R *d50, const R *w, const R *d,
+                                     const R *cn, R dx, R dt, R *qs_int_x, R *qs_comp_x, R *qs_int_y,
+                                     R *qs_comp_y) {
+  if (nx > 1) {
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < ny; i++)
+      for (int j = 1; j <= nx - 1; j++) {
+        const size_t a = IX(i, j - 1), b = IX(i, j), f = FX(i, j);
+        const R qs = combined_capacity(qx_ch[f], qx_fp[f], rmax(eta[a], eta[b]), rmax(z[a], z[b]),
+                                       rmax(z[a] - d[a], z[b] - d[b]), rmin(w[a], w[b]), C(0.5) * (n[a] + n[b]),
+                                       C(0.5) * (cn[a] + cn[b]), C(0.5) * (d50[a] + d50[b]), dx);
+        kahan_add(&qs_int_x[f], &qs_comp_x[f], qs * dt);
+      }
+  }
+  if (ny > 1) {
+#pragma omp parallel for schedule(static)
+    for (int i = 1; i <= ny - 1; i++)
+      for (int j = 0; j < nx; j++) {
+        const size_t a = IX(i - 1, j), b = IX(i, j), f = FY(i, j);
+        const R qs = combined_capacity(qy_ch[f], qy_fp[f], rmax(eta[a], eta[b]), rmax(z[a], z[b]),
+                                       rmax(z[a] - d[a], z[b] - d[b]), rmin(w[a], w[b]), C(0.5) * (n[a] + n[b]),
+                                       C(0.5) * (cn[a] + cn[b]), C(0.5) * (d50[a] + d50[b]), dx);
+        kahan_add(&qs_int_y[f], &qs_comp_y[f], qs * dt);
+      }
+  }
+}
+
+/* ========================================================================= */
 /* Point sources (solver/processes/inflow.py:74-113)                          */
 /* ========================================================================= */
 void API(rbo_inject_points)(int ny, int nx, R *h, R *comp, int nsrc, const int32_t *rows, const int32_t *cols,
@@ -417,22 +616,39 @@ typedef struct {
   int32_t bc[4];  /* per edge (north, south, east, west): 0 closed, 1 open, 2 fixed_stage */
   R *d50;         /* NULL: sediment unarmed */
   R *qs_int_x, *qs_comp_x, *qs_int_y, *qs_comp_y;
+  R *chan_w, *chan_d, *chan_n; /* (ny, nx); chan_w NULL: sub-grid channels unarmed */
+  R *qx_ch, *qx_fp;            /* (ny, nx+1) channel / floodplain components */
+  R *qy_ch, *qy_fp;            /* (ny+1, nx) */
 } rbo_li_state;
 
 void API(rbo_li_step)(rbo_li_state *s, double dt, double rain, int limit, double rain_scale) {
   const int ny = s->ny, nx = s->nx;
   const R dxf = (R)s->dx, dtf = (R)dt, gf = G;
-  API(rbo_compute_eta)(ny, nx, s->h, s->z, s->eta);
-  if (nx > 1) API(rbo_update_qx)(ny, nx, s->qx, s->eta, s->z, s->n, dxf, dtf, gf);
-  if (ny > 1) API(rbo_update_qy)(ny, nx, s->qy, s->eta, s->z, s->n, dxf, dtf, gf);
+  const int chan = s->chan_w != NULL;
+  if (!chan) {
+    API(rbo_compute_eta)(ny, nx, s->h, s->z, s->eta);
+    if (nx > 1) API(rbo_update_qx)(ny, nx, s->qx, s->eta, s->z, s->n, dxf, dtf, gf);
+    if (ny > 1) API(rbo_update_qy)(ny, nx, s->qy, s->eta, s->z, s->n, dxf, dtf, gf);
+  } else {
+    API(rbo_compute_eta_channels)(ny, nx, s->h, s->z, s->chan_w, s->chan_d, dxf, s->eta);
+    API(rbo_update_q_channels)(ny, nx, s->qx, s->qx_ch, s->qx_fp, s->qy, s->qy_ch, s->qy_fp, s->eta, s->z, s->n,
+                               s->chan_w, s->chan_d, s->chan_n, dxf, dtf, gf);
+  }
   API(rbo_zero_edges)(ny, nx, s->qx, s->qy);
   if (limit) {
     API(rbo_outflow_beta)(ny, nx, s->h, s->qx, s->qy, dxf, dtf, s->beta);
-    API(rbo_limit_q)(ny, nx, s->qx, s->qy, s->beta);
+    if (!chan)
+      API(rbo_limit_q)(ny, nx, s->qx, s->qy, s->beta);
+    else
+      API(rbo_limit_q_channels)(ny, nx, s->qx, s->qx_ch, s->qx_fp, s->qy, s->qy_ch, s->qy_fp, s->beta);
   }
-  if (s->d50)
+  if (s->d50 && !chan)
     API(rbo_accumulate_qs)(ny, nx, s->qx, s->qy, s->eta, s->z, s->n, s->d50, dtf, s->qs_int_x, s->qs_comp_x,
                            s->qs_int_y, s->qs_comp_y);
+  if (s->d50 && chan)
+    API(rbo_accumulate_qs_channels)(ny, nx, s->qx_ch, s->qx_fp, s->qy_ch, s->qy_fp, s->eta, s->z, s->n, s->d50,
+                                    s->chan_w, s->chan_d, s->chan_n, dxf, dtf, s->qs_int_x, s->qs_comp_x,
+                                    s->qs_int_y, s->qs_comp_y);
   const int compensated = s->h_comp != NULL;
   API(rbo_update_h)(ny, nx, s->h, s->qx, s->qy, dxf, dtf, compensated ? C(0.0) : (R)rain);
   if (compensated && s->rain == NULL) API(rbo_uniform_rain_c)(ny, nx, s->h, s->h_comp, (R)rain, dtf);
@@ -450,9 +666,12 @@ void API(rbo_li_step)(rbo_li_state *s, double dt, double rain, int limit, double
   }
 }
 
-/* local_inertial.py:515-544 compute_dt (host float64 arithmetic) */
-double API(rbo_li_compute_dt)(int ny, int nx, const R *h, double dx, double alpha, double dt_max) {
-  const double h_max = (double)API(rbo_reduce_hmax)(ny, nx, h);
+/* local_inertial.py:515-544 compute_dt (host float64 arithmetic); with channels
+ * armed (w, d non-NULL) the reduction is over the water column (:475-489). */
+double API(rbo_li_compute_dt)(int ny, int nx, const R *h, const R *w, const R *d, double dx, double alpha,
+                              double dt_max) {
+  const double h_max = (double)(w != NULL ? API(rbo_reduce_column_max)(ny, nx, h, w, d, (R)dx)
+                                          : API(rbo_reduce_hmax)(ny, nx, h));
   if (h_max <= 1.0e-3) return dt_max;
   const double dt = alpha * dx / sqrt(9.81 * h_max);
   return dt < dt_max ? dt : dt_max;

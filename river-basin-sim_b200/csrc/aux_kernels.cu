@@ -19,6 +19,19 @@ __global__ void __launch_bounds__(RED_NT) max_h_kernel(const float* __restrict__
   block_max_to<RED_NT>(m, key, s_w);
 }
 
+// local_inertial.py:475-489 reduce_column_max into a zeroed slot.
+__global__ void __launch_bounds__(RED_NT) max_column_kernel(const float* __restrict__ h, const float* __restrict__ w,
+                                                             const float* __restrict__ d, float dx, size_t n,
+                                                             unsigned int* key) {
+  __shared__ float s_w[RED_NT / 32];
+  float m = 0.0f;
+  for (size_t k = (size_t)blockIdx.x * RED_NT + threadIdx.x; k < n; k += (size_t)gridDim.x * RED_NT) {
+    const float v = column_depth(h[k], w[k], d[k], dx);
+    m = v > m ? v : m;
+  }
+  block_max_to<RED_NT>(m, key, s_w);
+}
+
 // hllc.py:948-966 _reduce_wavespeed into a zeroed slot.
 __global__ void __launch_bounds__(RED_NT) wavespeed_kernel(const float* __restrict__ h, const float* __restrict__ hu,
                                                             const float* __restrict__ hv, size_t n,
@@ -40,6 +53,14 @@ __global__ void zero_key_kernel(unsigned int* key) { *key = 0u; }
 cudaError_t reduce_max_h(const float* h, size_t n, unsigned int* key, cudaStream_t s) {
   zero_key_kernel<<<1, 1, 0, s>>>(key);
   max_h_kernel<<<WS_SUM_BLOCKS, RED_NT, 0, s>>>(h, n, key);
+  return cudaGetLastError();
+}
+
+cudaError_t reduce_max_column(const float* h, const float* w, const float* d, float dx32, size_t n,
+                              unsigned int* key, cudaStream_t s) {
+  if (w == nullptr) return reduce_max_h(h, n, key, s);
+  zero_key_kernel<<<1, 1, 0, s>>>(key);
+  max_column_kernel<<<WS_SUM_BLOCKS, RED_NT, 0, s>>>(h, w, d, dx32, n, key);
   return cudaGetLastError();
 }
 

@@ -125,6 +125,9 @@ static int li_params(const rb_li_fields* f, void* ws, rb::LiParams& p, const cha
     return fail(RB_ERR_ARG, "%s: missing state buffer", who);
   if (f->d50 && (!f->qs_int_x || !f->qs_comp_x || !f->qs_int_y || !f->qs_comp_y))
     return fail(RB_ERR_ARG, "%s: d50 given without the transport accumulators", who);
+  if (f->chan_w && (!f->chan_d || !f->chan_n || !f->qx_ch[0] || !f->qx_ch[1] || !f->qx_fp[0] || !f->qx_fp[1] ||
+                    !f->qy_ch[0] || !f->qy_ch[1] || !f->qy_fp[0] || !f->qy_fp[1]))
+    return fail(RB_ERR_ARG, "%s: chan_w given without the channel depth, roughness or face components", who);
   const bool banks = f->infil != nullptr || any_bc(f->bc, RB_BC_OPEN);
   p = rb::LiParams{};
   p.ny = f->ny;
@@ -146,6 +149,17 @@ static int li_params(const rb_li_fields* f, void* ws, rb::LiParams& p, const cha
   p.qs_comp_x = f->qs_comp_x;
   p.qs_int_y = f->qs_int_y;
   p.qs_comp_y = f->qs_comp_y;
+  if (f->chan_w != nullptr) {
+    p.cw = f->chan_w;
+    p.cd = f->chan_d;
+    p.cn = f->chan_n;
+    for (int b = 0; b < 2; b++) {
+      p.qxcb[b] = f->qx_ch[b];
+      p.qxfb[b] = f->qx_fp[b];
+      p.qycb[b] = f->qy_ch[b];
+      p.qyfb[b] = f->qy_fp[b];
+    }
+  }
   p.ledger = banks ? (double*)((char*)ws + rb::WS_LEDGER) : nullptr;
   p.err = &header(ws)->err;
   return RB_OK;
@@ -168,44 +182,17 @@ int rb_li_step(const rb_li_fields* f, int32_t cur, const rb_step_args* a, void* 
   if ((rc = check_bc(f->bc, false, "rb_li_step"))) return rc;
   if ((rc = check_dt(a->dt, "rb_li_step"))) return rc;
   if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_li_step: cur must be 0 or 1");
-  if (!f->h[0] || !f->h[1] || !f->qx[0] || !f->qx[1] || !f->qy[0] || !f->qy[1] || !f->z || !f->n)
-    return fail(RB_ERR_ARG, "rb_li_step: missing state buffer");
-  if (f->d50 && (!f->qs_int_x || !f->qs_comp_x || !f->qs_int_y || !f->qs_comp_y))
-    return fail(RB_ERR_ARG, "rb_li_step: d50 given without the transport accumulators");
-  const bool banks = f->infil != nullptr || any_bc(f->bc, RB_BC_OPEN);
-
-  rb::LiParams p{};
-  p.ny = f->ny;
-  p.nx = f->nx;
-  p.dx32 = (float)f->dx;
+  rb::LiParams p;
+  if ((rc = li_params(f, ws, p, "rb_li_step"))) return rc;
   p.dt32 = (float)a->dt;
-  const bool comp = f->h_comp != nullptr;
-  p.rain_cont = comp ? 0.0f : (float)a->rain;  // local_inertial.py:697
+  p.rain_cont = f->h_comp != nullptr ? 0.0f : (float)a->rain;  // local_inertial.py:697
   p.rain32 = (float)a->rain;
   p.scale32 = (float)a->rain_scale;
   p.dxdt = (float)(a->dt / f->dx);  // boundaries.py:329
   p.limit = a->limit ? 1 : 0;
-  for (int e = 0; e < 4; e++) p.bc[e] = f->bc[e];
-  for (int b = 0; b < 2; b++) {
-    p.hb[b] = f->h[b];
-    p.qxb[b] = f->qx[b];
-    p.qyb[b] = f->qy[b];
-  }
   p.cur = cur;
-  p.z = f->z;
-  p.n = f->n;
   p.clk = nullptr;
-  p.h_comp = f->h_comp;
-  p.rain_field = f->rain_field;
-  p.infil = f->infil;
-  p.d50 = f->d50;
-  p.qs_int_x = f->qs_int_x;
-  p.qs_comp_x = f->qs_comp_x;
-  p.qs_int_y = f->qs_int_y;
-  p.qs_comp_y = f->qs_comp_y;
-  p.ledger = banks ? (double*)((char*)ws + rb::WS_LEDGER) : nullptr;
   p.hmax_key = nullptr;
-  p.err = &header(ws)->err;
   RB_CUDA(rb::li_step_launch(p, (cudaStream_t)stream), "rb_li_step launch");
   return RB_OK;
 }
@@ -218,7 +205,10 @@ int rb_li_compute_dt(const rb_li_fields* f, int32_t cur, double alpha, double dt
   if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_li_compute_dt: cur must be 0 or 1");
   cudaStream_t s = (cudaStream_t)stream;
   unsigned int* key = &header(ws)->red_key;
-  RB_CUDA(rb::reduce_max_h(f->h[cur], (size_t)f->ny * f->nx, key, s), "rb_li_compute_dt reduce");
+  if (f->chan_w && !f->chan_d) return fail(RB_ERR_ARG, "rb_li_compute_dt: chan_w given without chan_d");
+  // local_inertial.py:529-539: the water column with channels armed, else h.
+  RB_CUDA(rb::reduce_max_column(f->h[cur], f->chan_w, f->chan_d, (float)f->dx, (size_t)f->ny * f->nx, key, s),
+          "rb_li_compute_dt reduce");
   unsigned int host_key = 0;
   RB_CUDA(cudaMemcpyAsync(&host_key, key, sizeof host_key, cudaMemcpyDeviceToHost, s), "rb_li_compute_dt copy");
   RB_CUDA(cudaStreamSynchronize(s), "rb_li_compute_dt sync");
@@ -383,7 +373,9 @@ int rb_li_clock_start(const rb_li_fields* f, int32_t cur, const rb_clock_config*
   if (rc) return rc;
   cudaStream_t s = (cudaStream_t)stream;
   if ((rc = clock_start(0, f->ny, f->nx, f->dx, cur, cfg, ws, s))) return rc;
-  RB_CUDA(rb::reduce_max_h(f->h[cur], (size_t)f->ny * f->nx, &header(ws)->clock.red_key, s), "rb_li_clock_start");
+  RB_CUDA(rb::reduce_max_column(f->h[cur], f->chan_w, f->chan_d, (float)f->dx, (size_t)f->ny * f->nx,
+                                &header(ws)->clock.red_key, s),
+          "rb_li_clock_start");
   return RB_OK;
 }
 
@@ -561,6 +553,9 @@ int rb_ensemble_init(rb_ensemble_layout* L, void* ens, const int32_t* scheme, co
     if (scheme[d] == 0) {
       const rb_li_fields& f = li[ili];
       if ((rc = li_params(&f, dom_ws[d], hli[ili], "rb_ensemble_init"))) return rc;
+      if (f.chan_w != nullptr)
+        return fail(RB_ERR_ARG, "rb_ensemble_init: domain %d: sub-grid channels are stepped one domain at a time "
+                    "(rb_li_step / rb_li_enqueue_steps)", d);
       hli[ili].clk = &clocks[d];
       hli[ili].hmax_key = &clocks[d].red_key;
       ny = f.ny, nx = f.nx, dx = f.dx;

@@ -19,6 +19,13 @@
 // the old h, qx, qy while this CTA writes new ones, the step reads buffer [cur]
 // and writes buffer [cur ^ 1].
 //
+// Sub-grid channels (solver/core/channels.py, local_inertial.py:275-500) are a
+// second instantiation (CH = true): eta through the storage curve, each face a
+// floodplain plus a channel component (both double buffered like qx / qy), both
+// scaled by the total flux's donor beta, the two-component bedload capacity, and
+// the water column instead of h for the next dt. The unarmed instantiation does
+// none of it.
+//
 // Per-cell HBM traffic (compulsory): read h, z, n, qx, qy, write h, qx, qy (32 B),
 // + h_comp read/write (8 B) when compensated rain is armed, + rain field / infil
 // reads (4 B each), + d50 and the four transport accumulators (36 B) when
@@ -54,24 +61,84 @@ __device__ __forceinline__ float drain(float h_edge, float q_out, float dxdt) {
   return h_edge - removed;
 }
 
+// friction.py:35-58 manning_denominator_radius (hydraulic radius R = A/P).
+__device__ __forceinline__ float manning_denominator_radius(float q_prev, float h_flow, float radius, float n,
+                                                            float g, float dt) {
+  return 1.0f + g * dt * n * n * fabsf(q_prev) / (h_flow * rb_pow43f(radius));
+}
+
+// local_inertial.py:294-320 _channel_flux with channels.py:120-135: the channel
+// component of a face, per unit channel width.
+__device__ __forceinline__ float channel_flux(float q_prev, float eta_max, float slope, float w_face, float z_bank,
+                                              float z_ch, float n_ch, float dt) {
+  if (w_face <= 0.0f) return 0.0f;
+  const float h_ch = rmin(eta_max, z_bank) - z_ch;
+  if (h_ch < kHDry) return 0.0f;
+  const float radius = w_face * h_ch / (w_face + 2.0f * h_ch);
+  const float num = q_prev - kG * h_ch * dt * slope;
+  const float den = manning_denominator_radius(q_prev, h_ch, radius, n_ch, kG, dt);
+  return num / den;
+}
+
+// local_inertial.py:323-336 _floodplain_flux: the plain face update above the banks.
+__device__ __forceinline__ float floodplain_flux(float q_prev, float eta_max, float slope, float z_bank, float n_fp,
+                                                 float dt) {
+  const float h_fp = eta_max - z_bank;
+  if (h_fp < kHDry) return 0.0f;
+  const float num = q_prev - kG * h_fp * dt * slope;
+  const float den = manning_denominator(q_prev, h_fp, n_fp, kG, dt);
+  return num / den;
+}
+
+// sediment.py:276-305 _combined_capacity: bedload per unit cell width of a
+// two-component face.
+__device__ __forceinline__ float combined_capacity(float q_ch, float q_fp, float eta_max, float z_bank, float z_ch,
+                                                   float w_face, float n_fp, float n_ch, float d50, float dx) {
+  const float h_fp = eta_max - z_bank;
+  const float qs_fp = face_capacity(q_fp, h_fp, h_fp, n_fp, d50);
+  float qs_ch = 0.0f;
+  if (w_face > 0.0f) {
+    const float h_ch = rmin(eta_max, z_bank) - z_ch;
+    if (h_ch >= kHDry) qs_ch = face_capacity(q_ch, h_ch, w_face * h_ch / (w_face + 2.0f * h_ch), n_ch, d50);
+  }
+  const float frac = w_face / dx;
+  return qs_fp * (1.0f - frac) + qs_ch * frac;
+}
+
 template <int TX, int TY>
-struct LiSmem {
+struct LiGeom {
   static constexpr int RW = TX + 4, RH = TY + 4;  // cells: cols x0-2 .. x0+TX+1, rows y0-2 .. y0+TY+1
   static constexpr int XW = TX + 3, XH = TY + 2;  // x-faces: cols x0-1 .. x0+TX+1, rows y0-1 .. y0+TY
   static constexpr int YW = TX + 2, YH = TY + 3;  // y-faces: cols x0-1 .. x0+TX,   rows y0-1 .. y0+TY+1
   static constexpr int BW = TX + 2, BH = TY + 2;  // beta:    cols x0-1 .. x0+TX,   rows y0-1 .. y0+TY
-  float h[RH][RW], z[RH][RW], n[RH][RW], eta[RH][RW];
-  float qx[XH][XW], qy[YH][YW], beta[BH][BW];
+};
+
+// Channel geometry of the halo and the two face components (sub-grid channels only).
+template <int TX, int TY, bool CH>
+struct LiChanSmem {};
+template <int TX, int TY>
+struct LiChanSmem<TX, TY, true> : LiGeom<TX, TY> {
+  using G = LiGeom<TX, TY>;
+  float w[G::RH][G::RW], d[G::RH][G::RW], cn[G::RH][G::RW];
+  float qxc[G::XH][G::XW], qxf[G::XH][G::XW], qyc[G::YH][G::YW], qyf[G::YH][G::YW];
+};
+
+template <int TX, int TY, bool CH = false>
+struct LiSmem : LiGeom<TX, TY> {
+  using G = LiGeom<TX, TY>;
+  float h[G::RH][G::RW], z[G::RH][G::RW], n[G::RH][G::RW], eta[G::RH][G::RW];
+  float qx[G::XH][G::XW], qy[G::YH][G::YW], beta[G::BH][G::BW];
   double red[8];
   float redf[8];
+  LiChanSmem<TX, TY, CH> ch;
 };
 
 // One CTA-wide tile of the step: tile (bx, by) of domain p, ledger slot `slot`.
 // Called by every thread of the block; returns uniformly.
-template <int TX, int TY, int NT>
-__device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_t slot, LiSmem<TX, TY>& S) {
+template <int TX, int TY, int NT, bool CH = false>
+__device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_t slot, LiSmem<TX, TY, CH>& S) {
   static_assert(NT / 32 <= 8, "reduction scratch sized for <= 8 warps");
-  using SM = LiSmem<TX, TY>;
+  using SM = LiSmem<TX, TY, CH>;
   constexpr int RW = SM::RW, RH = SM::RH, XW = SM::XW, XH = SM::XH, YW = SM::YW, YH = SM::YH;
   constexpr int BW = SM::BW, BH = SM::BH;
   auto& s_h = S.h;
@@ -112,9 +179,10 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
   for (int k = threadIdx.x; k < RH * RW; k += NT) {
     const int r = k / RW, c = k - r * RW;
     const int gi = y0 - 2 + r, gj = x0 - 2 + c;
-    float h = 0.0f, z = 0.0f, n = 0.0f;
-    if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
-      const size_t id = (size_t)gi * nx + gj;
+    float h = 0.0f, z = 0.0f, n = 0.0f, w = 0.0f, d = 0.0f, cn = 0.0f;
+    const bool in = gi >= 0 && gi < ny && gj >= 0 && gj < nx;
+    const size_t id = in ? (size_t)gi * nx + gj : 0;
+    if (in) {
       h = h_in[id];
       z = p.z[id];
       n = p.n[id];
@@ -122,7 +190,19 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
     s_h[r][c] = h;
     s_z[r][c] = z;
     s_n[r][c] = n;
-    s_eta[r][c] = h + z;
+    if constexpr (CH) {  // local_inertial.py:278-291 compute_eta_channels
+      if (in) {
+        w = p.cw[id];
+        d = p.cd[id];
+        cn = p.cn[id];
+      }
+      S.ch.w[r][c] = w;
+      S.ch.d[r][c] = d;
+      S.ch.cn[r][c] = cn;
+      s_eta[r][c] = eta_subgrid(h, z, w, d, dx);
+    } else {
+      s_eta[r][c] = h + z;
+    }
   }
   __syncthreads();
 
@@ -132,17 +212,38 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
     const int a = k / XW, b = k - a * XW;
     const int gi = y0 - 1 + a, gj = x0 - 1 + b;
     float q = 0.0f;
-    if (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1) {
-      const float eta_l = s_eta[a + 1][b], eta_r = s_eta[a + 1][b + 1];
-      const float h_flow = rmax(eta_l, eta_r) - rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
-      if (!(h_flow < kHDry)) {
-        const float qo = qx_in[(size_t)gi * (nx + 1) + gj];
-        const float n_face = 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]);
-        const float slope = (eta_r - eta_l) / dx;
-        const float num = qo - kG * h_flow * dt * slope;
-        const float den = manning_denominator(qo, h_flow, n_face, kG, dt);
-        q = num / den;
+    if constexpr (!CH) {
+      if (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1) {
+        const float eta_l = s_eta[a + 1][b], eta_r = s_eta[a + 1][b + 1];
+        const float h_flow = rmax(eta_l, eta_r) - rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
+        if (!(h_flow < kHDry)) {
+          const float qo = qx_in[(size_t)gi * (nx + 1) + gj];
+          const float n_face = 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]);
+          const float slope = (eta_r - eta_l) / dx;
+          const float num = qo - kG * h_flow * dt * slope;
+          const float den = manning_denominator(qo, h_flow, n_face, kG, dt);
+          q = num / den;
+        }
       }
+    } else {  // local_inertial.py:338-384 update_qx_channels
+      float qc = 0.0f, qf = 0.0f;
+      if (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1) {
+        const int r = a + 1, cl = b, cr = b + 1;
+        const float eta_l = s_eta[r][cl], eta_r = s_eta[r][cr];
+        const float eta_max = rmax(eta_l, eta_r);
+        const float slope = (eta_r - eta_l) / dx;
+        const float z_bank = rmax(s_z[r][cl], s_z[r][cr]);
+        const size_t fid = (size_t)gi * (nx + 1) + gj;
+        qf = floodplain_flux(p.qxfb[cur][fid], eta_max, slope, z_bank, 0.5f * (s_n[r][cl] + s_n[r][cr]), dt);
+        const float w_face = rmin(S.ch.w[r][cl], S.ch.w[r][cr]);
+        const float z_ch = rmax(s_z[r][cl] - S.ch.d[r][cl], s_z[r][cr] - S.ch.d[r][cr]);
+        qc = channel_flux(p.qxcb[cur][fid], eta_max, slope, w_face, z_bank, z_ch,
+                          0.5f * (S.ch.cn[r][cl] + S.ch.cn[r][cr]), dt);
+        const float frac = w_face / dx;
+        q = qf * (1.0f - frac) + qc * frac;
+      }
+      S.ch.qxc[a][b] = qc;
+      S.ch.qxf[a][b] = qf;
     }
     s_qx[a][b] = q;
   }
@@ -150,17 +251,38 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
     const int a = k / YW, b = k - a * YW;
     const int gi = y0 - 1 + a, gj = x0 - 1 + b;
     float q = 0.0f;
-    if (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx) {
-      const float eta_t = s_eta[a][b + 1], eta_b = s_eta[a + 1][b + 1];
-      const float h_flow = rmax(eta_t, eta_b) - rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
-      if (!(h_flow < kHDry)) {
-        const float qo = qy_in[(size_t)gi * nx + gj];
-        const float n_face = 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]);
-        const float slope = (eta_b - eta_t) / dx;
-        const float num = qo - kG * h_flow * dt * slope;
-        const float den = manning_denominator(qo, h_flow, n_face, kG, dt);
-        q = num / den;
+    if constexpr (!CH) {
+      if (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx) {
+        const float eta_t = s_eta[a][b + 1], eta_b = s_eta[a + 1][b + 1];
+        const float h_flow = rmax(eta_t, eta_b) - rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
+        if (!(h_flow < kHDry)) {
+          const float qo = qy_in[(size_t)gi * nx + gj];
+          const float n_face = 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]);
+          const float slope = (eta_b - eta_t) / dx;
+          const float num = qo - kG * h_flow * dt * slope;
+          const float den = manning_denominator(qo, h_flow, n_face, kG, dt);
+          q = num / den;
+        }
       }
+    } else {  // local_inertial.py:387-427 update_qy_channels
+      float qc = 0.0f, qf = 0.0f;
+      if (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx) {
+        const int c = b + 1, rt = a, rb = a + 1;
+        const float eta_t = s_eta[rt][c], eta_b = s_eta[rb][c];
+        const float eta_max = rmax(eta_t, eta_b);
+        const float slope = (eta_b - eta_t) / dx;
+        const float z_bank = rmax(s_z[rt][c], s_z[rb][c]);
+        const size_t fid = (size_t)gi * nx + gj;
+        qf = floodplain_flux(p.qyfb[cur][fid], eta_max, slope, z_bank, 0.5f * (s_n[rt][c] + s_n[rb][c]), dt);
+        const float w_face = rmin(S.ch.w[rt][c], S.ch.w[rb][c]);
+        const float z_ch = rmax(s_z[rt][c] - S.ch.d[rt][c], s_z[rb][c] - S.ch.d[rb][c]);
+        qc = channel_flux(p.qycb[cur][fid], eta_max, slope, w_face, z_bank, z_ch,
+                          0.5f * (S.ch.cn[rt][c] + S.ch.cn[rb][c]), dt);
+        const float frac = w_face / dx;
+        q = qf * (1.0f - frac) + qc * frac;
+      }
+      S.ch.qyc[a][b] = qc;
+      S.ch.qyf[a][b] = qf;
     }
     s_qy[a][b] = q;
   }
@@ -190,10 +312,17 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
       const int gj = x0 - 1 + b;
       if (gj >= 1 && gj <= nx - 1) {
         const float q = s_qx[a][b];
-        if (q > 0.0f)
-          s_qx[a][b] = q * s_beta[a][b - 1];
-        else if (q < 0.0f)
-          s_qx[a][b] = q * s_beta[a][b];
+        if constexpr (!CH) {
+          if (q > 0.0f)
+            s_qx[a][b] = q * s_beta[a][b - 1];
+          else if (q < 0.0f)
+            s_qx[a][b] = q * s_beta[a][b];
+        } else if (!(q == 0.0f)) {  // local_inertial.py:430-452 limit_qx_channels
+          const float bb = q < 0.0f ? s_beta[a][b] : s_beta[a][b - 1];
+          s_qx[a][b] = q * bb;
+          S.ch.qxc[a][b] = S.ch.qxc[a][b] * bb;
+          S.ch.qxf[a][b] = S.ch.qxf[a][b] * bb;
+        }
       }
     }
     for (int k = threadIdx.x; k < (TY + 1) * TX; k += NT) {
@@ -201,10 +330,17 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
       const int gi = y0 - 1 + a;
       if (gi >= 1 && gi <= ny - 1) {
         const float q = s_qy[a][b];
-        if (q > 0.0f)
-          s_qy[a][b] = q * s_beta[a - 1][b];
-        else if (q < 0.0f)
-          s_qy[a][b] = q * s_beta[a][b];
+        if constexpr (!CH) {
+          if (q > 0.0f)
+            s_qy[a][b] = q * s_beta[a - 1][b];
+          else if (q < 0.0f)
+            s_qy[a][b] = q * s_beta[a][b];
+        } else if (!(q == 0.0f)) {  // local_inertial.py:455-472 limit_qy_channels
+          const float bb = q < 0.0f ? s_beta[a][b] : s_beta[a - 1][b];
+          s_qy[a][b] = q * bb;
+          S.ch.qyc[a][b] = S.ch.qyc[a][b] * bb;
+          S.ch.qyf[a][b] = S.ch.qyf[a][b] * bb;
+        }
       }
     }
     __syncthreads();
@@ -218,7 +354,23 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
     const size_t fid = (size_t)gi * (nx + 1) + gj;
     const float q = s_qx[a][b];
     qx_out[fid] = q;
-    if (p.d50 != nullptr && gj >= 1 && gj <= nx - 1) {
+    if constexpr (CH) {
+      p.qxcb[cur ^ 1][fid] = S.ch.qxc[a][b];
+      p.qxfb[cur ^ 1][fid] = S.ch.qxf[a][b];
+      if (p.d50 != nullptr && gj >= 1 && gj <= nx - 1) {  // sediment.py:308-342
+        const int r = a + 1, cl = b, cr = b + 1;
+        const size_t ci = (size_t)gi * nx + gj - 1;
+        const float qs = combined_capacity(
+            S.ch.qxc[a][b], S.ch.qxf[a][b], rmax(s_eta[r][cl], s_eta[r][cr]), rmax(s_z[r][cl], s_z[r][cr]),
+            rmax(s_z[r][cl] - S.ch.d[r][cl], s_z[r][cr] - S.ch.d[r][cr]), rmin(S.ch.w[r][cl], S.ch.w[r][cr]),
+            0.5f * (s_n[r][cl] + s_n[r][cr]), 0.5f * (S.ch.cn[r][cl] + S.ch.cn[r][cr]),
+            0.5f * (p.d50[ci] + p.d50[ci + 1]), dx);
+        float tot = p.qs_int_x[fid], comp = p.qs_comp_x[fid];
+        kahan_add(tot, comp, qs * dt);
+        p.qs_int_x[fid] = tot;
+        p.qs_comp_x[fid] = comp;
+      }
+    } else if (p.d50 != nullptr && gj >= 1 && gj <= nx - 1) {
       const float eta_max = rmax(s_eta[a + 1][b], s_eta[a + 1][b + 1]);
       const float z_bank = rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
       const float h_face = eta_max - z_bank;
@@ -238,7 +390,22 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
     const size_t fid = (size_t)gi * nx + gj;
     const float q = s_qy[a][b];
     qy_out[fid] = q;
-    if (p.d50 != nullptr && gi >= 1 && gi <= ny - 1) {
+    if constexpr (CH) {
+      p.qycb[cur ^ 1][fid] = S.ch.qyc[a][b];
+      p.qyfb[cur ^ 1][fid] = S.ch.qyf[a][b];
+      if (p.d50 != nullptr && gi >= 1 && gi <= ny - 1) {  // sediment.py:345-377
+        const int c = b + 1, rt = a, rb = a + 1;
+        const float qs = combined_capacity(
+            S.ch.qyc[a][b], S.ch.qyf[a][b], rmax(s_eta[rt][c], s_eta[rb][c]), rmax(s_z[rt][c], s_z[rb][c]),
+            rmax(s_z[rt][c] - S.ch.d[rt][c], s_z[rb][c] - S.ch.d[rb][c]), rmin(S.ch.w[rt][c], S.ch.w[rb][c]),
+            0.5f * (s_n[rt][c] + s_n[rb][c]), 0.5f * (S.ch.cn[rt][c] + S.ch.cn[rb][c]),
+            0.5f * (p.d50[fid - nx] + p.d50[fid]), dx);
+        float tot = p.qs_int_y[fid], comp = p.qs_comp_y[fid];
+        kahan_add(tot, comp, qs * dt);
+        p.qs_int_y[fid] = tot;
+        p.qs_comp_y[fid] = comp;
+      }
+    } else if (p.d50 != nullptr && gi >= 1 && gi <= ny - 1) {
       const float eta_max = rmax(s_eta[a][b + 1], s_eta[a + 1][b + 1]);
       const float z_bank = rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
       const float h_face = eta_max - z_bank;
@@ -305,7 +472,12 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
       loss += (double)avail - (double)h;
     }
     h_out[id] = h;
-    hmax = h > hmax ? h : hmax;
+    if constexpr (CH) {  // local_inertial.py:475-489: the water column sets the next dt
+      const float col = column_depth(h, S.ch.w[r + 2][c + 2], S.ch.d[r + 2][c + 2], dx);
+      hmax = col > hmax ? col : hmax;
+    } else {
+      hmax = h > hmax ? h : hmax;
+    }
     bad |= !(fabsf(h) <= FLT_MAX);
   }
 
@@ -318,16 +490,19 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
   __syncthreads();  // the shared tile is reused by the caller's next tile
 }
 
-template <int TX, int TY, int NT>
+template <int TX, int TY, int NT, bool CH>
 __global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
-  __shared__ LiSmem<TX, TY> S;
-  li_tile<TX, TY, NT>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S);
+  __shared__ LiSmem<TX, TY, CH> S;
+  li_tile<TX, TY, NT, CH>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
 
 template <int TX, int TY, int NT>
 static cudaError_t launch_li(const LiParams& p, cudaStream_t s) {
   const dim3 grid((p.nx + TX - 1) / TX, (p.ny + TY - 1) / TY);
-  li_step_kernel<TX, TY, NT><<<grid, NT, 0, s>>>(p);
+  if (p.cw != nullptr)
+    li_step_kernel<TX, TY, NT, true><<<grid, NT, 0, s>>>(p);
+  else
+    li_step_kernel<TX, TY, NT, false><<<grid, NT, 0, s>>>(p);
   return cudaGetLastError();
 }
 

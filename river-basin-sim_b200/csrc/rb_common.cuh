@@ -31,6 +31,32 @@ __device__ __forceinline__ void kahan_add(float& total, float& comp, float inc) 
   total = t;
 }
 
+// channels.py:58-70 eta_subgrid: the storage curve h -> eta.
+__device__ __forceinline__ float eta_subgrid(float h, float z, float w, float d, float dx) {
+  float eta = h + z;
+  if (w > 0.0f && d > 0.0f) {
+    const float h_bf = w * d / dx;
+    if (h <= h_bf)
+      eta = z - d + h * dx / w;
+    else
+      eta = z + (h - h_bf);
+  }
+  return eta;
+}
+
+// channels.py:73-83 column_depth: the water column that sets the wave speed.
+__device__ __forceinline__ float column_depth(float h, float w, float d, float dx) {
+  float col = h;
+  if (w > 0.0f && d > 0.0f) {
+    const float h_bf = w * d / dx;
+    if (h <= h_bf)
+      col = h * dx / w;
+    else
+      col = d + (h - h_bf);
+  }
+  return col;
+}
+
 // friction.py:18-31 manning_denominator
 __device__ __forceinline__ float manning_denominator(float q_prev, float h_flow, float n, float g, float dt) {
   return 1.0f + g * dt * n * n * fabsf(q_prev) / rb_pow73f(h_flow);

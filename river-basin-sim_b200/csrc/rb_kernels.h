@@ -70,8 +70,11 @@ struct LiParams {
   const float *rain_field, *infil;
   const float *d50;
   float *qs_int_x, *qs_comp_x, *qs_int_y, *qs_comp_y;
+  const float *cw, *cd, *cn;           // sub-grid channel geometry, or null (unarmed)
+  float *qxcb[2], *qxfb[2];            // channel / floodplain x-face components, double buffered
+  float *qycb[2], *qyfb[2];
   double *ledger;          // 2 doubles per tile, or null when nothing is banked
-  unsigned int *hmax_key;  // fused max(h_new) for the next dt, or null
+  unsigned int *hmax_key;  // fused max(h_new) (water column with channels) for the next dt, or null
   unsigned int *err;
 };
 
@@ -137,6 +140,9 @@ size_t ws_hllc_bytes(int ny, int nx);
 size_t ws_hllc_u1_offset(int ny, int nx);
 
 cudaError_t reduce_max_h(const float* h, size_t n, unsigned int* key, cudaStream_t s);
+// Max of the water column (channels.py:73-83) when w is set, else of h.
+cudaError_t reduce_max_column(const float* h, const float* w, const float* d, float dx32, size_t n,
+                              unsigned int* key, cudaStream_t s);
 cudaError_t reduce_wavespeed(const float* h, const float* hu, const float* hv, size_t n, unsigned int* key,
                              cudaStream_t s);
 cudaError_t sum_f64(const float* x, size_t n, double* partials, double* out, cudaStream_t s);

@@ -35,6 +35,8 @@ class LiFields(ctypes.Structure):
         ("h", _P * 2), ("qx", _P * 2), ("qy", _P * 2), ("z", _P), ("n", _P),
         ("h_comp", _P), ("rain_field", _P), ("infil", _P), ("bc", ctypes.c_int32 * 4),
         ("d50", _P), ("qs_int_x", _P), ("qs_comp_x", _P), ("qs_int_y", _P), ("qs_comp_y", _P),
+        ("chan_w", _P), ("chan_d", _P), ("chan_n", _P),
+        ("qx_ch", _P * 2), ("qx_fp", _P * 2), ("qy_ch", _P * 2), ("qy_fp", _P * 2),
     ]  # fmt: skip
 
 

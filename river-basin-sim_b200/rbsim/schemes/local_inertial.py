@@ -15,6 +15,9 @@ from ..state import State
 def compute_dt(state: State, alpha: float = 0.7, dt_max: float = 30.0) -> float:
     """``dt = alpha dx / sqrt(g h_max)``, ``dt_max`` when ``h_max <= H_DRY`` (:515-544).
 
+    With sub-grid channels armed, ``h_max`` is the deepest water column
+    (channels.column_depth), which is what the wave speed sees.
+
     Synchronising: the max-depth reduction runs on the device and its one float
     is read back, as the reference reads ``h_max`` back every step.
     """
@@ -31,10 +34,9 @@ def step(state: State, dt: float, rain: float = 0.0, limit: bool = True, rain_sc
 
     ``rain`` is the uniform rate (m/s), ``rain_scale`` gates ``state.rain`` (the
     field), ``limit`` the donor limiter. Optional physics (compensation, rain
-    field, infiltration, open edges, morphology) runs when armed on the state.
+    field, infiltration, open edges, morphology, sub-grid channels) runs when
+    armed on the state.
     """
-    if state.channels is not None:
-        raise NotImplementedError("sub-grid channels are outside this build's solver path")
     args = _lib.StepArgs(float(dt), float(rain), float(rain_scale), 1 if limit else 0, 0)
     _lib.check(_lib.lib().rb_li_step(ctypes.byref(state.li_fields()), state.cur, ctypes.byref(args),
                                      state.workspace.data_ptr(), state.stream))  # fmt: skip

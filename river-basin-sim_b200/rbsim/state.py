@@ -137,7 +137,7 @@ class State:
         self.infil: torch.Tensor | None = None
         self.rain: torch.Tensor | None = None
         self.sediment: SedimentState | None = None
-        self.channels = None  # sub-grid channels are not part of this build's path
+        self.channels = None  # ChannelState once sub-grid channels are armed (channels.arm_channels)
         self.hllc = None  # set by the HLLC scheme when armed (marker only)
         self.boundaries = {e: "closed" for e in EDGES}
         self.open_edges: frozenset[str] = frozenset()
@@ -227,6 +227,27 @@ class State:
             self.h_comp = torch.zeros(self.grid.shape, dtype=torch.float32, device=self.device)
             self._invalidate()
 
+    def arm_channel_fields(self, w: np.ndarray, d: np.ndarray, n: np.ndarray):
+        """Device side of channels.arm_channels (geometry already validated there):
+        the geometry fields and the four double-buffered face components, zeroed."""
+        from .channels import ChannelState
+
+        g, dev = self.grid, self.device
+        has = w > 0
+        pairs = {
+            "qx_ch": _Pair(torch.zeros(g.qx_shape, dtype=torch.float32, device=dev)),
+            "qx_fp": _Pair(torch.zeros(g.qx_shape, dtype=torch.float32, device=dev)),
+            "qy_ch": _Pair(torch.zeros(g.qy_shape, dtype=torch.float32, device=dev)),
+            "qy_fp": _Pair(torch.zeros(g.qy_shape, dtype=torch.float32, device=dev)),
+        }
+        self.channels = ChannelState(
+            w=_f32(w, g.shape, dev), d=_f32(d, g.shape, dev), n=_f32(n, g.shape, dev),
+            width_max=float(w.max()), depth_max=float(d.max()), channel_cells=int(has.sum()),
+            _state=self, _pairs=pairs,
+        )  # fmt: skip
+        self._invalidate()
+        return self.channels
+
     def arm_loss_accumulator(self) -> None:
         self._loss_armed = True
 
@@ -311,6 +332,12 @@ class State:
                 _ptr(sed.qs_comp_x) if sed else None, _ptr(sed.qs_int_y) if sed else None,
                 _ptr(sed.qs_comp_y) if sed else None,
             )  # fmt: skip
+            ch = self.channels
+            if ch is not None:
+                f = self._fields_cache
+                f.chan_w, f.chan_d, f.chan_n = ch.w.data_ptr(), ch.d.data_ptr(), ch.n.data_ptr()
+                for key in ("qx_ch", "qx_fp", "qy_ch", "qy_fp"):
+                    setattr(f, key, (ctypes.c_void_p * 2)(*[t.data_ptr() for t in ch._pairs[key].bufs]))
         return self._fields_cache
 
     def hllc_fields(self) -> _lib.HllcFields:

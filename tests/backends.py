@@ -42,6 +42,12 @@ class OracleBackend:
     def set_bc(self, st, bc, curves=None):
         st.set_open_boundaries(bc, curves)
 
+    def arm_channels(self, st, w, d, n=None):
+        st.arm_channels(w, d, n)
+
+    def channel_n(self, st):
+        return st.channels.n.copy()
+
     def compute_dt(self, st, scheme, alpha, dt_max):
         return self.o.SCHEMES[scheme][0](st, alpha, dt_max)
 
@@ -142,6 +148,14 @@ class GpuBackend:
 
     def set_bc(self, st, bc, curves=None):
         st.set_open_boundaries(bc, curves)
+
+    def arm_channels(self, st, w, d, n=None):
+        from rbsim.channels import arm_channels
+
+        arm_channels(st, w, d, n)
+
+    def channel_n(self, st):
+        return st.channels.n.cpu().numpy()
 
     def compute_dt(self, st, scheme, alpha, dt_max):
         return self.rb.get_scheme(scheme).compute_dt(st, alpha=alpha, dt_max=dt_max)

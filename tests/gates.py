@@ -447,4 +447,179 @@ def gate_inflow_closed_basin(be):
     assert led.max_rel_error < MASS_GATE and rec.inflow_cum > 0.0
 
 
+# --- sub-grid channels ------------------------------------------------------- #
+_EAST_OPEN = {"east": "open", "west": "closed", "north": "closed", "south": "closed"}
+
+
+def _slope_bed(ny, nx, dx, slope, base=5.0):
+    xx = np.broadcast_to(np.arange(nx), (ny, nx))
+    return ((nx - 1 - xx) * dx * slope + base).astype(np.float32)
+
+
+def normal_depth(discharge, width, slope, manning):
+    """Manning normal depth of a rectangular section, R = A/P (bisection on Q(h))."""
+
+    def q_of(h):
+        area = width * h
+        return area * (area / (width + 2.0 * h)) ** (2.0 / 3.0) * math.sqrt(slope) / manning
+
+    lo, hi = 1e-6, 100.0
+    for _ in range(200):
+        mid = 0.5 * (lo + hi)
+        if q_of(mid) < discharge:
+            lo = mid
+        else:
+            hi = mid
+    return 0.5 * (lo + hi)
+
+
+def _run_steady(be, st, inflows, steps, dt_max):
+    inj = be.injector(inflows, st)
+    led = be.ledger(st)
+    t = 0.0
+    for _ in range(steps):
+        dt = be.compute_dt(st, LI, 0.7, dt_max)
+        led.add_inflow(inj.apply(st, t, dt))
+        be.step(st, LI, dt)
+        t += dt
+    led.record(st, t)
+    return led
+
+
+def gate_channels_zero_width_is_m1_bitwise(be):
+    """solver/core/test_channels.py:162 -- w = 0 channels reproduce the plain scheme bit for bit."""
+    ny, nx, dx = 8, 24, 40.0
+    bed = _slope_bed(ny, nx, dx, 0.004)
+    plain = be.make(bed, dx, depth=0.05, manning=0.03)
+    armed = be.make(bed, dx, depth=0.05, manning=0.03)
+    be.arm_channels(armed, np.zeros((ny, nx), np.float32), np.zeros((ny, nx), np.float32))
+    for _ in range(60):
+        dt_p = be.compute_dt(plain, LI, 0.7, 5.0)
+        dt_a = be.compute_dt(armed, LI, 0.7, 5.0)
+        assert dt_p == dt_a
+        be.step(plain, LI, dt_p, rain=1e-5)
+        be.step(armed, LI, dt_a, rain=1e-5)
+    np.testing.assert_array_equal(be.h(armed), be.h(plain))
+    np.testing.assert_array_equal(be.qx(armed), be.qx(plain))
+    np.testing.assert_array_equal(be.qy(armed), be.qy(plain))
+
+
+def gate_channels_dt_sees_the_water_column(be):
+    """test_channels.py:187 -- in-bank the CFL depth is h dx / w, not h."""
+    ny, nx, dx = 4, 8, 200.0
+    w, d, h0 = 20.0, 3.0, 0.05
+    bed = np.full((ny, nx), 10.0, np.float32)
+    plain = be.make(bed, dx, depth=h0, manning=0.035)
+    armed = be.make(bed, dx, depth=h0, manning=0.035)
+    be.arm_channels(armed, np.full((ny, nx), w, np.float32), np.full((ny, nx), d, np.float32))
+    dt_plain = be.compute_dt(plain, LI, 0.7, 1e6)
+    dt_armed = be.compute_dt(armed, LI, 0.7, 1e6)
+    assert abs(dt_plain / (0.7 * dx / math.sqrt(9.81 * h0)) - 1.0) < 1e-5
+    assert abs(dt_armed / (0.7 * dx / math.sqrt(9.81 * h0 * dx / w)) - 1.0) < 1e-5
+    assert dt_armed < dt_plain / 3.0
+
+
+def gate_channels_default_roughness_is_the_floodplain(be):
+    """test_channels.py:146 -- arming without a roughness field uses the cell's n."""
+    bed = np.full((6, 10), 10.0, np.float32)
+    st = be.make(bed, 50.0, depth=0.0, manning=0.035)
+    be.arm_channels(st, np.full((6, 10), 8.0, np.float32), np.full((6, 10), 1.5, np.float32))
+    np.testing.assert_array_equal(be.channel_n(st), np.full((6, 10), np.float32(0.035)))
+
+
+def gate_channels_closed_box_mass(be):
+    """test_channels.py:203 -- a closed channelled bowl conserves volume (rel < 1e-6)."""
+    ny, nx, dx = 10, 20, 50.0
+    yy, xx = np.mgrid[0:ny, 0:nx]
+    bed = (20.0 + 0.02 * ((yy - ny / 2) ** 2 + (xx - nx / 2) ** 2)).astype(np.float32)
+    st = be.make(bed, dx, depth=0.2, manning=0.03)
+    w = np.zeros((ny, nx), np.float32)
+    d = np.zeros((ny, nx), np.float32)
+    w[ny // 2, :] = 15.0
+    d[ny // 2, :] = 2.0
+    be.arm_channels(st, w, d)
+    v0 = float(as_f64(be.h(st)).sum())
+    for _ in range(300):
+        be.step(st, LI, be.compute_dt(st, LI, 0.7, 5.0))
+    h = be.h(st)
+    assert np.isfinite(h).all() and h.min() >= -1e-9
+    assert abs(float(as_f64(h).sum()) - v0) / v0 < 1e-6
+
+
+def gate_subgrid_channel_normal_depth(be):
+    """validation/test_subgrid_channel.py:100 -- a 20 m channel in 50 m cells settles at the
+    Manning normal depth of its own section (within 5 %), mass within the gate."""
+    nx, dx = 100, 50.0
+    slope, n_ch, width, bankfull, discharge = 0.001, 0.03, 20.0, 4.0, 30.0
+    st = be.make(_slope_bed(1, nx, dx, slope), dx, depth=0.0, manning=0.05)
+    be.arm_channels(st, np.full((1, nx), width, np.float32), np.full((1, nx), bankfull, np.float32),
+                    np.full((1, nx), n_ch, np.float32))  # fmt: skip
+    be.set_bc(st, _EAST_OPEN)
+    led = _run_steady(be, st, [((0, 0), [(0.0, discharge), (1.0e9, discharge)])], 3000, 10.0)
+    column = be.h(st)[0] * dx / width
+    median = float(np.median(column[10 : nx - 10]))
+    h_n = normal_depth(discharge, width, slope, n_ch)
+    assert np.isfinite(column).all() and led.max_rel_error < MASS_GATE
+    assert median < bankfull
+    assert abs(median / h_n - 1.0) < 0.05, (median, h_n)
+
+
+def gate_subgrid_channel_overbank_spill(be):
+    """validation/test_subgrid_channel.py:140 -- past bank full water reaches the floodplain;
+    the closed-domain ledger holds."""
+    ny, nx, dx = 7, 30, 50.0
+    st = be.make(_slope_bed(ny, nx, dx, 0.0005), dx, depth=0.0, manning=0.05)
+    row = ny // 2
+    w = np.zeros((ny, nx), np.float32)
+    d = np.zeros((ny, nx), np.float32)
+    w[row, :] = 20.0
+    d[row, :] = 1.0
+    be.arm_channels(st, w, d, np.full((ny, nx), 0.03, np.float32))
+    led = _run_steady(be, st, [((row, 2), [(0.0, 60.0), (1.0e9, 60.0)])], 1200, 5.0)
+    h = be.h(st)
+    h_bf = 20.0 * 1.0 / dx
+    floodplain = np.delete(h, row, axis=0)
+    assert np.isfinite(h).all() and h.min() >= -1e-9
+    assert h[row].max() > h_bf and (floodplain > 1e-3).sum() > 0
+    assert led.max_rel_error < MASS_GATE
+
+
+def gate_subgrid_channel_matches_resolved_reach(be):
+    """validation/test_subgrid_channel.py:177 -- a 100 m-cell sub-grid reach against the same
+    channel resolved at 10 m: each near its own analytical section (10 %), the two depths
+    within 12 % and the stored volumes within 20 %."""
+    length_m, slope, n_ch, width, bankfull, discharge = 2000.0, 0.0008, 0.035, 40.0, 2.0, 40.0
+    dxf = 10.0
+    nyf, nxf = 10, int(length_m / dxf)
+    bed_f = _slope_bed(nyf, nxf, dxf, slope)
+    bed_f[3:7, :] -= bankfull
+    fine = be.make(bed_f, dxf, depth=0.0, manning=n_ch)
+    be.set_bc(fine, _EAST_OPEN)
+    per_cell = discharge / 4.0
+    led_f = _run_steady(be, fine, [((r, 0), [(0.0, per_cell), (1.0e9, per_cell)]) for r in range(3, 7)], 6000, 5.0)
+    dxc = 100.0
+    nxc = int(length_m / dxc)
+    coarse = be.make(_slope_bed(1, nxc, dxc, slope), dxc, depth=0.0, manning=n_ch)
+    be.arm_channels(coarse, np.full((1, nxc), width, np.float32), np.full((1, nxc), bankfull, np.float32),
+                    np.full((1, nxc), n_ch, np.float32))  # fmt: skip
+    be.set_bc(coarse, _EAST_OPEN)
+    led_c = _run_steady(be, coarse, [((0, 0), [(0.0, discharge), (1.0e9, discharge)])], 2000, 10.0)
+
+    def interior(a):
+        k = len(a)
+        return a[k // 5 : -k // 5]
+
+    fine_depth = float(np.median(interior(be.h(fine)[3:7].mean(axis=0))))
+    coarse_depth = float(np.median(interior(be.h(coarse)[0] * dxc / width)))
+    fine_volume = float(as_f64(be.h(fine)).sum()) * dxf * dxf
+    coarse_volume = float(as_f64(be.h(coarse)).sum()) * dxc * dxc
+    h_wide = (discharge / width * n_ch / math.sqrt(slope)) ** 0.6
+    h_section = normal_depth(discharge, width, slope, n_ch)
+    assert led_f.max_rel_error < MASS_GATE and led_c.max_rel_error < MASS_GATE
+    assert abs(fine_depth / h_wide - 1.0) < 0.10, (fine_depth, h_wide)
+    assert abs(coarse_depth / h_section - 1.0) < 0.10, (coarse_depth, h_section)
+    assert abs(coarse_depth / fine_depth - 1.0) < 0.12
+    assert abs(coarse_volume / fine_volume - 1.0) < 0.20
+
+
 GATES = {name[len("gate_"):]: fn for name, fn in sorted(globals().items()) if name.startswith("gate_")}

@@ -10,7 +10,8 @@ Every optional physics branch of the reference step is reached by at least one
 case: the donor limiter, closed/open/fixed_stage edges, compensated and plain
 uniform rain, compensated and plain rain fields, infiltration, inflow point sources
 (compensated), bedload accumulation with Exner activations and bounds, wet/dry
-fronts, dry cells and one-row domains.
+fronts, dry cells, one-row domains and sub-grid channels (in and over bank,
+with and without bedload).
 """
 
 from __future__ import annotations
@@ -106,6 +107,48 @@ def case_li_sediment():
     return dict(scheme="local_inertial", bed=bed, dx=dx, depth=0.5, manning=0.03, qx0=qx0,
                 boundaries=_bc(east="open"), sediment=dict(d50=d50, porosity=0.4, every=10, dz_lo=lo, dz_hi=hi),
                 steps=25, alpha=0.7, dt_max=2.0)  # fmt: skip
+
+
+def _channel_valley(ny, nx, dx, rng):
+    """A down-valley slope with a V cross-section, a sub-grid channel along the
+    valley floor (two rows, one gap), and per-cell channel roughness."""
+    yy, xx = np.mgrid[0:ny, 0:nx].astype(np.float64)
+    mid = (ny - 1) / 2.0
+    bed = (2e-3 * (nx - 1 - xx) * dx + 0.02 * np.abs(yy - mid) * dx + 0.05 * np.sin(0.9 * xx)).astype(np.float32)
+    w = np.zeros((ny, nx), np.float32)
+    d = np.zeros((ny, nx), np.float32)
+    rows = [int(np.floor(mid)), int(np.ceil(mid))]
+    w[rows, :] = rng.uniform(8.0, 20.0, size=(2, nx)).astype(np.float32)
+    d[rows, :] = rng.uniform(0.8, 2.5, size=(2, nx)).astype(np.float32)
+    w[rows[0], nx // 3] = d[rows[0], nx // 3] = 0.0  # a gap: the narrower side controls the face
+    cn = rng.uniform(0.02, 0.04, size=(ny, nx)).astype(np.float32)
+    return bed, w, d, cn
+
+
+def case_li_channels():
+    rng = np.random.default_rng(11)
+    ny, nx, dx = 10, 16, 40.0
+    bed, w, d, cn = _channel_valley(ny, nx, dx, rng)
+    depth = np.full((ny, nx), 0.02, np.float32)
+    depth[:, :4] = 0.9  # spills over bank full upstream, in-bank downstream
+    return dict(scheme="local_inertial", bed=bed, dx=dx, depth=depth, manning=0.045,
+                channels=dict(width=w, depth=d, manning=cn), compensated=True, rain=30.0 / 3.6e6,
+                boundaries=_bc(east="open"), steps=30, alpha=0.7, dt_max=8.0)  # fmt: skip
+
+
+def case_li_channels_sediment():
+    rng = np.random.default_rng(12)
+    ny, nx, dx = 8, 14, 20.0
+    bed, w, d, cn = _channel_valley(ny, nx, dx, rng)
+    bed = bed + (0.01 * dx * np.arange(nx)[::-1]).astype(np.float32)  # steeper: transport above critical
+    d50 = np.full((ny, nx), 0.002, np.float32)
+    lo = np.full((ny, nx), -np.inf, np.float32)
+    hi = np.full((ny, nx), np.inf, np.float32)
+    lo[:, 2:5] = -0.003
+    return dict(scheme="local_inertial", bed=bed, dx=dx, depth=0.4, manning=0.04,
+                channels=dict(width=w, depth=d, manning=cn), boundaries=_bc(east="open"),
+                sediment=dict(d50=d50, porosity=0.4, every=8, dz_lo=lo, dz_hi=hi),
+                steps=24, alpha=0.7, dt_max=2.0)  # fmt: skip
 
 
 def case_li_dambreak_row():

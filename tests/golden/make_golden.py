@@ -29,6 +29,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 class ReferenceAPI:
     def __init__(self):
         from solver.core import hllc, local_inertial
+        from solver.core.channels import arm_channels
         from solver.core.sediment import arm_sediment
         from solver.core.state import State
         from solver.io.config import Inflow
@@ -39,6 +40,7 @@ class ReferenceAPI:
         self.schemes = {"local_inertial": local_inertial, "hllc_fv": hllc}
         self.hllc = hllc
         self.arm_sediment = arm_sediment
+        self.arm_channels = arm_channels
         self.Inflow = Inflow
         self.InflowInjector = InflowInjector
         self.MorphologyProcess = MorphologyProcess
@@ -67,6 +69,9 @@ class ReferenceAPI:
             st.set_open_boundaries(case["boundaries"], case.get("stage_curves"))
         if case.get("sediment"):
             self.arm_sediment(st, case["sediment"]["d50"], case["sediment"]["porosity"])
+        if case.get("channels"):
+            ch = case["channels"]
+            self.arm_channels(st, ch["width"], ch["depth"], ch.get("manning"))
         return st
 
     def compute_dt(self, st, alpha, dt_max):
@@ -103,6 +108,9 @@ class ReferenceAPI:
             for k in ("qs_int_x", "qs_comp_x", "qs_int_y", "qs_comp_y", "dz_cum", "dz_unapplied"):
                 out[k] = getattr(sed, k).numpy().copy()
             out["z"] = st.z.numpy().copy()
+        if st.channels is not None:
+            for k in ("qx_ch", "qx_fp", "qy_ch", "qy_fp"):
+                out[k] = getattr(st.channels, k).numpy().copy()
         return out
 
 

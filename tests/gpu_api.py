@@ -9,6 +9,7 @@ from __future__ import annotations
 import numpy as np
 
 import rbsim
+from rbsim.channels import arm_channels
 from rbsim.grid import Grid
 from rbsim.processes.inflow import Inflow, InflowInjector
 from rbsim.processes.morphology import MorphologyProcess
@@ -40,6 +41,9 @@ class GpuAPI:
             st.set_open_boundaries(case["boundaries"], case.get("stage_curves"))
         if case.get("sediment"):
             arm_sediment(st, case["sediment"]["d50"], case["sediment"]["porosity"])
+        if case.get("channels"):
+            ch = case["channels"]
+            arm_channels(st, ch["width"], ch["depth"], ch.get("manning"))
         return st
 
     def compute_dt(self, st, alpha, dt_max):
@@ -71,5 +75,8 @@ class GpuAPI:
             for k in ("qs_int_x", "qs_comp_x", "qs_int_y", "qs_comp_y", "dz_cum", "dz_unapplied"):
                 out[k] = getattr(sed, k).cpu().numpy()
             out["z"] = st.z.cpu().numpy()
+        if st.channels is not None:
+            for k in ("qx_ch", "qx_fp", "qy_ch", "qy_fp"):
+                out[k] = getattr(st.channels, k).cpu().numpy()
         st.check_device_errors()
         return out

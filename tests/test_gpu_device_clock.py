@@ -30,6 +30,20 @@ def _li_state(n=96, seed=3):
     return st
 
 
+def _li_channel_state(n=96, seed=4):
+    """The LI state above plus a sub-grid channel along the valley rows."""
+    from rbsim.channels import arm_channels
+
+    st = _li_state(n, seed)
+    rng = np.random.default_rng(seed + 100)
+    w = np.zeros((n, n), np.float32)
+    d = np.zeros((n, n), np.float32)
+    w[n // 2 - 1 : n // 2 + 1, :] = rng.uniform(2.0, 8.0, (2, n)).astype(np.float32)
+    d[n // 2 - 1 : n // 2 + 1, :] = rng.uniform(0.5, 1.5, (2, n)).astype(np.float32)
+    arm_channels(st, w, d, np.full((n, n), 0.025, np.float32))
+    return st
+
+
 def _hllc_state(n=80):
     import rbsim
     from rbsim.schemes import hllc
@@ -60,14 +74,15 @@ def _host_run(st, scheme_name, end, every, rain, rain_dur, alpha, dt_max):
     return frames, rain_vol, sched.sync_times
 
 
-@pytest.mark.parametrize("scheme_name", ["local_inertial", "hllc_fv"])
+@pytest.mark.parametrize("scheme_name", ["local_inertial", "local_inertial+channels", "hllc_fv"])
 @pytest.mark.parametrize("graph_steps", [1, 7, 32])
 def test_device_clock_matches_host_scheduler(scheme_name, graph_steps):
     from rbsim.device_clock import DeviceClock
 
-    if scheme_name == "local_inertial":
+    if scheme_name.startswith("local_inertial"):
         end, every, rain, rain_dur, alpha, dt_max = 600.0, 120.0, 30.0 / 3.6e6, 250.0, 0.7, 30.0
-        make = _li_state
+        make = _li_channel_state if scheme_name.endswith("channels") else _li_state
+        scheme_name = "local_inertial"
     else:
         end, every, rain, rain_dur, alpha, dt_max = 6.0, 1.5, 1e-4, 2.0, 0.45, 30.0
         make = _hllc_state

@@ -51,6 +51,9 @@ class OracleAPI:
             st.set_open_boundaries(case["boundaries"], case.get("stage_curves"))
         if case.get("sediment"):
             st.arm_sediment(case["sediment"]["d50"], case["sediment"]["porosity"])
+        if case.get("channels"):
+            ch = case["channels"]
+            st.arm_channels(ch["width"], ch["depth"], ch.get("manning"))
         return st
 
     def compute_dt(self, st, alpha, dt_max):
@@ -90,6 +93,9 @@ class OracleAPI:
             for k in ("qs_int_x", "qs_comp_x", "qs_int_y", "qs_comp_y", "dz_cum", "dz_unapplied"):
                 out[k] = getattr(sed, k).copy()
             out["z"] = st.z.copy()
+        if st.channels is not None:
+            for k in ("qx_ch", "qx_fp", "qy_ch", "qy_fp"):
+                out[k] = getattr(st.channels, k).copy()
         return out
 
 
