@@ -258,6 +258,24 @@ int rb_ensemble_enqueue(const rb_ensemble_layout *L, void *ens, int32_t nsteps, 
 /* Commit and read every domain's clock into out[ndom]. Synchronising. */
 int rb_ensemble_read(const rb_ensemble_layout *L, void *ens, rb_clock_state *out, void *stream);
 
+/* --- a step that allocates nothing ---------------------------------------------
+ * No counterpart in the reference. rb_hllc_step with its scratch in a static
+ * device array inside the library instead of a caller-allocated workspace, for
+ * callers that cannot allocate device memory: hosts whose own allocator owns all
+ * device memory (an embedding engine, a plugin host that forbids allocation after
+ * start-up), a framework whose allocator is frozen while it records a CUDA graph,
+ * or a loop that cannot take cudaMalloc's implicit device synchronisation.
+ * Limit: 1,048,576 cells (e.g. 1024 x 1024); larger grids return RB_ERR_ARG. The
+ * array (~14 MiB) is reserved on every GPU that loads the library until exit.
+ * Every call shares it: the loss ledger and error word are cleared at the start
+ * of each call, and calls that overlap on the GPU race. The first call on a
+ * device looks up the array's address (cudaGetSymbolAddress), so make it before
+ * any stream capture. If loss_out (device, one double) is given, it receives the
+ * depth this step banked through open / fixed_stage edges and infiltration
+ * (metres summed over cells). Calls no allocation routine. */
+int rb_hllc_step_noalloc(const rb_hllc_fields *f, int32_t cur, const rb_step_args *a, double *loss_out,
+                         void *stream);
+
 /* --- diagnostics ------------------------------------------------------------ */
 /* Message of this thread's last failed call (empty if none). Returns its length. */
 int rb_last_error(char *buf, size_t n);

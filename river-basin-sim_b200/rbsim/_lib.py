@@ -122,6 +122,8 @@ SIGNATURES = {
     "rb_ensemble_set_targets": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, _P, _P, _P]),
     "rb_ensemble_enqueue": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, ctypes.c_int32, _P]),
     "rb_ensemble_read": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, _P, _P]),
+    "rb_hllc_step_noalloc": (ctypes.c_int, [ctypes.POINTER(HllcFields), ctypes.c_int32, ctypes.POINTER(StepArgs),
+                                            _P, _P]),
     "rb_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
     "rb_version": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)] * 3),
 }  # fmt: skip
