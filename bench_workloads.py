@@ -197,18 +197,18 @@ def ensemble_256(args):
     sts = fresh()
     rains = [r for _, r, _ in spec]
 
-    def make(li_v, hl_v):
+    def make(li_v, hl_v, t_start, graph_steps=8):
         e = Ensemble(sts, ["local_inertial"] * len(sts), alpha=0.7, dt_max=30.0, sync_times=[[horizon]] * len(sts),
                      rain_rate=rains, rain_until=[horizon] * len(sts), li_variant=li_v, hllc_variant=hl_v,
-                     graph_steps=8)  # fmt: skip
+                     graph_steps=graph_steps, t0=0.0 if t_start is None else t_start)  # fmt: skip
         e.set_targets(horizon)
         return e
 
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    best, timings = autotune(make, probe_replays=1, candidates=[(0, 0), (1, 0), (2, 0)])
-    ens = make(*best)
-    ens.graph_steps = 32
+    # the probe replays are real steps of the run; the batch continues from where they stopped
+    best, timings, t_reached = autotune(make, probe_replays=1, candidates=[(0, 0), (1, 0), (2, 0)])
+    ens = make(*best, t_reached, graph_steps=32)
     replays = ens.run_until(horizon)
     torch.cuda.synchronize()
     batched_wall = time.perf_counter() - t0

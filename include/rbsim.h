@@ -207,6 +207,12 @@ typedef struct rb_clock_state {
  * Not capturable: copies the configuration from host memory. */
 int rb_li_clock_start(const rb_li_fields *f, int32_t cur, const rb_clock_config *cfg, void *ws, void *stream);
 int rb_hllc_clock_start(const rb_hllc_fields *f, int32_t cur, const rb_clock_config *cfg, void *ws, void *stream);
+/* Re-seed compute_dt's reduction from the state in buffer [cur] after something
+ * outside the clocked steps changed it between spans (a reservoir transfer,
+ * solver/processes/reservoir.py:215-263, runs between ticks and the reference's
+ * next compute_dt reads the changed state). Capturable. */
+int rb_li_clock_reseed(const rb_li_fields *f, int32_t cur, void *ws, void *stream);
+int rb_hllc_clock_reseed(const rb_hllc_fields *f, int32_t cur, void *ws, void *stream);
 /* Let the clock run until t_target (a sync time) or max_steps more steps. Capturable. */
 int rb_clock_set_target(void *ws, double t_target, int32_t max_steps, void *stream);
 /* One plan (commit the previous step, plan the next). Capturable. */
@@ -257,6 +263,30 @@ int rb_ensemble_set_targets(const rb_ensemble_layout *L, void *ens, const double
 int rb_ensemble_enqueue(const rb_ensemble_layout *L, void *ens, int32_t nsteps, void *stream);
 /* Commit and read every domain's clock into out[ndom]. Synchronising. */
 int rb_ensemble_read(const rb_ensemble_layout *L, void *ens, rb_clock_state *out, void *stream);
+
+/* --- kernel tuning -------------------------------------------------------------
+ * No counterpart in the reference. A process-wide choice among the HLLC stage
+ * kernel's variants (tile shape, block size, faces per work item, load batching).
+ * Every variant computes bit-identical results; this is a speed knob only, read at
+ * each launch (a captured graph keeps the variant it was captured with). The
+ * library starts with the variant measured fastest on B200 (4: 32 x 32 tiles,
+ * 512 threads). */
+int rb_hllc_set_kernel_variant(int32_t variant);
+int rb_hllc_kernel_variants(int32_t *count);
+
+/* --- reservoir release (solver/processes/reservoir.py) -------------------------
+ * Boxes are inclusive (r0, c0, r1, c1), as Structure.pool / .outlet. h is the
+ * current depth buffer, modified in place between steps. */
+/* reservoir.py:97-121 _withdraw_pool: h -= h * scale over the pool box (scale in
+ * [0, 1]); taken (device, (r1-r0+1) x (c1-c0+1) float64) receives each cell's exact
+ * float64 depth removed, for the host to sum as reservoir.py:246 does. */
+int rb_reservoir_withdraw(float *h, int32_t ny, int32_t nx, int32_t r0, int32_t c0, int32_t r1, int32_t c1,
+                          float scale, double *taken, void *stream);
+/* reservoir.py:124-144 _deliver_release: h += float32(add_depth) over the outlet box;
+ * the rounding shortfall (add_depth - actual gain, summed over the box) is banked in
+ * the workspace's loss ledger, where the reference banks it in loss_cum. */
+int rb_reservoir_deliver(float *h, int32_t ny, int32_t nx, int32_t r0, int32_t c0, int32_t r1, int32_t c1,
+                         double add_depth, void *ws, void *stream);
 
 /* --- a step that allocates nothing ---------------------------------------------
  * No counterpart in the reference. rb_hllc_step with its scratch in a static

@@ -17,6 +17,7 @@ points with ctypes, and restates the host-side Python of the reference path:
 * ``arm_channels`` / storage curve       -- solver/core/channels.py:140-312
 * ``arm_sediment`` / Exner activation    -- solver/core/sediment.py:658-709,
                                             solver/processes/morphology.py:223-321
+* ``ReservoirOperator``                  -- solver/processes/reservoir.py:149-263
 * ``MassLedger``                         -- solver/core/massbalance.py:39-158
 
 ``pow_mode`` selects how the four fractional powers are evaluated: 0 = libm
@@ -505,6 +506,78 @@ class _Kahan:
         t = self.total + y
         self.comp = (t - self.total) - y
         self.total = t
+
+
+class ReservoirOperator:
+    """solver/processes/reservoir.py:149-263 with config.py:228-241 (the release rule),
+    restated in numpy: ``structure`` is a dict of the reference Structure's fields.
+    Float32 depth arithmetic and float64 banking as the reference kernels
+    ``_withdraw_pool`` (:97-121) and ``_deliver_release`` (:124-144)."""
+
+    def __init__(self, structure: dict, st: State):
+        self.s = dict(structure)
+        self.st = st
+        self.records = []
+        r0, c0, r1, c1 = self.s["pool"]
+        o0, p0, o1, p1 = self.s["outlet"]
+        self.pool = (slice(r0, r1 + 1), slice(c0, c1 + 1))
+        self.outlet = (slice(o0, o1 + 1), slice(p0, p1 + 1))
+        self.outlet_cells = (o1 - o0 + 1) * (p1 - p0 + 1)
+        pool_z = st.z[self.pool].astype(np.float32)
+        a, b = np.unravel_index(int(np.argmin(pool_z)), pool_z.shape)
+        self.gauge = (r0 + int(a), c0 + int(b))
+        st._ensure_loss_cum()
+
+    def discharge_at(self, stage):
+        rule = self.s.get("release_rule", "none")
+        if rule == "none" or stage is None:
+            return 0.0
+        if rule == "fixed":
+            return float(self.s["release_m3_s"])
+        span = self.s["crest_m"] - float(self.s["target_stage_m"])
+        frac = (stage - float(self.s["target_stage_m"])) / span
+        return float(self.s["release_max_m3_s"]) * min(max(frac, 0.0), 1.0)
+
+    def pool_stage(self):
+        h = float(self.st.h[self.gauge])
+        if h <= H_DRY:
+            return None
+        return float(self.st.z[self.gauge]) + h
+
+    def advance(self, t: float, dt_slow: float):
+        stage = self.pool_stage()
+        q = self.discharge_at(stage)
+        volume = self._transfer(q * float(dt_slow)) if q > 0.0 else 0.0
+        rec = _Release(float(t), stage, q, volume)
+        self.records.append(rec)
+        return rec
+
+    def _transfer(self, requested_m3: float) -> float:
+        st, area = self.st, self.st.cell_area
+        stored = float(st.h[self.pool].astype(np.float64).sum()) * area
+        if stored <= 0.0:
+            return 0.0
+        scale = np.float32(min(1.0, requested_m3 / stored))
+        avail = st.h[self.pool].astype(np.float32)
+        h_new = (avail - avail * scale).astype(np.float32)
+        st.h[self.pool] = h_new
+        removed = float((avail.astype(np.float64) - h_new.astype(np.float64)).sum()) * area
+        if removed <= 0.0:
+            return 0.0
+        add = removed / area / self.outlet_cells
+        avail = st.h[self.outlet].astype(np.float32)
+        h_new = (avail + np.float32(add)).astype(np.float32)
+        st.h[self.outlet] = h_new
+        st.loss_cum[self.outlet] += add - (h_new.astype(np.float64) - avail.astype(np.float64))
+        return removed
+
+
+@dataclass
+class _Release:
+    time: float
+    stage: float | None
+    discharge_m3_s: float
+    volume_m3: float
 
 
 class MassLedger:

@@ -124,6 +124,57 @@ __global__ void inject_kernel(float* h, int nx, int nsrc, const int32_t* rows, c
   }
 }
 
+// solver/processes/reservoir.py:97-121 _withdraw_pool: remove scale * h from each
+// cell of the pool box and record the exact float64 depth each cell gave up.
+__global__ void reservoir_withdraw_kernel(float* __restrict__ h, int nx, int r0, int c0, int rows, int cols,
+                                          float scale, double* __restrict__ taken) {
+  const int64_t n = (int64_t)rows * cols;
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (int64_t)gridDim.x * blockDim.x) {
+    const int a = (int)(k / cols), b = (int)(k - (int64_t)a * cols);
+    const size_t id = (size_t)(r0 + a) * nx + (c0 + b);
+    const float avail = h[id];
+    const float h_new = avail - avail * scale;
+    h[id] = h_new;
+    taken[k] = (double)avail - (double)h_new;
+  }
+}
+
+// reservoir.py:124-144 _deliver_release: add float32(add_depth) to each outlet cell
+// and bank what rounding kept from arriving (add_depth - actual gain) in the loss
+// ledger. One block, fixed thread-to-cell map: the banked sum is deterministic.
+__global__ void __launch_bounds__(256) reservoir_deliver_kernel(float* __restrict__ h, int nx, int r0, int c0,
+                                                                int rows, int cols, double add_depth,
+                                                                double* ledger_slot) {
+  __shared__ double s_w[256 / 32];
+  const int64_t n = (int64_t)rows * cols;
+  double short_sum = 0.0;
+  for (int64_t k = threadIdx.x; k < n; k += 256) {
+    const int a = (int)(k / cols), b = (int)(k - (int64_t)a * cols);
+    const size_t id = (size_t)(r0 + a) * nx + (c0 + b);
+    const float avail = h[id];
+    const float h_new = avail + (float)add_depth;
+    h[id] = h_new;
+    const double delivered = (double)h_new - (double)avail;
+    short_sum += add_depth - delivered;
+  }
+  const double tot = block_sum<256>(short_sum, s_w);
+  if (threadIdx.x == 0 && ledger_slot != nullptr) ledger_add(ledger_slot, tot);
+}
+
+cudaError_t reservoir_withdraw(float* h, int nx, int r0, int c0, int rows, int cols, float scale, double* taken,
+                               cudaStream_t s) {
+  const int64_t n = (int64_t)rows * cols;
+  const int blocks = (int)((n + 255) / 256 < 1184 ? (n + 255) / 256 : 1184);
+  reservoir_withdraw_kernel<<<blocks, 256, 0, s>>>(h, nx, r0, c0, rows, cols, scale, taken);
+  return cudaGetLastError();
+}
+
+cudaError_t reservoir_deliver(float* h, int nx, int r0, int c0, int rows, int cols, double add_depth,
+                              double* ledger_slot, cudaStream_t s) {
+  reservoir_deliver_kernel<<<1, 256, 0, s>>>(h, nx, r0, c0, rows, cols, add_depth, ledger_slot);
+  return cudaGetLastError();
+}
+
 cudaError_t inject_points(float* h, int nx, int nsrc, const int32_t* rows, const int32_t* cols,
                           const float* add, float* comp, cudaStream_t s) {
   if (nsrc <= 0) return cudaSuccess;

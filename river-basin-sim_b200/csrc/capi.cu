@@ -113,6 +113,7 @@ size_t rb_hllc_workspace_bytes(int32_t ny, int32_t nx) {
 int rb_workspace_init(void* ws, size_t bytes, void* stream) {
   if (ws == nullptr || bytes < rb::WS_LEDGER) return fail(RB_ERR_ARG, "rb_workspace_init: workspace too small");
   RB_CUDA(cudaMemsetAsync(ws, 0, bytes, (cudaStream_t)stream), "rb_workspace_init");
+  rb::hllc_prepare_device();  // kernel attributes, before any stream capture
   return RB_OK;
 }
 
@@ -387,10 +388,48 @@ int rb_hllc_clock_start(const rb_hllc_fields* f, int32_t cur, const rb_clock_con
     if (f->bc[e] == RB_BC_STAGE && cfg->stage_off[e + 1] <= cfg->stage_off[e])
       return fail(RB_ERR_ARG, "rb_hllc_clock_start: fixed_stage edge %d has no stage curve", e);
   cudaStream_t s = (cudaStream_t)stream;
+  rb::hllc_prepare_device();
   if ((rc = clock_start(1, f->ny, f->nx, f->dx, cur, cfg, ws, s))) return rc;
   RB_CUDA(rb::reduce_wavespeed(f->h[cur], f->hu[cur], f->hv[cur], (size_t)f->ny * f->nx, &header(ws)->clock.red_key,
                                s),
           "rb_hllc_clock_start");
+  return RB_OK;
+}
+
+int rb_hllc_set_kernel_variant(int32_t variant) {
+  if (!rb::hllc_set_kernel_variant(variant))
+    return fail(RB_ERR_ARG, "rb_hllc_set_kernel_variant: variant %d is not in [0, %d)", variant,
+                rb::hllc_kernel_variant_count());
+  return RB_OK;
+}
+
+int rb_hllc_kernel_variants(int32_t* count) {
+  if (count == nullptr) return fail(RB_ERR_ARG, "rb_hllc_kernel_variants: null argument");
+  *count = rb::hllc_kernel_variant_count();
+  return RB_OK;
+}
+
+int rb_li_clock_reseed(const rb_li_fields* f, int32_t cur, void* ws, void* stream) {
+  if (f == nullptr || ws == nullptr || !f->h[0] || !f->h[1]) return fail(RB_ERR_ARG, "rb_li_clock_reseed: null argument");
+  int rc = check_grid(f->ny, f->nx, f->dx, "rb_li_clock_reseed");
+  if (rc) return rc;
+  if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_li_clock_reseed: cur must be 0 or 1");
+  if (f->chan_w && !f->chan_d) return fail(RB_ERR_ARG, "rb_li_clock_reseed: chan_w given without chan_d");
+  RB_CUDA(rb::reduce_max_column(f->h[cur], f->chan_w, f->chan_d, (float)f->dx, (size_t)f->ny * f->nx,
+                                &header(ws)->clock.red_key, (cudaStream_t)stream),
+          "rb_li_clock_reseed");
+  return RB_OK;
+}
+
+int rb_hllc_clock_reseed(const rb_hllc_fields* f, int32_t cur, void* ws, void* stream) {
+  if (f == nullptr || ws == nullptr || !f->h[cur & 1] || !f->hu[cur & 1] || !f->hv[cur & 1])
+    return fail(RB_ERR_ARG, "rb_hllc_clock_reseed: null argument");
+  int rc = check_grid(f->ny, f->nx, f->dx, "rb_hllc_clock_reseed");
+  if (rc) return rc;
+  if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_hllc_clock_reseed: cur must be 0 or 1");
+  RB_CUDA(rb::reduce_wavespeed(f->h[cur], f->hu[cur], f->hv[cur], (size_t)f->ny * f->nx, &header(ws)->clock.red_key,
+                               (cudaStream_t)stream),
+          "rb_hllc_clock_reseed");
   return RB_OK;
 }
 
@@ -684,6 +723,37 @@ int rb_inject_points(float* h, int32_t ny, int32_t nx, int32_t nsrc, const int32
   if (nsrc == 0) return RB_OK;
   if (!h || !rows || !cols || !add_depth) return fail(RB_ERR_ARG, "rb_inject_points: null argument");
   RB_CUDA(rb::inject_points(h, nx, nsrc, rows, cols, add_depth, comp, (cudaStream_t)stream), "rb_inject_points");
+  return RB_OK;
+}
+
+static int check_box(int32_t ny, int32_t nx, int32_t r0, int32_t c0, int32_t r1, int32_t c1, const char* who) {
+  if (ny < 1 || nx < 1) return fail(RB_ERR_ARG, "%s: bad grid %d x %d", who, ny, nx);
+  if (!(0 <= r0 && r0 <= r1 && r1 < ny && 0 <= c0 && c0 <= c1 && c1 < nx))
+    return fail(RB_ERR_ARG, "%s: box (%d, %d, %d, %d) is outside the %d x %d grid", who, r0, c0, r1, c1, ny, nx);
+  return RB_OK;
+}
+
+int rb_reservoir_withdraw(float* h, int32_t ny, int32_t nx, int32_t r0, int32_t c0, int32_t r1, int32_t c1,
+                          float scale, double* taken, void* stream) {
+  int rc = check_box(ny, nx, r0, c0, r1, c1, "rb_reservoir_withdraw");
+  if (rc) return rc;
+  if (!h || !taken) return fail(RB_ERR_ARG, "rb_reservoir_withdraw: null argument");
+  if (!(scale >= 0.0f && scale <= 1.0f)) return fail(RB_ERR_ARG, "rb_reservoir_withdraw: scale must be in [0, 1]");
+  RB_CUDA(rb::reservoir_withdraw(h, nx, r0, c0, r1 - r0 + 1, c1 - c0 + 1, scale, taken, (cudaStream_t)stream),
+          "rb_reservoir_withdraw");
+  return RB_OK;
+}
+
+int rb_reservoir_deliver(float* h, int32_t ny, int32_t nx, int32_t r0, int32_t c0, int32_t r1, int32_t c1,
+                         double add_depth, void* ws, void* stream) {
+  int rc = check_box(ny, nx, r0, c0, r1, c1, "rb_reservoir_deliver");
+  if (rc) return rc;
+  if (!h || !ws) return fail(RB_ERR_ARG, "rb_reservoir_deliver: null argument");
+  if (!(add_depth >= 0.0) || !std::isfinite(add_depth))
+    return fail(RB_ERR_ARG, "rb_reservoir_deliver: add_depth must be finite and >= 0");
+  double* slot0 = (double*)((char*)ws + rb::WS_LEDGER);  // ledger slot 0 of the domain's workspace
+  RB_CUDA(rb::reservoir_deliver(h, nx, r0, c0, r1 - r0 + 1, c1 - c0 + 1, add_depth, slot0, (cudaStream_t)stream),
+          "rb_reservoir_deliver");
   return RB_OK;
 }
 

@@ -75,6 +75,12 @@ __device__ __forceinline__ void commit(DevClock* c) {
   }
 }
 
+// steps + budget, saturated at INT_MAX (a budget of INT_MAX means "no limit").
+__device__ __forceinline__ int step_limit(int steps, int budget) {
+  const long long m = (long long)steps + (long long)(budget < 0 ? 0 : budget);
+  return m > 2147483647LL ? 2147483647 : (int)m;
+}
+
 __device__ void clock_plan(DevClock* c) {
   commit(c);
   c->active = 0;
@@ -162,7 +168,7 @@ __global__ void clock_target_many_kernel(DevClock* clocks, int n, const double* 
     commit(c);
     c->active = 0;
     c->t_target = t_target[d];
-    c->max_steps = c->steps + max_steps[d];
+    c->max_steps = step_limit(c->steps, max_steps[d]);
   }
 }
 
@@ -191,7 +197,7 @@ __global__ void clock_target_kernel(DevClock* c, double t_target, int max_steps)
   commit(c);
   c->active = 0;
   c->t_target = t_target;
-  c->max_steps = c->steps + max_steps;
+  c->max_steps = step_limit(c->steps, max_steps);
 }
 
 // inflow.py:167-200 InflowInjector.apply for the planned step: midpoint discharge,

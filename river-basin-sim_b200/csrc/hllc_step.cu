@@ -20,6 +20,7 @@
 // own faces. Stage 1 writes U1 = (h1, hu1, hv1) to workspace buffers; stage 2
 // reads U1 with the halo and U^n on the tile and writes U^{n+1} to the other
 // buffer of the caller's double-buffered (h, hu, hv).
+#include <atomic>
 #include <cfloat>
 
 #include "rb_common.cuh"
@@ -124,51 +125,17 @@ __device__ __forceinline__ Rec recon(const Cell& m, const Cell& c, const Cell& p
   return r;
 }
 
-// hllc.py:191-247, the mass component only (identical arithmetic to hllc_flux's fh).
-__device__ __forceinline__ float hllc_mass(float hl, float ul, float hr, float ur) {
-  const float g = kG;
-  const float cl = sqrtf(g * rmax(hl, 0.0f));
-  const float cr = sqrtf(g * rmax(hr, 0.0f));
-  const bool dry_l = hl <= kHDry, dry_r = hr <= kHDry;
-  if (dry_l && dry_r) return 0.0f;
-  float sl, sr;
-  if (dry_l) {
-    sl = ur - 2.0f * cr;
-    sr = ur + cr;
-  } else if (dry_r) {
-    sl = ul - cl;
-    sr = ul + 2.0f * cl;
-  } else {
-    const float hs = 0.5f * (cl + cr) + 0.25f * (ul - ur);
-    const float h_star = rmax(hs * hs / g, 0.0f);
-    const float c_star = sqrtf(g * h_star);
-    const float u_star = 0.5f * (ul + ur) + cl - cr;
-    sl = rmin(ul - cl, u_star - c_star);
-    sr = rmax(ur + cr, u_star + c_star);
-  }
-  const float fh_l = hl * ul;
-  const float fh_r = hr * ur;
-  if (sl >= 0.0f) return fh_l;
-  if (sr <= 0.0f) return fh_r;
-  const float inv = 1.0f / (sr - sl);
-  return (sr * fh_l - sl * fh_r + sl * sr * (hr - hl)) * inv;
-}
-
 // The face between a left cell's east values and a right cell's west values:
 // Audusse hydrostatic reconstruction and HLLC (hllc.py:344-354), with the left and
 // right bed-slope corrections of the normal momentum flux.
-__device__ __forceinline__ void face_flux(const Rec& L, const Rec& R, bool full, float& fh, float& fmn_l,
-                                          float& fmn_r, float& fmt) {
+__device__ __forceinline__ void face_flux(const Rec& L, const Rec& R, float& fh, float& fmn_l, float& fmn_r,
+                                          float& fmt) {
   const float g = kG;
   const float h_l = rmax(L.eE - L.zE, 0.0f);
   const float h_r = rmax(R.eW - R.zW, 0.0f);
   const float z_star = rmax(L.zE, R.zW);
   const float hl_star = rmax(L.eE - z_star, 0.0f);
   const float hr_star = rmax(R.eW - z_star, 0.0f);
-  if (!full) {
-    fh = hllc_mass(hl_star, L.nE, hr_star, R.nW);
-    return;
-  }
   float f0, f1, f2;
   hllc_flux(hl_star, L.nE, L.tE, hr_star, R.nW, R.tW, f0, f1, f2);
   fh = f0;
@@ -189,15 +156,18 @@ struct HllcSmem {
   float fxl[TY][TX + 1], fxr[TY][TX + 1], fxt[TY][TX + 1];  // tile x-faces
   float fyl[TY + 1][TX], fyr[TY + 1][TX], fyt[TY + 1][TX];  // tile y-faces
   float beta[BH][BW];
-  double red[8];
-  float redf[8];
+  double red[16];
+  float redf[16];
 };
 
 // One Heun stage of tile (bx, by) of domain p; ledger slot `slot`. Called by every
-// thread of the block; returns uniformly.
-template <int TX, int TY, int NT, int STAGE>
+// thread of the block; returns uniformly. FU faces per work item in the face phase
+// (1: each face reconstructs its four-cell stencil; 2 or 3: a rolling window that
+// reconstructs each cell once); LP 1 issues a thread's halo loads before its
+// divisions. Every choice computes the same bits.
+template <int TX, int TY, int NT, int STAGE, int FU = 1, int LP = 1>
 __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, size_t slot, HllcSmem<TX, TY>& S) {
-  static_assert(NT / 32 <= 8, "reduction scratch sized for <= 8 warps");
+  static_assert(NT / 32 <= 16, "reduction scratch sized for <= 16 warps");
   using SM = HllcSmem<TX, TY>;
   constexpr int H = SM::H, RW = SM::RW, RH = SM::RH, XW = SM::XW, XH = SM::XH, YW = SM::YW, YH = SM::YH;
   constexpr int BW = SM::BW, BH = SM::BH;
@@ -248,139 +218,211 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
   const float dx = p.dx32;
 
   // 1. stage the clamped halo and the primitives (hllc.py:262-282).
-  for (int k = threadIdx.x; k < RH * RW; k += NT) {
-    const int r = k / RW, c = k - r * RW;
-    const int gi = min(max(y0 - H + r, 0), ny - 1), gj = min(max(x0 - H + c, 0), nx - 1);
-    const size_t id = (size_t)gi * nx + gj;
-    const float hh = h_s[id];
-    float u = 0.0f, v = 0.0f;
-    if (hh > kHDry) {
-      u = hu_s[id] / hh;
-      v = hv_s[id] / hh;
+  if constexpr (LP == 0) {
+    for (int k = threadIdx.x; k < RH * RW; k += NT) {
+      const int r = k / RW, c = k - r * RW;
+      const int gi = min(max(y0 - H + r, 0), ny - 1), gj = min(max(x0 - H + c, 0), nx - 1);
+      const size_t id = (size_t)gi * nx + gj;
+      const float hh = h_s[id];
+      float u = 0.0f, v = 0.0f;
+      if (hh > kHDry) {
+        u = hu_s[id] / hh;
+        v = hv_s[id] / hh;
+      }
+      s_h[r][c] = hh;
+      s_u[r][c] = u;
+      s_v[r][c] = v;
+      s_z[r][c] = p.z[id];
     }
-    s_h[r][c] = hh;
-    s_u[r][c] = u;
-    s_v[r][c] = v;
-    s_z[r][c] = p.z[id];
+  } else {
+    // All of a thread's loads are issued before any of its divisions, so the
+    // global-memory latency of the whole halo overlaps.
+    constexpr int NL = (RH * RW + NT - 1) / NT;
+    float lh[NL], lhu[NL], lhv[NL], lz[NL];
+#pragma unroll
+    for (int i = 0; i < NL; i++) {
+      const int k = threadIdx.x + i * NT;
+      if (k < RH * RW) {
+        const int r = k / RW, c = k - r * RW;
+        const int gi = min(max(y0 - H + r, 0), ny - 1), gj = min(max(x0 - H + c, 0), nx - 1);
+        const size_t id = (size_t)gi * nx + gj;
+        lh[i] = h_s[id];
+        lhu[i] = hu_s[id];
+        lhv[i] = hv_s[id];
+        lz[i] = p.z[id];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NL; i++) {
+      const int k = threadIdx.x + i * NT;
+      if (k < RH * RW) {
+        const int r = k / RW, c = k - r * RW;
+        const float hh = lh[i];
+        float u = 0.0f, v = 0.0f;
+        if (hh > kHDry) {
+          u = lhu[i] / hh;
+          v = lhv[i] / hh;
+        }
+        s_h[r][c] = hh;
+        s_u[r][c] = u;
+        s_v[r][c] = v;
+        s_z[r][c] = lz[i];
+      }
+    }
   }
   __syncthreads();
 
   // 2. face fluxes (hllc.py:285-424) with boundary corrections (:993-1109).
-  // A thread takes FU consecutive faces along the normal and reconstructs each cell
-  // once in a rolling window of three cells: the reference's face-local eta_l /
-  // eta_r are exactly the left cell's east and the right cell's west values.
-  // The faces of the 1-cell ring around the tile only feed the limiter's beta, so
-  // they get the mass flux alone.
-  constexpr int FU = 3;
-  constexpr int GX = (XW + FU - 1) / FU, GY = (YH + FU - 1) / FU;
-  for (int k = threadIdx.x; k < XH * GX; k += NT) {
-    const int a = k / GX, g = k - a * GX;
-    const int gi = y0 - 1 + a;
-    if (gi < 0 || gi >= ny) continue;
-    const int r = a + 2;
-    const int b0 = g * FU;
-    Cell c0{s_h[r][b0 + 1], s_u[r][b0 + 1], s_v[r][b0 + 1], s_z[r][b0 + 1]};
-    Cell cp{s_h[r][b0 + 2], s_u[r][b0 + 2], s_v[r][b0 + 2], s_z[r][b0 + 2]};
-    Rec left = recon(Cell{s_h[r][b0], s_u[r][b0], s_v[r][b0], s_z[r][b0]}, c0, cp);
-#pragma unroll
-    for (int f = 0; f < FU; f++) {
-      const int b = b0 + f;
-      if (b >= XW) break;
-      const Cell cn{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
-      const Rec right = recon(c0, cp, cn);
-      const int gj = x0 - 1 + b;
-      if (gj >= 0 && gj <= nx) {
-        const bool inner = a >= 1 && a <= TY && b >= 1 && b <= TX + 1;
-        float fh, fl = 0.0f, fr = 0.0f, ft = 0.0f;
-        const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
-        if (kind == RB_BC_OPEN) {
-          face_flux(left, right, inner, fh, fl, fr, ft);
-        } else {
-          // edge cell: column 0 (west, region column b+2) or nx-1 (east, b+1)
-          const Cell& e = gj == 0 ? cp : c0;
-          float f1;
-          if (kind == RB_BC_CLOSED) {  // reflective wall, hllc.py:442-481
-            if (gj == 0)
-              hllc_flux(e.h, -e.un, e.ut, e.h, e.un, e.ut, fh, f1, ft);
-            else
-              hllc_flux(e.h, e.un, e.ut, e.h, -e.un, e.ut, fh, f1, ft);
-          } else {  // prescribed surface, hllc.py:537-581
-            const float h_g = rmax((gj == 0 ? stage_w : stage_e) - e.z, 0.0f);
-            if (gj == 0)
-              hllc_flux(h_g, e.un, e.ut, e.h, e.un, e.ut, fh, f1, ft);
-            else
-              hllc_flux(e.h, e.un, e.ut, h_g, e.un, e.ut, fh, f1, ft);
-          }
-          if (gj == 0)
-            fr = f1;  // only the inward slot is read (hllc.py:439-440)
-          else
-            fl = f1;
-        }
-        s_fxh[a][b] = fh;
-        if (inner) {
-          s_fxl[a - 1][b - 1] = fl;
-          s_fxr[a - 1][b - 1] = fr;
-          s_fxt[a - 1][b - 1] = ft;
-        }
-      }
-      left = right;
-      c0 = cp;
-      cp = cn;
+  // An edge face (gj == 0 / nx, gi == 0 / ny) of a closed or fixed_stage edge is a
+  // ghost-state Riemann problem on the edge cell e; only the inward normal-momentum
+  // slot is read (hllc.py:439-440).
+  auto edge_flux = [&](int kind, bool low, const Cell& e, float stage, float& fh, float& fl, float& fr, float& ft) {
+    float f1;
+    if (kind == RB_BC_CLOSED) {  // reflective wall, hllc.py:442-521
+      if (low)
+        hllc_flux(e.h, -e.un, e.ut, e.h, e.un, e.ut, fh, f1, ft);
+      else
+        hllc_flux(e.h, e.un, e.ut, e.h, -e.un, e.ut, fh, f1, ft);
+    } else {  // prescribed surface, hllc.py:537-628
+      const float h_g = rmax(stage - e.z, 0.0f);
+      if (low)
+        hllc_flux(h_g, e.un, e.ut, e.h, e.un, e.ut, fh, f1, ft);
+      else
+        hllc_flux(e.h, e.un, e.ut, h_g, e.un, e.ut, fh, f1, ft);
     }
-  }
-  // y-faces: normal velocity v, transverse u (hllc.py:357-424).
-  for (int k = threadIdx.x; k < GY * YW; k += NT) {
-    const int g = k / YW, b = k - g * YW;
-    const int gj = x0 - 1 + b;
-    if (gj < 0 || gj >= nx) continue;
-    const int c = b + 2;
-    const int a0 = g * FU;
-    Cell c0{s_h[a0 + 1][c], s_v[a0 + 1][c], s_u[a0 + 1][c], s_z[a0 + 1][c]};
-    Cell cp{s_h[a0 + 2][c], s_v[a0 + 2][c], s_u[a0 + 2][c], s_z[a0 + 2][c]};
-    Rec left = recon(Cell{s_h[a0][c], s_v[a0][c], s_u[a0][c], s_z[a0][c]}, c0, cp);
-#pragma unroll
-    for (int f = 0; f < FU; f++) {
-      const int a = a0 + f;
-      if (a >= YH) break;
-      const Cell cn{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
-      const Rec right = recon(c0, cp, cn);
-      const int gi = y0 - 1 + a;
-      if (gi >= 0 && gi <= ny) {
-        const bool inner = a >= 1 && a <= TY + 1 && b >= 1 && b <= TX;
-        float fh, fl = 0.0f, fr = 0.0f, ft = 0.0f;
-        const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
-        if (kind == RB_BC_OPEN) {
-          face_flux(left, right, inner, fh, fl, fr, ft);
-        } else {
-          const Cell& e = gi == 0 ? cp : c0;  // edge cell row 0 (north) or ny-1 (south)
-          float f1;
-          if (kind == RB_BC_CLOSED) {  // hllc.py:483-521
-            if (gi == 0)
-              hllc_flux(e.h, -e.un, e.ut, e.h, e.un, e.ut, fh, f1, ft);
-            else
-              hllc_flux(e.h, e.un, e.ut, e.h, -e.un, e.ut, fh, f1, ft);
-          } else {  // hllc.py:584-628
-            const float h_g = rmax((gi == 0 ? stage_n : stage_s) - e.z, 0.0f);
-            if (gi == 0)
-              hllc_flux(h_g, e.un, e.ut, e.h, e.un, e.ut, fh, f1, ft);
-            else
-              hllc_flux(e.h, e.un, e.ut, h_g, e.un, e.ut, fh, f1, ft);
-          }
-          if (gi == 0)
-            fr = f1;
-          else
-            fl = f1;
-        }
-        s_fyh[a][b] = fh;
-        if (inner) {
-          s_fyl[a - 1][b - 1] = fl;
-          s_fyr[a - 1][b - 1] = fr;
-          s_fyt[a - 1][b - 1] = ft;
-        }
+    fl = 0.0f;
+    fr = 0.0f;
+    if (low)
+      fr = f1;
+    else
+      fl = f1;
+  };
+  if constexpr (FU == 1) {
+    // One face per work item: four cells along the normal.
+    for (int k = threadIdx.x; k < XH * XW; k += NT) {
+      const int a = k / XW, b = k - a * XW;
+      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+      if (gi < 0 || gi >= ny || gj < 0 || gj > nx) continue;
+      const int r = a + 2;  // cell row; stencil columns b .. b+3 (cells gj-2 .. gj+1)
+      float fh, fl, fr, ft;
+      const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
+      if (kind == RB_BC_OPEN) {
+        const Cell c0{s_h[r][b], s_u[r][b], s_v[r][b], s_z[r][b]};
+        const Cell c1{s_h[r][b + 1], s_u[r][b + 1], s_v[r][b + 1], s_z[r][b + 1]};
+        const Cell c2{s_h[r][b + 2], s_u[r][b + 2], s_v[r][b + 2], s_z[r][b + 2]};
+        const Cell c3{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
+        face_flux(recon(c0, c1, c2), recon(c1, c2, c3), fh, fl, fr, ft);
+      } else {
+        const int ce = gj == 0 ? b + 2 : b + 1;  // the edge cell: column 0 or nx-1
+        edge_flux(kind, gj == 0, Cell{s_h[r][ce], s_u[r][ce], s_v[r][ce], s_z[r][ce]}, gj == 0 ? stage_w : stage_e,
+                  fh, fl, fr, ft);
       }
-      left = right;
-      c0 = cp;
-      cp = cn;
+      s_fxh[a][b] = fh;
+      if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
+        s_fxl[a - 1][b - 1] = fl;
+        s_fxr[a - 1][b - 1] = fr;
+        s_fxt[a - 1][b - 1] = ft;
+      }
+    }
+    for (int k = threadIdx.x; k < YH * YW; k += NT) {
+      const int a = k / YW, b = k - a * YW;
+      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+      if (gj < 0 || gj >= nx || gi < 0 || gi > ny) continue;
+      const int c = b + 2;  // cell column; stencil rows a .. a+3 (cells gi-2 .. gi+1)
+      float fh, fl, fr, ft;
+      const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
+      if (kind == RB_BC_OPEN) {
+        const Cell c0{s_h[a][c], s_v[a][c], s_u[a][c], s_z[a][c]};
+        const Cell c1{s_h[a + 1][c], s_v[a + 1][c], s_u[a + 1][c], s_z[a + 1][c]};
+        const Cell c2{s_h[a + 2][c], s_v[a + 2][c], s_u[a + 2][c], s_z[a + 2][c]};
+        const Cell c3{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
+        face_flux(recon(c0, c1, c2), recon(c1, c2, c3), fh, fl, fr, ft);
+      } else {
+        const int re = gi == 0 ? a + 2 : a + 1;  // the edge cell: row 0 or ny-1
+        edge_flux(kind, gi == 0, Cell{s_h[re][c], s_v[re][c], s_u[re][c], s_z[re][c]}, gi == 0 ? stage_n : stage_s,
+                  fh, fl, fr, ft);
+      }
+      s_fyh[a][b] = fh;
+      if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
+        s_fyl[a - 1][b - 1] = fl;
+        s_fyr[a - 1][b - 1] = fr;
+        s_fyt[a - 1][b - 1] = ft;
+      }
+    }
+  } else {
+    // FU consecutive faces per work item along the normal, each cell reconstructed
+    // once in a rolling window: the reference's face-local eta_l / eta_r are the
+    // left cell's east and the right cell's west values.
+    constexpr int GX = (XW + FU - 1) / FU, GY = (YH + FU - 1) / FU;
+    for (int k = threadIdx.x; k < XH * GX; k += NT) {
+      const int a = k / GX, g = k - a * GX;
+      const int gi = y0 - 1 + a;
+      if (gi < 0 || gi >= ny) continue;
+      const int r = a + 2;
+      const int b0 = g * FU;
+      Cell c0{s_h[r][b0 + 1], s_u[r][b0 + 1], s_v[r][b0 + 1], s_z[r][b0 + 1]};
+      Cell cp{s_h[r][b0 + 2], s_u[r][b0 + 2], s_v[r][b0 + 2], s_z[r][b0 + 2]};
+      Rec left = recon(Cell{s_h[r][b0], s_u[r][b0], s_v[r][b0], s_z[r][b0]}, c0, cp);
+#pragma unroll
+      for (int f = 0; f < FU; f++) {
+        const int b = b0 + f;
+        const int bb = b < XW ? b : XW - 1;  // a unit past the row end recomputes the last face, unstored
+        const Cell cn{s_h[r][bb + 3], s_u[r][bb + 3], s_v[r][bb + 3], s_z[r][bb + 3]};
+        const Rec right = recon(c0, cp, cn);
+        const int gj = x0 - 1 + b;
+        if (b < XW && gj >= 0 && gj <= nx) {
+          float fh, fl, fr, ft;
+          const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
+          if (kind == RB_BC_OPEN)
+            face_flux(left, right, fh, fl, fr, ft);
+          else  // edge cell: column 0 (cp) or nx-1 (c0)
+            edge_flux(kind, gj == 0, gj == 0 ? cp : c0, gj == 0 ? stage_w : stage_e, fh, fl, fr, ft);
+          s_fxh[a][b] = fh;
+          if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
+            s_fxl[a - 1][b - 1] = fl;
+            s_fxr[a - 1][b - 1] = fr;
+            s_fxt[a - 1][b - 1] = ft;
+          }
+        }
+        left = right;
+        c0 = cp;
+        cp = cn;
+      }
+    }
+    for (int k = threadIdx.x; k < GY * YW; k += NT) {
+      const int g = k / YW, b = k - g * YW;
+      const int gj = x0 - 1 + b;
+      if (gj < 0 || gj >= nx) continue;
+      const int c = b + 2;
+      const int a0 = g * FU;
+      Cell c0{s_h[a0 + 1][c], s_v[a0 + 1][c], s_u[a0 + 1][c], s_z[a0 + 1][c]};
+      Cell cp{s_h[a0 + 2][c], s_v[a0 + 2][c], s_u[a0 + 2][c], s_z[a0 + 2][c]};
+      Rec left = recon(Cell{s_h[a0][c], s_v[a0][c], s_u[a0][c], s_z[a0][c]}, c0, cp);
+#pragma unroll
+      for (int f = 0; f < FU; f++) {
+        const int a = a0 + f;
+        const int aa = a < YH ? a : YH - 1;
+        const Cell cn{s_h[aa + 3][c], s_v[aa + 3][c], s_u[aa + 3][c], s_z[aa + 3][c]};
+        const Rec right = recon(c0, cp, cn);
+        const int gi = y0 - 1 + a;
+        if (a < YH && gi >= 0 && gi <= ny) {
+          float fh, fl, fr, ft;
+          const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
+          if (kind == RB_BC_OPEN)
+            face_flux(left, right, fh, fl, fr, ft);
+          else  // edge cell: row 0 (cp) or ny-1 (c0)
+            edge_flux(kind, gi == 0, gi == 0 ? cp : c0, gi == 0 ? stage_n : stage_s, fh, fl, fr, ft);
+          s_fyh[a][b] = fh;
+          if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
+            s_fyl[a - 1][b - 1] = fl;
+            s_fyr[a - 1][b - 1] = fr;
+            s_fyt[a - 1][b - 1] = ft;
+          }
+        }
+        left = right;
+        c0 = cp;
+        cp = cn;
+      }
     }
   }
   __syncthreads();
@@ -450,10 +492,33 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
   const float g = kG;
   float smax = 0.0f;
   bool bad = false;
-  for (int k = threadIdx.x; k < TY * TX; k += NT) {
+  // The global inputs of this thread's cells are loaded first, all of them, so their
+  // latency overlaps instead of stalling each cell's update in turn.
+  constexpr int NC = (TX * TY + NT - 1) / NT;
+  float g_hus[NC], g_hvs[NC], g_hn[NC], g_hun[NC], g_hvn[NC], g_n[NC];
+#pragma unroll
+  for (int i = 0; i < NC; i++) {
+    const int k = threadIdx.x + i * NT;
     const int r = k / TX, c = k - r * TX;
     const int gi = y0 + r, gj = x0 + c;
-    if (gi >= ny || gj >= nx) continue;
+    if (k < TX * TY && gi < ny && gj < nx) {
+      const size_t id = (size_t)gi * nx + gj;
+      g_hus[i] = hu_s[id];
+      g_hvs[i] = hv_s[id];
+      if (STAGE == 2) {
+        g_hn[i] = h_n[id];
+        g_hun[i] = hu_n[id];
+        g_hvn[i] = hv_n[id];
+        g_n[i] = p.n[id];
+      }
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < NC; i++) {
+    const int k = threadIdx.x + i * NT;
+    const int r = k / TX, c = k - r * TX;
+    const int gi = y0 + r, gj = x0 + c;
+    if (k >= TX * TY || gi >= ny || gj >= nx) continue;
     const size_t id = (size_t)gi * nx + gj;
     const int R = r + H, Cc = c + H;  // this cell in the staged region
     const float dh = -((s_fxh[r + 1][c + 2] - s_fxh[r + 1][c + 1]) + (s_fyh[r + 2][c + 1] - s_fyh[r + 1][c + 1])) *
@@ -482,20 +547,20 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       const float hh = rmax(hg + dt * dh, 0.0f);
       float hu1 = 0.0f, hv1 = 0.0f;
       if (hh > kHDry) {
-        hu1 = hu_s[id] + dt * dhu;
-        hv1 = hv_s[id] + dt * dhv;
+        hu1 = g_hus[i] + dt * dhu;
+        hv1 = g_hvs[i] + dt * dhv;
       }
       p.h1[id] = hh;
       p.hu1[id] = hu1;
       p.hv1[id] = hv1;
     } else {  // hllc.py:881-909, then friction :912-939, then sources :1350-1373
-      float hh = rmax(0.5f * (h_n[id] + hg + dt * dh), 0.0f);
+      float hh = rmax(0.5f * (g_hn[i] + hg + dt * dh), 0.0f);
       float hu = 0.0f, hv = 0.0f;
       if (hh > kHDry) {
-        hu = 0.5f * (hu_n[id] + hu_s[id] + dt * dhu);
-        hv = 0.5f * (hv_n[id] + hv_s[id] + dt * dhv);
+        hu = 0.5f * (g_hun[i] + g_hus[i] + dt * dhu);
+        hv = 0.5f * (g_hvn[i] + g_hvs[i] + dt * dhv);
         const float mom = sqrtf(hu * hu + hv * hv);
-        const float denom = manning_denominator(mom, hh, p.n[id], g, dt);
+        const float denom = manning_denominator(mom, hh, g_n[i], g, dt);
         hu = hu / denom;
         hv = hv / denom;
       }
@@ -546,27 +611,95 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
   __syncthreads();  // the shared tile is reused by the caller's next tile
 }
 
-template <int TX, int TY, int NT, int STAGE>
-__global__ void __launch_bounds__(NT) hllc_stage_kernel(const HllcParams p) {
-  __shared__ HllcSmem<TX, TY> S;
-  hllc_tile<TX, TY, NT, STAGE>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S);
+// The single-domain stage kernel. Shared memory is dynamic (a 32 x 32 tile needs
+// more than the 48 KB a static array may take); __launch_bounds__ asks for two
+// resident 512-thread blocks (or four of 256) per SM, i.e. at most 64 registers.
+template <int TX, int TY, int NT, int STAGE, int FU, int LP>
+__global__ void __launch_bounds__(NT, 1024 / NT) hllc_stage_kernel(const HllcParams p) {
+  extern __shared__ __align__(16) unsigned char hllc_smem_raw[];
+  auto& S = *reinterpret_cast<HllcSmem<TX, TY>*>(hllc_smem_raw);
+  hllc_tile<TX, TY, NT, STAGE, FU, LP>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
 
-template <int TX, int TY, int NT>
+// The shared-memory opt-in is a per-device function attribute: set once per device
+// for an instantiation (setting it twice is harmless if threads race here).
+template <int TX, int TY, int NT, int FU, int LP>
+static void prepare_hllc() {
+  constexpr int smem = (int)sizeof(HllcSmem<TX, TY>);
+  static std::atomic<unsigned long long> attr_set{0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(attr_set.load() & bit)) {
+    cudaFuncSetAttribute(hllc_stage_kernel<TX, TY, NT, 1, FU, LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(hllc_stage_kernel<TX, TY, NT, 2, FU, LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr_set.fetch_or(bit);
+  }
+}
+
+template <int TX, int TY, int NT, int FU, int LP>
 static cudaError_t launch_hllc(const HllcParams& p, int stage, cudaStream_t s) {
+  constexpr size_t smem = sizeof(HllcSmem<TX, TY>);
+  static_assert(smem <= 227 * 1024, "tile does not fit in shared memory");
+  prepare_hllc<TX, TY, NT, FU, LP>();
   const dim3 grid((p.nx + TX - 1) / TX, (p.ny + TY - 1) / TY);
   if (stage == 1)
-    hllc_stage_kernel<TX, TY, NT, 1><<<grid, NT, 0, s>>>(p);
+    hllc_stage_kernel<TX, TY, NT, 1, FU, LP><<<grid, NT, smem, s>>>(p);
   else
-    hllc_stage_kernel<TX, TY, NT, 2><<<grid, NT, 0, s>>>(p);
+    hllc_stage_kernel<TX, TY, NT, 2, FU, LP><<<grid, NT, smem, s>>>(p);
   return cudaGetLastError();
 }
 
-cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s) {
-  return launch_hllc<HLLC_TX, HLLC_TY, HLLC_NT>(p, stage, s);
+// Kernel variants of the single-domain stage: tile, block size, faces per work item,
+// load batching. All compute the same bits; they differ only in speed. The default
+// is the fastest measured on B200 for the 2048 x 2048 dam break (ms per step, plan
+// included: 0.604, 0.517, 0.522, 0.556, 0.504, 0.511 for variants 0..5).
+struct HllcKernelVariant {
+  int tx, ty, nt, fu, lp;
+};
+static const HllcKernelVariant kHllcVariants[] = {
+    {32, 16, 256, 1, 0}, {32, 16, 256, 1, 1}, {32, 16, 256, 3, 1},
+    {32, 16, 256, 2, 1}, {32, 32, 512, 1, 1}, {64, 16, 512, 1, 1},
+};
+constexpr int kNumHllcVariants = (int)(sizeof(kHllcVariants) / sizeof(kHllcVariants[0]));
+constexpr int kDefaultHllcVariant = 4;
+static std::atomic<int> g_hllc_variant{kDefaultHllcVariant};
+
+int hllc_kernel_variant_count() { return kNumHllcVariants; }
+
+// Set every variant's shared-memory opt-in on the current device, outside any
+// stream capture (called by the non-capturable set-up entry points).
+void hllc_prepare_device() {
+  prepare_hllc<32, 16, 256, 1, 0>();
+  prepare_hllc<32, 16, 256, 1, 1>();
+  prepare_hllc<32, 16, 256, 3, 1>();
+  prepare_hllc<32, 16, 256, 2, 1>();
+  prepare_hllc<32, 32, 512, 1, 1>();
+  prepare_hllc<64, 16, 512, 1, 1>();
+}
+bool hllc_set_kernel_variant(int v) {
+  if (v < 0 || v >= kNumHllcVariants) return false;
+  g_hllc_variant.store(v);
+  return true;
 }
 
-int hllc_tiles(int ny, int nx) { return ((nx + HLLC_TX - 1) / HLLC_TX) * ((ny + HLLC_TY - 1) / HLLC_TY); }
+cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s) {
+  switch (g_hllc_variant.load()) {
+    case 1: return launch_hllc<32, 16, 256, 1, 1>(p, stage, s);
+    case 2: return launch_hllc<32, 16, 256, 3, 1>(p, stage, s);
+    case 3: return launch_hllc<32, 16, 256, 2, 1>(p, stage, s);
+    case 5: return launch_hllc<64, 16, 512, 1, 1>(p, stage, s);
+    case 0: return launch_hllc<32, 16, 256, 1, 0>(p, stage, s);
+    default: return launch_hllc<32, 32, 512, 1, 1>(p, stage, s);
+  }
+}
+
+// Tiles of the current variant (one ledger slot each); never more than the 32 x 8
+// tiling the workspace ledger is sized for.
+int hllc_tiles(int ny, int nx) {
+  const HllcKernelVariant& v = kHllcVariants[g_hllc_variant.load()];
+  return ((nx + v.tx - 1) / v.tx) * ((ny + v.ty - 1) / v.ty);
+}
 
 // Ensemble: one Heun stage over the (domain, local tile) work-list of every HLLC
 // domain (stage 2 of any domain starts only after stage 1 of all of them, as the

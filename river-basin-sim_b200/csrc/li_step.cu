@@ -175,33 +175,105 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
   const float dx = p.dx32;
   const float dtdx = dt / dx;
 
-  // 1. stage h, z, n (halo 2) and eta = h + z (local_inertial.py:61-69).
-  for (int k = threadIdx.x; k < RH * RW; k += NT) {
-    const int r = k / RW, c = k - r * RW;
-    const int gi = y0 - 2 + r, gj = x0 - 2 + c;
-    float h = 0.0f, z = 0.0f, n = 0.0f, w = 0.0f, d = 0.0f, cn = 0.0f;
-    const bool in = gi >= 0 && gi < ny && gj >= 0 && gj < nx;
-    const size_t id = in ? (size_t)gi * nx + gj : 0;
-    if (in) {
-      h = h_in[id];
-      z = p.z[id];
-      n = p.n[id];
-    }
-    s_h[r][c] = h;
-    s_z[r][c] = z;
-    s_n[r][c] = n;
-    if constexpr (CH) {  // local_inertial.py:278-291 compute_eta_channels
-      if (in) {
-        w = p.cw[id];
-        d = p.cd[id];
-        cn = p.cn[id];
+  // 1. stage h, z, n (halo 2) and eta = h + z (local_inertial.py:61-69), and the
+  //    previous discharge of every face the tile updates. Each thread issues all of
+  //    its loads before it stores any, so their latency overlaps.
+  {
+    constexpr int NL = (RH * RW + NT - 1) / NT;
+    float lh[NL], lz[NL], ln[NL], lw[NL], ld[NL], lc[NL];
+#pragma unroll
+    for (int i = 0; i < NL; i++) {
+      const int k = threadIdx.x + i * NT;
+      const int r = k / RW, c = k - r * RW;
+      const int gi = y0 - 2 + r, gj = x0 - 2 + c;
+      lh[i] = lz[i] = ln[i] = lw[i] = ld[i] = lc[i] = 0.0f;
+      if (k < RH * RW && gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
+        const size_t id = (size_t)gi * nx + gj;
+        lh[i] = h_in[id];
+        lz[i] = p.z[id];
+        ln[i] = p.n[id];
+        if constexpr (CH) {
+          lw[i] = p.cw[id];
+          ld[i] = p.cd[id];
+          lc[i] = p.cn[id];
+        }
       }
-      S.ch.w[r][c] = w;
-      S.ch.d[r][c] = d;
-      S.ch.cn[r][c] = cn;
-      s_eta[r][c] = eta_subgrid(h, z, w, d, dx);
-    } else {
-      s_eta[r][c] = h + z;
+    }
+#pragma unroll
+    for (int i = 0; i < NL; i++) {
+      const int k = threadIdx.x + i * NT;
+      if (k >= RH * RW) continue;
+      const int r = k / RW, c = k - r * RW;
+      s_h[r][c] = lh[i];
+      s_z[r][c] = lz[i];
+      s_n[r][c] = ln[i];
+      if constexpr (CH) {  // local_inertial.py:278-291 compute_eta_channels
+        S.ch.w[r][c] = lw[i];
+        S.ch.d[r][c] = ld[i];
+        S.ch.cn[r][c] = lc[i];
+        s_eta[r][c] = eta_subgrid(lh[i], lz[i], lw[i], ld[i], dx);
+      } else {
+        s_eta[r][c] = lh[i] + lz[i];
+      }
+    }
+    // previous face discharges (interior faces only; the rest are never read)
+    constexpr int NX_ = (XH * XW + NT - 1) / NT, NY_ = (YH * YW + NT - 1) / NT;
+    float fq[NX_], fc[NX_], ff[NX_], gq[NY_], gc[NY_], gf[NY_];
+#pragma unroll
+    for (int i = 0; i < NX_; i++) {
+      const int k = threadIdx.x + i * NT;
+      const int a = k / XW, b = k - a * XW;
+      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+      fq[i] = fc[i] = ff[i] = 0.0f;
+      if (k < XH * XW && gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1) {
+        const size_t fid = (size_t)gi * (nx + 1) + gj;
+        if constexpr (CH) {
+          fc[i] = p.qxcb[cur][fid];
+          ff[i] = p.qxfb[cur][fid];
+        } else {
+          fq[i] = qx_in[fid];
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NY_; i++) {
+      const int k = threadIdx.x + i * NT;
+      const int a = k / YW, b = k - a * YW;
+      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+      gq[i] = gc[i] = gf[i] = 0.0f;
+      if (k < YH * YW && gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx) {
+        const size_t fid = (size_t)gi * nx + gj;
+        if constexpr (CH) {
+          gc[i] = p.qycb[cur][fid];
+          gf[i] = p.qyfb[cur][fid];
+        } else {
+          gq[i] = qy_in[fid];
+        }
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NX_; i++) {
+      const int k = threadIdx.x + i * NT;
+      if (k >= XH * XW) continue;
+      const int a = k / XW, b = k - a * XW;
+      if constexpr (CH) {
+        S.ch.qxc[a][b] = fc[i];
+        S.ch.qxf[a][b] = ff[i];
+      } else {
+        s_qx[a][b] = fq[i];
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < NY_; i++) {
+      const int k = threadIdx.x + i * NT;
+      if (k >= YH * YW) continue;
+      const int a = k / YW, b = k - a * YW;
+      if constexpr (CH) {
+        S.ch.qyc[a][b] = gc[i];
+        S.ch.qyf[a][b] = gf[i];
+      } else {
+        s_qy[a][b] = gq[i];
+      }
     }
   }
   __syncthreads();
@@ -217,7 +289,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
         const float eta_l = s_eta[a + 1][b], eta_r = s_eta[a + 1][b + 1];
         const float h_flow = rmax(eta_l, eta_r) - rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
         if (!(h_flow < kHDry)) {
-          const float qo = qx_in[(size_t)gi * (nx + 1) + gj];
+          const float qo = s_qx[a][b];  // previous discharge, staged above
           const float n_face = 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]);
           const float slope = (eta_r - eta_l) / dx;
           const float num = qo - kG * h_flow * dt * slope;
@@ -233,11 +305,10 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
         const float eta_max = rmax(eta_l, eta_r);
         const float slope = (eta_r - eta_l) / dx;
         const float z_bank = rmax(s_z[r][cl], s_z[r][cr]);
-        const size_t fid = (size_t)gi * (nx + 1) + gj;
-        qf = floodplain_flux(p.qxfb[cur][fid], eta_max, slope, z_bank, 0.5f * (s_n[r][cl] + s_n[r][cr]), dt);
+        qf = floodplain_flux(S.ch.qxf[a][b], eta_max, slope, z_bank, 0.5f * (s_n[r][cl] + s_n[r][cr]), dt);
         const float w_face = rmin(S.ch.w[r][cl], S.ch.w[r][cr]);
         const float z_ch = rmax(s_z[r][cl] - S.ch.d[r][cl], s_z[r][cr] - S.ch.d[r][cr]);
-        qc = channel_flux(p.qxcb[cur][fid], eta_max, slope, w_face, z_bank, z_ch,
+        qc = channel_flux(S.ch.qxc[a][b], eta_max, slope, w_face, z_bank, z_ch,
                           0.5f * (S.ch.cn[r][cl] + S.ch.cn[r][cr]), dt);
         const float frac = w_face / dx;
         q = qf * (1.0f - frac) + qc * frac;
@@ -256,7 +327,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
         const float eta_t = s_eta[a][b + 1], eta_b = s_eta[a + 1][b + 1];
         const float h_flow = rmax(eta_t, eta_b) - rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
         if (!(h_flow < kHDry)) {
-          const float qo = qy_in[(size_t)gi * nx + gj];
+          const float qo = s_qy[a][b];
           const float n_face = 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]);
           const float slope = (eta_b - eta_t) / dx;
           const float num = qo - kG * h_flow * dt * slope;
@@ -272,11 +343,10 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
         const float eta_max = rmax(eta_t, eta_b);
         const float slope = (eta_b - eta_t) / dx;
         const float z_bank = rmax(s_z[rt][c], s_z[rb][c]);
-        const size_t fid = (size_t)gi * nx + gj;
-        qf = floodplain_flux(p.qyfb[cur][fid], eta_max, slope, z_bank, 0.5f * (s_n[rt][c] + s_n[rb][c]), dt);
+        qf = floodplain_flux(S.ch.qyf[a][b], eta_max, slope, z_bank, 0.5f * (s_n[rt][c] + s_n[rb][c]), dt);
         const float w_face = rmin(S.ch.w[rt][c], S.ch.w[rb][c]);
         const float z_ch = rmax(s_z[rt][c] - S.ch.d[rt][c], s_z[rb][c] - S.ch.d[rb][c]);
-        qc = channel_flux(p.qycb[cur][fid], eta_max, slope, w_face, z_bank, z_ch,
+        qc = channel_flux(S.ch.qyc[a][b], eta_max, slope, w_face, z_bank, z_ch,
                           0.5f * (S.ch.cn[rt][c] + S.ch.cn[rb][c]), dt);
         const float frac = w_face / dx;
         q = qf * (1.0f - frac) + qc * frac;

@@ -118,6 +118,9 @@ cudaError_t ens_hllc_launch(int variant, int grid, int stage, const HllcParams* 
                             cudaStream_t s);
 void set_last_error(const char* msg);  // the message rb_last_error returns on this thread
 int hllc_tiles(int ny, int nx);
+int hllc_kernel_variant_count();
+bool hllc_set_kernel_variant(int v);
+void hllc_prepare_device();
 
 // Workspace layout (byte offsets from the workspace base).
 struct WsHeader {
@@ -147,6 +150,10 @@ cudaError_t reduce_wavespeed(const float* h, const float* hu, const float* hv, s
                              cudaStream_t s);
 cudaError_t sum_f64(const float* x, size_t n, double* partials, double* out, cudaStream_t s);
 cudaError_t sum_ledger(const double* ledger, size_t nslots, double* partials, double* out, cudaStream_t s);
+cudaError_t reservoir_withdraw(float* h, int nx, int r0, int c0, int rows, int cols, float scale, double* taken,
+                               cudaStream_t s);
+cudaError_t reservoir_deliver(float* h, int nx, int r0, int c0, int rows, int cols, double add_depth,
+                              double* ledger_slot, cudaStream_t s);
 cudaError_t inject_points(float* h, int nx, int nsrc, const int32_t* rows, const int32_t* cols,
                           const float* add, float* comp, cudaStream_t s);
 cudaError_t exner_apply(int ny, int nx, float dx32, float inv1mp, float* qs_int_x, float* qs_int_y,

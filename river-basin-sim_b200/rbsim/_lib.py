@@ -122,6 +122,14 @@ SIGNATURES = {
     "rb_ensemble_set_targets": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, _P, _P, _P]),
     "rb_ensemble_enqueue": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, ctypes.c_int32, _P]),
     "rb_ensemble_read": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, _P, _P]),
+    "rb_hllc_set_kernel_variant": (ctypes.c_int, [ctypes.c_int32]),
+    "rb_hllc_kernel_variants": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
+    "rb_li_clock_reseed": (ctypes.c_int, [ctypes.POINTER(LiFields), ctypes.c_int32, _P, _P]),
+    "rb_hllc_clock_reseed": (ctypes.c_int, [ctypes.POINTER(HllcFields), ctypes.c_int32, _P, _P]),
+    "rb_reservoir_withdraw": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_float, _P, _P]),
+    "rb_reservoir_deliver": (ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32, ctypes.c_int32,
+                                            ctypes.c_int32, ctypes.c_int32, ctypes.c_double, _P, _P]),
     "rb_hllc_step_noalloc": (ctypes.c_int, [ctypes.POINTER(HllcFields), ctypes.c_int32, ctypes.POINTER(StepArgs),
                                             _P, _P]),
     "rb_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),

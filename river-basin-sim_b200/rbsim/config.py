@@ -1,11 +1,11 @@
 """Scenario configuration for the solver path (the subset of solver/io/config.py it reads).
 
 Reads the same TOML tables and keys as the reference (``[meta] [grid] [run]
-[rainfall] [parameters] [sediment] [[inflow]] [boundaries]``, HANDOFF.md's schema);
-terrain comes from ``[grid] dem`` (a raw little-endian float32 ``.r32`` with
-``shape = [ny, nx]``) or is handed to ``run_simulation`` as an array, since tile
-mosaics, coarsening, datums, sub-grid channels and structures are outside this
-build's path. Unsupported tables raise ``ConfigError`` rather than being ignored.
+[rainfall] [parameters] [sediment] [channels] [[inflow]] [[structures]]
+[boundaries]``, HANDOFF.md's schema); terrain comes from ``[grid] dem`` (a raw
+little-endian float32 ``.r32`` with ``shape = [ny, nx]``) or is handed to
+``run_simulation`` as an array, since tile mosaics, coarsening and datums are
+outside this build's path.
 """
 
 from __future__ import annotations
@@ -20,11 +20,85 @@ from .processes.inflow import Inflow
 from .schemes import KNOWN_SCHEMES
 
 EDGES = ("north", "south", "east", "west")
-_UNSUPPORTED = ("channels", "structures")
+_UNSUPPORTED: tuple[str, ...] = ()
+_STRUCTURE_KINDS = {"dam", "levee"}
+_RELEASE_RULES = {"none", "fixed", "target_stage"}
+_DEFAULT_RELEASE_INTERVAL_S = 900.0
 
 
 class ConfigError(ValueError):
     """A scenario config is malformed or asks for something outside the solver path."""
+
+
+@dataclass
+class Structure:
+    """A dam or levee with an optional release rule (solver/io/config.py:147-241).
+
+    ``cells`` + ``crest_m`` raise the bed to the crest (processes.reservoir.apply_barriers);
+    a ``dam`` may carry a release rule evaluated on the slow clock every ``interval_s``,
+    moving water from the inclusive ``pool`` box to the inclusive ``outlet`` box.
+    """
+
+    name: str = "dam"
+    kind: str = "dam"
+    cells: list = field(default_factory=list)
+    crest_m: float = 0.0
+    release_rule: str = "none"
+    release_m3_s: float = 0.0
+    target_stage_m: float | None = None
+    release_max_m3_s: float = 0.0
+    pool: tuple | None = None
+    outlet: tuple | None = None
+    interval_s: float = _DEFAULT_RELEASE_INTERVAL_S
+
+    def __post_init__(self) -> None:
+        n = self.name
+        if self.kind not in _STRUCTURE_KINDS:
+            raise ValueError(f"structure '{n}': type must be one of {sorted(_STRUCTURE_KINDS)}")
+        if not self.cells:
+            raise ValueError(f"structure '{n}': needs at least one barrier cell")
+        if self.release_rule not in _RELEASE_RULES:
+            raise ValueError(f"structure '{n}': release_rule must be one of {sorted(_RELEASE_RULES)}")
+        if self.kind == "levee" and self.release_rule != "none":
+            raise ValueError(f"structure '{n}': a levee is barrier geometry only; use type='dam' for a release rule")
+        if self.interval_s <= 0:
+            raise ValueError(f"structure '{n}': interval_s must be > 0")
+        if self.release_rule == "none":
+            return
+        if self.pool is None or self.outlet is None:
+            raise ValueError(f"structure '{n}': release_rule='{self.release_rule}' needs both a 'pool' box and an "
+                             "'outlet' cell (where the released water is delivered)")  # fmt: skip
+        r0, c0, r1, c1 = self.pool
+        if r1 < r0 or c1 < c0:
+            raise ValueError(f"structure '{n}': pool must be [row0, col0, row1, col1]")
+        o0, p0, o1, p1 = self.outlet
+        if o1 < o0 or p1 < p0:
+            raise ValueError(f"structure '{n}': outlet must be [row, col] or [row0, col0, row1, col1]")
+        if not (o1 < r0 or o0 > r1 or p1 < c0 or p0 > c1):
+            raise ValueError(f"structure '{n}': the outlet {self.outlet} overlaps the pool {self.pool}; the release "
+                             "would just shuffle water within the reservoir")  # fmt: skip
+        if self.release_rule == "fixed" and self.release_m3_s <= 0:
+            raise ValueError(f"structure '{n}': release_rule='fixed' needs release_m3_s > 0")
+        if self.release_rule == "target_stage":
+            if self.target_stage_m is None:
+                raise ValueError(f"structure '{n}': release_rule='target_stage' needs target_stage_m")
+            if self.release_max_m3_s <= 0:
+                raise ValueError(f"structure '{n}': release_rule='target_stage' needs release_max_m3_s > 0 (the cap "
+                                 "the proportional rule scales toward)")  # fmt: skip
+            if self.target_stage_m >= self.crest_m:
+                raise ValueError(f"structure '{n}': target_stage_m ({self.target_stage_m}) must be below crest_m "
+                                 f"({self.crest_m}) -- the rule ramps between the two")  # fmt: skip
+
+    def discharge_at(self, stage: float | None) -> float:
+        """Release the rule asks for at a pool stage (config.py:228-241): ``fixed`` is
+        constant; ``target_stage`` ramps from 0 at the target to the cap at the crest."""
+        if self.release_rule == "none" or stage is None:
+            return 0.0
+        if self.release_rule == "fixed":
+            return float(self.release_m3_s)
+        span = self.crest_m - float(self.target_stage_m)
+        frac = (stage - float(self.target_stage_m)) / span
+        return float(self.release_max_m3_s) * min(max(frac, 0.0), 1.0)
 
 
 @dataclass
@@ -50,6 +124,10 @@ class Scenario:
     sediment_porosity: float = 0.4
     sediment_interval_s: float = 900.0
     alluvium_thickness: float | np.ndarray | None = None
+    channel_width: float | np.ndarray = 0.0  # m; a scenario has channels iff a width is given
+    channel_depth: float | np.ndarray = 0.0  # bank-full depth below the floodplain bed, m
+    channel_manning: float | np.ndarray | None = None  # None: the floodplain roughness
+    structures: list = field(default_factory=list)
     bed: np.ndarray | None = None
 
     @property
@@ -59,6 +137,10 @@ class Scenario:
     @property
     def has_sediment(self) -> bool:
         return self.sediment_d50 is not None
+
+    @property
+    def has_channels(self) -> bool:
+        return not np.isscalar(self.channel_width) or float(self.channel_width) > 0.0
 
     @property
     def stage_events(self) -> list[float]:
@@ -143,4 +225,47 @@ def load_config(path) -> Scenario:
         sc.sediment_interval_s = float(sed.get("interval_s", 900.0))
         if "alluvium_thickness" in sed:
             sc.alluvium_thickness = _field(sed["alluvium_thickness"], base, shape, "alluvium_thickness")
+    chan = doc.get("channels")
+    if chan is not None:  # config.py:873-885, validated as :421-441
+        sc.channel_width = _field(chan.get("width", 0.0), base, shape, "[channels] width")
+        sc.channel_depth = _field(chan.get("depth", 0.0), base, shape, "[channels] depth")
+        if "manning" in chan:
+            sc.channel_manning = _field(chan["manning"], base, shape, "[channels] manning")
+        if sc.has_channels and sc.scheme != "local_inertial":
+            raise ConfigError(f"[channels] requires scheme='local_inertial'; the '{sc.scheme}' scheme has no "
+                              "sub-grid channel model")  # fmt: skip
+        if np.isscalar(sc.channel_width) and sc.channel_width < 0:
+            raise ConfigError(f"[channels] width must be >= 0, got {sc.channel_width}")
+        if sc.has_channels and np.isscalar(sc.channel_depth) and sc.channel_depth <= 0:
+            raise ConfigError("[channels] a width without a bank-full depth is not a channel; set [channels] depth")
+        if sc.channel_manning is not None and np.isscalar(sc.channel_manning) and sc.channel_manning <= 0:
+            raise ConfigError(f"[channels] manning must be > 0, got {sc.channel_manning}")
+    for k, entry in enumerate(doc.get("structures", [])):  # config.py:676-730
+        name = str(entry.get("name", f"structure{k}"))
+        if "crest_m" not in entry:
+            raise ConfigError(f"[[structures]] #{k} ('{name}'): 'crest_m' is required")
+        pool = entry.get("pool")
+        if pool is not None:
+            if not (isinstance(pool, list) and len(pool) == 4):
+                raise ConfigError(f"[[structures]] #{k} ('{name}'): 'pool' must be [row0, col0, row1, col1]")
+            pool = tuple(int(v) for v in pool)
+        outlet = entry.get("outlet")
+        if outlet is not None:
+            if not (isinstance(outlet, list) and len(outlet) in (2, 4)):
+                raise ConfigError(f"[[structures]] #{k} ('{name}'): 'outlet' must be [row, col] or "
+                                  "[row0, col0, row1, col1]")  # fmt: skip
+            vals = tuple(int(v) for v in outlet)
+            outlet = (vals[0], vals[1], vals[0], vals[1]) if len(vals) == 2 else vals
+        try:
+            sc.structures.append(Structure(
+                name=name, kind=str(entry.get("type", "dam")),
+                cells=[(int(c[0]), int(c[1])) for c in entry.get("cells", [])],
+                crest_m=float(entry["crest_m"]), release_rule=str(entry.get("release_rule", "none")),
+                release_m3_s=float(entry.get("release_m3_s", 0.0)),
+                target_stage_m=float(entry["target_stage_m"]) if "target_stage_m" in entry else None,
+                release_max_m3_s=float(entry.get("release_max_m3_s", 0.0)), pool=pool, outlet=outlet,
+                interval_s=float(entry.get("interval_s", _DEFAULT_RELEASE_INTERVAL_S)),
+            ))  # fmt: skip
+        except (TypeError, ValueError, IndexError) as e:
+            raise ConfigError(f"[[structures]] #{k} ('{name}'): {e}") from e
     return sc

@@ -141,11 +141,21 @@ class DeviceClock:
         start = self.steps
         self.set_target(t_target, max_steps)
         while True:
+            before = self.steps
             self._replay()
             st = self.read()
             taken = st.steps - start
             if st.t >= t_target - EPS_T or taken >= max_steps:
                 return taken
+            if st.steps == before:  # an inactive clock would otherwise spin here forever
+                raise RuntimeError(f"device clock made no progress toward t={t_target} (t={st.t}, "
+                                   f"steps={st.steps}, err={st.err})")  # fmt: skip
+
+    def reseed(self) -> None:
+        """Recompute the next step's CFL reduction from the current state: call after
+        anything outside the clocked steps changed h (or hu, hv) between spans."""
+        fn = self._L.rb_hllc_clock_reseed if self.scheme == "hllc_fv" else self._L.rb_li_clock_reseed
+        _lib.check(fn(ctypes.byref(self._fields), self.state.cur, self.state.workspace.data_ptr(), self.state.stream))
 
     def enqueue_span(self, max_steps: int) -> None:
         """Enqueue (without waiting) replays covering at most ``max_steps`` more steps."""

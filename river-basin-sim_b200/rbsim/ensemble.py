@@ -121,24 +121,35 @@ class Ensemble:
 
         self.set_targets(t_target)
         tt = list(t_target) if np.ndim(t_target) else [t_target] * len(self.states)
+        before = [c.steps for c in self.read()]
         for k in range(max_replays):
             self.replay()
             clk = self.read()
             if all(c.t >= t - EPS_T for c, t in zip(clk, tt, strict=True)):
                 return k + 1
+            now = [c.steps for c in clk]
+            if now == before:  # no member stepped: the clocks are inactive, stop instead of spinning
+                raise RuntimeError("ensemble made no progress toward its targets")
+            before = now
         raise RuntimeError("ensemble did not reach its targets")
 
 
 def autotune(make_ensemble, probe_replays: int = 2, candidates=None):
-    """Time each (li_variant, hllc_variant) on the run; return (best pair, timings in ms per replay).
+    """Time each (li_variant, hllc_variant) on the run itself; return (best pair, ms per replay, times).
 
-    ``make_ensemble(li_variant, hllc_variant)`` builds an Ensemble over the same
-    member states (already targeted); each candidate replays ``probe_replays`` times.
+    ``make_ensemble(li_variant, hllc_variant, t0)`` builds an Ensemble over the same
+    member states, already targeted, with each member's clock starting at ``t0[d]``
+    (``None`` for the first candidate: the caller's start). Each candidate takes
+    1 + ``probe_replays`` replays of real steps, and the next one continues every
+    clock where it stopped, so the probing is part of the run: every variant
+    computes the same bits, and a clock that restarted at the run's start would
+    lay different steps toward its sync times. Build the production ensemble with
+    ``t0 = times`` (the simulated time each member reached).
     """
     candidates = candidates or [(a, b) for a in LI_VARIANTS for b in HLLC_VARIANTS]
-    timings = {}
+    timings, t0 = {}, None
     for li_v, hl_v in candidates:
-        ens = make_ensemble(li_v, hl_v)
+        ens = make_ensemble(li_v, hl_v, t0)
         ens.replay()  # capture + first replay, untimed
         start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record()
@@ -147,9 +158,9 @@ def autotune(make_ensemble, probe_replays: int = 2, candidates=None):
         stop.record()
         stop.synchronize()
         timings[(li_v, hl_v)] = start.elapsed_time(stop) / probe_replays
-        ens.read()
+        t0 = [c.t for c in ens.read()]
     best = min(timings, key=timings.get)
-    return best, timings
+    return best, timings, t0
 
 
 def log_uniform_sides(n: int, lo: int, hi: int, seed: int) -> list[int]:

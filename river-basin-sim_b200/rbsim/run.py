@@ -1,10 +1,12 @@
 """Run a scenario on the B200 and stream results to the Zarr store (solver/run.py:140-584).
 
 Same arming order and hot-loop semantics as the reference ``run_simulation``:
-fields -> morphology (z0 captured after the bed is final) -> infiltration ->
-rain field -> areal-source compensation -> inflow injector -> boundaries ->
-ledgers -> writer + frame 0 -> the scheduler's ticks: inject, step, bank rain,
-advance due slow processes, record + write at output ticks.
+barriers raised into the bed -> fields -> sub-grid channels -> morphology (z0
+captured after the bed is final, structure cells frozen) -> infiltration -> rain
+field -> areal-source compensation -> inflow injector -> boundaries -> reservoir
+operators -> ledgers -> writer + frame 0 -> the scheduler's ticks: inject, step,
+bank rain, advance due slow processes (reservoirs before morphology), record +
+write at output ticks.
 
 Two ways through the ticks, with identical results:
 
@@ -35,6 +37,7 @@ from .io.zarr_writer import AsyncFrameWriter, ZarrWriter
 from .massbalance import MassLedger, SedimentLedger
 from .processes.inflow import InflowInjector
 from .processes.morphology import MorphologyProcess, bed_change_bounds
+from .processes.reservoir import apply_barriers, build_operators
 from .scheduler import EPS_T, MultiRateScheduler
 from .schemes import get_scheme, hllc
 from .sediment import arm_sediment
@@ -64,15 +67,29 @@ def run_simulation(scenario: Scenario, bed=None, out_path="results.zarr", *, dev
     if sc.dx is None:
         raise ValueError("scenario.dx is unresolved")
     scheme = get_scheme(sc.scheme)
+    bed = apply_barriers(np.asarray(bed, np.float32), sc.structures)  # run.py:199
     st = State.from_bed(bed, sc.dx, depth=sc.initial_depth, manning=sc.manning, device=device)
     grid = st.grid
     if sc.scheme == "hllc_fv":
         hllc.arm_hllc(st)
 
+    channels = None
+    if sc.has_channels:  # run.py:204-228
+        from .channels import arm_channels
+
+        shape = grid.shape
+        channels = arm_channels(st, np.broadcast_to(np.asarray(sc.channel_width, np.float32), shape),
+                                np.broadcast_to(np.asarray(sc.channel_depth, np.float32), shape),
+                                None if sc.channel_manning is None
+                                else np.broadcast_to(np.asarray(sc.channel_manning, np.float32), shape))  # fmt: skip
+        if verbose:
+            print(f"  channels      : {channels.summary()}")
+
     morphology = None
     if sc.has_sediment:
         arm_sediment(st, sc.sediment_d50, sc.sediment_porosity)
-        dz_lo, dz_hi = bed_change_bounds(grid.shape, alluvium_thickness=sc.alluvium_thickness)
+        frozen = [cell for s in sc.structures for cell in s.cells]  # run.py:252-258: dams do not scour
+        dz_lo, dz_hi = bed_change_bounds(grid.shape, alluvium_thickness=sc.alluvium_thickness, frozen_cells=frozen)
         morphology = MorphologyProcess(st, sc.sediment_interval_s, dz_lo=dz_lo, dz_hi=dz_hi)
         if verbose:
             print(f"  morphology    : {morphology.summary()}")
@@ -91,6 +108,7 @@ def run_simulation(scenario: Scenario, bed=None, out_path="results.zarr", *, dev
         st.arm_source_compensation()
     injector = InflowInjector(sc.inflows, grid, st.device) if sc.inflows else None
     st.set_open_boundaries(sc.boundaries, sc.stage_curves)
+    reservoirs = build_operators(sc.structures, st)  # after the State: they arm the loss ledger
 
     ledger = MassLedger.from_state(st)
     sed_ledger = SedimentLedger.from_state(st) if morphology is not None else None
@@ -104,8 +122,13 @@ def run_simulation(scenario: Scenario, bed=None, out_path="results.zarr", *, dev
     }  # fmt: skip
     if morphology is not None:
         attrs["sediment"] = {"law": "mpm", **morphology.as_attrs()}
+    if channels is not None:
+        attrs["channels"] = channels.as_attrs()
     writer = ZarrWriter(out_path, grid, n_frames, attrs, bed_change=morphology is not None)
     writer.write_bed(np.asarray(bed, np.float32))
+    if channels is not None:  # run.py:331-335
+        writer.write_static("channel_width", channels.w.cpu().numpy())
+        writer.write_static("channel_depth", channels.d.cpu().numpy())
     frames = AsyncFrameWriter(writer, st.device)
 
     def emit(t_out: float) -> None:
@@ -117,7 +140,8 @@ def run_simulation(scenario: Scenario, bed=None, out_path="results.zarr", *, dev
     sched = MultiRateScheduler(
         end_time=sc.end_time, output_every=sc.output_every,
         events=[sc.rain_duration, *inflow_events, *sc.stage_events],
-        processes=[morphology.as_slow_process()] if morphology is not None else [],
+        processes=[*(r.as_slow_process() for r in reservoirs),
+                   *([morphology.as_slow_process()] if morphology is not None else [])],
     )  # fmt: skip
 
     def on_output(t1: float) -> None:
@@ -154,6 +178,7 @@ def run_simulation(scenario: Scenario, bed=None, out_path="results.zarr", *, dev
             ledger.add_inflow(clock.inflow_volume - banked_inflow)
             ledger.add_inflow(clock.rain_volume - banked_rain)
             banked_rain, banked_inflow = clock.rain_volume, clock.inflow_volume
+            any_fired = False
             for p in procs:  # scheduler.py:234-242, on the step that landed here
                 times, fired = pending[p.name], False
                 while times and t1 >= times[0] - EPS_T:
@@ -162,6 +187,9 @@ def run_simulation(scenario: Scenario, bed=None, out_path="results.zarr", *, dev
                 if fired:
                     p.advance(t1, t1 - last_ran[p.name])
                     last_ran[p.name] = t1
+                    any_fired = True
+            if any_fired and reservoirs:  # a release moved water: the next dt reads the new state
+                clock.reseed()
             if t1 >= next_output - EPS_T and next_output <= sc.end_time + EPS_T:
                 next_output += sc.output_every
                 on_output(t1)
@@ -191,6 +219,8 @@ def run_simulation(scenario: Scenario, bed=None, out_path="results.zarr", *, dev
     if morphology is not None:
         final["morphology"] = morphology.series
         final.update(sed_ledger.as_attrs())
+    if reservoirs:
+        final["reservoir_releases"] = {r.structure.name: r.series for r in reservoirs}
     writer.finalize(final)
     if verbose and ledger.max_rel_error >= 1e-6:
         print(f"  warning: mass balance {ledger.max_rel_error:.2e} exceeds the 1e-6 gate")

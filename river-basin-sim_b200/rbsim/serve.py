@@ -174,9 +174,12 @@ class Server:
             if ens is None:
                 ens = _build_ensemble(active, self.graph_steps)
                 rebuilds += 1
+            before = [m.steps for m in active]
             ens.replay()
             replays += 1
             clk = ens.read()
+            if all(m.base_steps + c.steps == b for m, c, b in zip(active, clk, before, strict=True)):
+                raise RuntimeError("the batch made no progress in a replay (every member's clock is inactive)")
             finished, retarget = [], False
             for m, c in zip(active, clk, strict=True):
                 m.t, m.steps = c.t, m.base_steps + c.steps

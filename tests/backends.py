@@ -45,6 +45,9 @@ class OracleBackend:
     def arm_channels(self, st, w, d, n=None):
         st.arm_channels(w, d, n)
 
+    def reservoir(self, st, structure: dict):
+        return self.o.ReservoirOperator(structure, st)
+
     def channel_n(self, st):
         return st.channels.n.copy()
 
@@ -153,6 +156,12 @@ class GpuBackend:
         from rbsim.channels import arm_channels
 
         arm_channels(st, w, d, n)
+
+    def reservoir(self, st, structure: dict):
+        from rbsim.config import Structure
+        from rbsim.processes.reservoir import ReservoirOperator
+
+        return ReservoirOperator(Structure(**structure), st)
 
     def channel_n(self, st):
         return st.channels.n.cpu().numpy()

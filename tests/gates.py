@@ -622,4 +622,131 @@ def gate_subgrid_channel_matches_resolved_reach(be):
     assert abs(coarse_volume / fine_volume - 1.0) < 0.20
 
 
+# --- reservoirs (solver/processes/test_reservoir.py) ------------------------- #
+_RNY, _RNX, _RDX, _DAM_ROW, _CREST = 12, 8, 10.0, 6, 5.0
+
+
+def _basin():
+    z = np.zeros((_RNY, _RNX), np.float32)
+    z[: _DAM_ROW + 1] = 2.0
+    z[_DAM_ROW + 1 :] = np.linspace(2.0, 0.0, _RNY - _DAM_ROW - 1, dtype=np.float32)[:, None]
+    return z
+
+
+def _dam(**kw):
+    base = dict(name="d", kind="dam", cells=[(_DAM_ROW, j) for j in range(_RNX)], crest_m=_CREST,
+                release_rule="fixed", release_m3_s=1.0, pool=(0, 0, 5, _RNX - 1), outlet=(8, 2, 10, 5),
+                interval_s=300.0)  # fmt: skip
+    base.update(kw)
+    return base
+
+
+def _barriers(bed, dam):
+    out = bed.copy()
+    for i, j in dam["cells"]:
+        out[i, j] = max(float(out[i, j]), float(dam["crest_m"]))
+    return out
+
+
+def _pool_depth(surface):
+    bed = _basin()
+    h = np.zeros((_RNY, _RNX), np.float32)
+    h[:_DAM_ROW] = np.maximum(surface - bed[:_DAM_ROW], 0.0)
+    return h
+
+
+def _vol(h):
+    return float(np.asarray(h, np.float64).sum()) * _RDX * _RDX
+
+
+def _run_pool(be, bed, h0, steps=300):
+    st = be.make(bed, _RDX, depth=h0, manning=0.03)
+    be.arm_hllc(st)
+    for _ in range(steps):
+        be.step(st, HLLC, be.compute_dt(st, HLLC, 0.45, 5.0))
+    return be.h(st)
+
+
+def gate_reservoir_barrier_impounds(be):
+    """test_reservoir.py:108 -- the dam keeps > 90 % of the pool; without it most escapes."""
+    h0 = _pool_depth(4.5)
+    kept = _run_pool(be, _barriers(_basin(), _dam()), h0)
+    spilt = _run_pool(be, _basin(), h0)
+    v0 = _vol(h0)
+    assert _vol(kept[:_DAM_ROW]) > 0.9 * v0
+    assert _vol(spilt[:_DAM_ROW]) < 0.5 * _vol(kept[:_DAM_ROW])
+    assert np.isfinite(kept).all() and kept.min() >= 0.0
+
+
+def gate_reservoir_pool_above_crest_overtops(be):
+    """test_reservoir.py:128 -- overtopping is ordinary solver physics."""
+    bed = _barriers(_basin(), _dam())
+    over = _run_pool(be, bed, _pool_depth(_CREST + 0.5))
+    under = _run_pool(be, bed, _pool_depth(_CREST - 0.5))
+    below_over, below_under = _vol(over[_DAM_ROW + 1 :]), _vol(under[_DAM_ROW + 1 :])
+    assert below_over > 100.0 and below_over > 10.0 * max(below_under, 1e-9)
+
+
+def gate_reservoir_transfer_is_mass_exact(be):
+    """test_reservoir.py:141 -- pool loss == released volume; the domain total moves only by
+    the banked rounding."""
+    dam = _dam()
+    st = be.make(_barriers(_basin(), dam), _RDX, depth=_pool_depth(4.5), manning=0.03)
+    op = be.reservoir(st, dam)
+    before = be.h(st)
+    v_before, pool_before = _vol(before), _vol(before[0:6, :])
+    rec = op.advance(300.0, 300.0)
+    after = be.h(st)
+    v_after, pool_after = _vol(after), _vol(after[0:6, :])
+    banked = be.loss_volume(st)
+    assert abs(rec.volume_m3 / 300.0 - 1.0) < 1e-6
+    assert abs((pool_before - pool_after) / rec.volume_m3 - 1.0) < 1e-9
+    assert abs((v_before - v_after) - banked) <= 1e-9 * v_before
+    assert abs(v_before - v_after) < 1e-6 * v_before
+
+
+def gate_reservoir_release_capped_by_pool(be):
+    """test_reservoir.py:177 -- a rule that outruns its reservoir delivers what it holds."""
+    dam = _dam(release_m3_s=10_000.0)
+    h0 = _pool_depth(2.02)
+    st = be.make(_barriers(_basin(), dam), _RDX, depth=h0, manning=0.03)
+    rec = be.reservoir(st, dam).advance(300.0, 300.0)
+    stored = _vol(h0)
+    assert rec.volume_m3 <= stored + 1e-9 and abs(rec.volume_m3 / stored - 1.0) < 1e-6
+    assert float(be.h(st)[: _DAM_ROW + 1].min()) >= 0.0
+
+
+def gate_reservoir_dry_pool_is_a_no_op(be):
+    """test_reservoir.py:191."""
+    dam = _dam()
+    st = be.make(_barriers(_basin(), dam), _RDX, depth=0.0, manning=0.03)
+    rec = be.reservoir(st, dam).advance(300.0, 300.0)
+    assert rec.stage is None and rec.discharge_m3_s == 0.0 and rec.volume_m3 == 0.0
+
+
+def gate_reservoir_target_stage_draws_down(be):
+    """test_reservoir.py:199 -- the closed-loop rule draws the pool toward its target and eases off."""
+    dam = _dam(release_rule="target_stage", target_stage_m=3.0, release_max_m3_s=8.0)
+    st = be.make(_barriers(_basin(), dam), _RDX, depth=_pool_depth(4.8), manning=0.03)
+    op = be.reservoir(st, dam)
+    recs = [op.advance(300.0 * k, 300.0) for k in range(1, 25)]
+    stages = [r.stage for r in recs]
+    qs = [r.discharge_m3_s for r in recs]
+    assert stages[0] > stages[-1] and qs[0] > qs[-1]
+    assert max(qs) <= dam["release_max_m3_s"] + 1e-9
+    assert stages[-1] >= dam["target_stage_m"] - 0.05 and stages[-1] < 4.8
+
+
+def gate_reservoir_gauge_is_the_deepest_cell(be):
+    """test_reservoir.py:313 -- a film high on a wall of the pool box does not read as the stage."""
+    bed = _basin().copy()
+    bed[0, 0] = 8.0
+    bed[3, 3] = 1.0
+    depth = np.zeros_like(bed)
+    depth[0, 0] = 0.05
+    st = be.make(bed, _RDX, depth=depth, manning=0.03)
+    op = be.reservoir(st, _dam())
+    assert op.pool_stage() is None
+
+
 GATES = {name[len("gate_"):]: fn for name, fn in sorted(globals().items()) if name.startswith("gate_")}

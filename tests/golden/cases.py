@@ -10,8 +10,8 @@ Every optional physics branch of the reference step is reached by at least one
 case: the donor limiter, closed/open/fixed_stage edges, compensated and plain
 uniform rain, compensated and plain rain fields, infiltration, inflow point sources
 (compensated), bedload accumulation with Exner activations and bounds, wet/dry
-fronts, dry cells, one-row domains and sub-grid channels (in and over bank,
-with and without bedload).
+fronts, dry cells, one-row domains, sub-grid channels (in and over bank,
+with and without bedload) and reservoir releases (fixed and target-stage rules).
 """
 
 from __future__ import annotations
@@ -151,6 +151,36 @@ def case_li_channels_sediment():
                 steps=24, alpha=0.7, dt_max=2.0)  # fmt: skip
 
 
+def _reservoir_basin(ny, nx, dam_row, crest):
+    """A flat reservoir floor behind a dam row, a valley falling away below it; the
+    dam cells already raised to the crest (what apply_barriers does)."""
+    z = np.zeros((ny, nx), np.float32)
+    z[: dam_row + 1] = 2.0
+    z[dam_row + 1 :] = np.linspace(2.0, 0.0, ny - dam_row - 1, dtype=np.float32)[:, None]
+    z[dam_row, :] = np.maximum(z[dam_row, :], crest)
+    return z
+
+
+def _reservoir_case(scheme, rule, steps, every, alpha):
+    ny, nx, dam_row, crest = 12, 8, 6, 5.0
+    bed = _reservoir_basin(ny, nx, dam_row, crest)
+    depth = np.zeros((ny, nx), np.float32)
+    depth[:dam_row] = np.maximum(4.6 - bed[:dam_row], 0.0)
+    dam = dict(name="d", kind="dam", cells=[(dam_row, j) for j in range(nx)], crest_m=crest, pool=(0, 0, 5, nx - 1),
+               outlet=(8, 2, 10, 5), interval_s=60.0, **rule)  # fmt: skip
+    return dict(scheme=scheme, bed=bed, dx=10.0, depth=depth, manning=0.03, reservoir=dict(structure=dam, every=every),
+                boundaries=_bc(south="open"), steps=steps, alpha=alpha, dt_max=3.0)  # fmt: skip
+
+
+def case_li_reservoir_fixed():
+    return _reservoir_case("local_inertial", dict(release_rule="fixed", release_m3_s=3.0), 30, 6, 0.7)
+
+
+def case_hllc_reservoir_target_stage():
+    rule = dict(release_rule="target_stage", target_stage_m=3.0, release_max_m3_s=40.0)
+    return _reservoir_case("hllc_fv", rule, 24, 4, 0.45)
+
+
 def case_li_dambreak_row():
     nx, dx = 40, 0.5
     x = (np.arange(nx) + 0.5 - nx / 2.0) * dx
@@ -253,9 +283,11 @@ def run_case(case: dict, api) -> dict:
     inj = api.injector(case, st) if case.get("inflows") else None
     morph = api.morphology(case, st) if case.get("sediment") else None
     every = case["sediment"]["every"] if morph else 0
+    res = api.reservoir(case, st) if case.get("reservoir") else None
+    res_every = case["reservoir"]["every"] if res else 0
     t = 0.0
-    dts, vols = [], []
-    last_act = 0.0
+    dts, vols, releases = [], [], []
+    last_act = last_rel = 0.0
     for k in range(case["steps"]):
         dt = api.compute_dt(st, case["alpha"], case["dt_max"])
         dts.append(dt)
@@ -263,6 +295,10 @@ def run_case(case: dict, api) -> dict:
             vols.append(inj.apply(st, t, dt))
         api.step(st, dt, case.get("rain", 0.0), case.get("rain_scale", 1.0), t)
         t += dt
+        if res is not None and (k + 1) % res_every == 0:
+            rec = res.advance(t, t - last_rel)
+            last_rel = t
+            releases.append([rec.time, np.nan if rec.stage is None else rec.stage, rec.discharge_m3_s, rec.volume_m3])
         if morph is not None and (k + 1) % every == 0:
             morph.advance(t, t - last_act)
             last_act = t
@@ -270,4 +306,6 @@ def run_case(case: dict, api) -> dict:
     out["dts"] = np.asarray(dts, np.float64)
     if inj is not None:
         out["inflow_volumes"] = np.asarray(vols, np.float64)
+    if res is not None:
+        out["releases"] = np.asarray(releases, np.float64)
     return out

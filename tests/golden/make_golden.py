@@ -34,7 +34,9 @@ class ReferenceAPI:
         from solver.core.state import State
         from solver.io.config import Inflow
         from solver.processes.inflow import InflowInjector
+        from solver.io.config import Structure
         from solver.processes.morphology import MorphologyProcess
+        from solver.processes.reservoir import ReservoirOperator
 
         self.State = State
         self.schemes = {"local_inertial": local_inertial, "hllc_fv": hllc}
@@ -44,6 +46,8 @@ class ReferenceAPI:
         self.Inflow = Inflow
         self.InflowInjector = InflowInjector
         self.MorphologyProcess = MorphologyProcess
+        self.Structure = Structure
+        self.ReservoirOperator = ReservoirOperator
         self.case = None
 
     def make_state(self, case):
@@ -90,6 +94,9 @@ class ReferenceAPI:
     def morphology(self, case, st):
         sed = case["sediment"]
         return self.MorphologyProcess(st, 1.0e9, dz_lo=sed["dz_lo"], dz_hi=sed["dz_hi"])
+
+    def reservoir(self, case, st):
+        return self.ReservoirOperator(self.Structure(**case["reservoir"]["structure"]), st)
 
     def outputs(self, st, case):
         out = {"h": st.h.numpy().copy()}

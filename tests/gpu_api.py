@@ -60,6 +60,12 @@ class GpuAPI:
         sed = case["sediment"]
         return MorphologyProcess(st, 1.0e9, dz_lo=sed["dz_lo"], dz_hi=sed["dz_hi"])
 
+    def reservoir(self, case, st):
+        from rbsim.config import Structure
+        from rbsim.processes.reservoir import ReservoirOperator
+
+        return ReservoirOperator(Structure(**case["reservoir"]["structure"]), st)
+
     def outputs(self, st, case):
         out = {"h": st.h.cpu().numpy()}
         if case["scheme"] == "hllc_fv":

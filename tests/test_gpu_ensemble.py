@@ -77,14 +77,14 @@ def test_autotune_picks_a_candidate_and_keeps_results_exact():
     specs = [("local_inertial", 200, 333, 10.0), ("local_inertial", 128, 128, 10.0)]
     members = [_member(s, ny, nx, dx, seed=40 + k) for k, (s, ny, nx, dx) in enumerate(specs)]
 
-    def make(li_v, hl_v):
+    def make(li_v, hl_v, t0):
         e = Ensemble(members, [s[0] for s in specs], alpha=0.7, dt_max=30.0, sync_times=[[1e6]] * 2,
-                     li_variant=li_v, hllc_variant=hl_v, graph_steps=4)  # fmt: skip
+                     li_variant=li_v, hllc_variant=hl_v, graph_steps=4, t0=0.0 if t0 is None else t0)  # fmt: skip
         e.set_targets(1e6)
         return e
 
-    best, timings = autotune(make, probe_replays=1, candidates=[(0, 0), (1, 0), (2, 0)])
-    assert best in timings and len(timings) == 3
+    best, timings, t_reached = autotune(make, probe_replays=1, candidates=[(0, 0), (1, 0), (2, 0)])
+    assert best in timings and len(timings) == 3 and t_reached[0] > 0.0
     steps = [members[0].cur]  # 3 candidates x (1 + 1) replays x 4 steps = 24 steps each
     solo = _member("local_inertial", 200, 333, 10.0, seed=40)
     clk = DeviceClock(solo, "local_inertial", alpha=0.7, dt_max=30.0, sync_times=[1e6], graph_steps=24)

@@ -162,3 +162,35 @@ def test_reruns_are_bitwise_identical(name):
     b = run_case(CASES[name](), GpuAPI())
     for key in a:
         np.testing.assert_array_equal(a[key], b[key], err_msg=key)
+
+
+def _hllc_variants():
+    import ctypes
+
+    from rbsim import _lib
+
+    n = ctypes.c_int32(0)
+    _lib.check(_lib.lib().rb_hllc_kernel_variants(ctypes.byref(n)))
+    return n.value
+
+
+@pytest.mark.parametrize("shape", [(301, 419), (5, 2), (1, 600)])
+def test_every_hllc_kernel_variant_matches_oracle_bitwise(shape):
+    """The stage kernel's variants (tile shape, block size, faces per thread, load batching)
+    are a speed choice only: each reproduces the oracle exactly, on a ragged grid with
+    open and fixed_stage edges and on degenerate shapes."""
+    from gpu_api import GpuAPI
+    from rbsim import _lib
+
+    case = _synthetic_hllc(*shape, seed=13)
+    case["boundaries"] = {"north": "closed", "south": "open", "east": "fixed_stage", "west": "open"}
+    case["stage_curves"] = {"east": [(0.0, 4.0), (10.0, 6.0)]}
+    case["steps"] = 12
+    want = _oracle_outputs(case)
+    L = _lib.lib()
+    try:
+        for v in range(_hllc_variants()):
+            _lib.check(L.rb_hllc_set_kernel_variant(v))
+            _compare(run_case(case, GpuAPI()), want, f"hllc{shape} variant {v}")
+    finally:
+        _lib.check(L.rb_hllc_set_kernel_variant(4))  # the library's default

@@ -122,6 +122,20 @@ def test_config_loader(tmp_path):
     bad.write_text('[meta]\nscheme = "local_inertial"\n[boundaries]\neast = { type = "fixed_stage", level = 1.0 }\n')
     with pytest.raises(ConfigError, match="hllc_fv"):
         load_config(bad)
-    bad.write_text("[channels]\nwidth = 3.0\n")
-    with pytest.raises(ConfigError, match="outside"):
+    bad.write_text("[channels]\nwidth = 3.0\n")  # a width without a bank-full depth
+    with pytest.raises(ConfigError, match="bank-full depth"):
+        load_config(bad)
+    bad.write_text('[meta]\nscheme = "hllc_fv"\n[channels]\nwidth = 3.0\ndepth = 1.0\n')
+    with pytest.raises(ConfigError, match="local_inertial"):
+        load_config(bad)
+    bad.write_text('[channels]\nwidth = 3.0\ndepth = 1.5\nmanning = 0.03\n'
+                   '[[structures]]\nname = "d"\ncells = [[1, 1], [1, 2]]\ncrest_m = 5.0\n'
+                   'release_rule = "fixed"\nrelease_m3_s = 2.0\npool = [0, 0, 0, 4]\noutlet = [3, 2]\n')
+    sc = load_config(bad)
+    assert sc.has_channels and sc.channel_depth == 1.5 and sc.channel_manning == 0.03
+    (dam,) = sc.structures
+    assert dam.outlet == (3, 2, 3, 2) and dam.cells == [(1, 1), (1, 2)] and dam.discharge_at(4.0) == 2.0
+    bad.write_text('[[structures]]\nname = "d"\ncells = [[1, 1]]\ncrest_m = 5.0\nrelease_rule = "fixed"\n'
+                   'release_m3_s = 2.0\npool = [0, 0, 2, 4]\noutlet = [1, 2]\n')
+    with pytest.raises(ConfigError, match="overlaps the pool"):
         load_config(bad)

@@ -78,6 +78,9 @@ class OracleAPI:
 
         return _M()
 
+    def reservoir(self, case, st):
+        return oracle.ReservoirOperator(case["reservoir"]["structure"], st)
+
     def outputs(self, st, case):
         out = {"h": st.h.copy()}
         if case["scheme"] == "hllc_fv":
