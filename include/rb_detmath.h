@@ -29,10 +29,11 @@
  *  of the division-free Newton iteration for the inverse cube root,
  *  w <- w + w (1 - t w^3) / 3, square the error each time (2.6e-4 -> 1.4e-7 ->
  *  4e-14). Then cbrt(t) = t w^2, and the 2^q scaling is exact.
- *  Logarithm: ln d = e ln2 + ln m with m moved into [0.75, 1.5), and
- *  ln m = 2 atanh(s), s = (m-1)/(m+1), |s| <= 1/5, summed to s^9 (abs error < 4e-9).
  *  Exponent offset: x^(p - delta) = x^p * exp(-delta ln x) with |delta ln x| < 1e-5,
- *  so exp(-u) = 1 - u + u^2/2 to 1e-16.
+ *  so exp(-u) = 1 - u + u^2/2 to 1e-16. Because delta < 1e-7, ln x is needed only
+ *  to ~1e-5 absolute for a 1e-12 result: ln x = e ln2 (double) + ln m, with m (the
+ *  float mantissa, exact in float) moved into [0.75, 1.5) and ln m = 2 atanh(s),
+ *  s = (m-1)/(m+1) in float, |s| <= 1/5, summed to s^9 in float (abs error < 2e-7).
  */
 #ifndef RB_DETMATH_H
 #define RB_DETMATH_H
@@ -91,20 +92,20 @@ RB_HD double rb_cbrt_pos(double d) {
   return c * rb_double_of((uint64_t)(q + 1023) << 52);
 }
 
-/* Natural log of a finite d > 0 that is a widened float, absolute error < 4e-9. */
+/* Natural log of a finite d > 0 that is a widened float, absolute error < 3e-7:
+ * enough for the exponent offsets below, which scale it by |delta| < 1e-7. */
 RB_HD double rb_log_pos(double d) {
   const uint64_t b = rb_bits_of(d);
   int e = (int)((b >> 52) & 0x7ff) - 1023;
-  double m = rb_double_of((b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL);
-  if (m >= 1.5) {
-    m = m * 0.5;
+  float m = (float)rb_double_of((b & 0x000fffffffffffffULL) | 0x3ff0000000000000ULL); /* exact */
+  if (m >= 1.5f) {
+    m = m * 0.5f;
     e = e + 1;
   }
-  const double s = (m - 1.0) / (m + 1.0);
-  const double s2 = s * s;
-  const double series =
-      (((((1.0 / 9.0) * s2 + (1.0 / 7.0)) * s2 + (1.0 / 5.0)) * s2 + (1.0 / 3.0)) * s2 + 1.0) * s;
-  return (double)e * 0.6931471805599453 + 2.0 * series;
+  const float s = (m - 1.0f) / (m + 1.0f);
+  const float s2 = s * s;
+  const float series = ((((0.111111112f * s2 + 0.142857149f) * s2 + 0.200000003f) * s2 + 0.333333343f) * s2 + 1.0f) * s;
+  return (double)e * 0.6931471805599453 + 2.0 * (double)series;
 }
 
 /* exp(-delta * ln d) for the tiny exponent offsets above. */
@@ -142,6 +143,27 @@ RB_HD float rb_pow15f(float x) {
   if (!(x >= 0.0f)) return (x - x) / (x - x);
   const double d = (double)x;
   return (float)(d * sqrt(d));
+}
+
+/* (n / d >= 0.0f) for a float quotient, without the division in all but a rare
+ * case, for any n and any non-NaN d with |d| > 1e-12 (the only use: the HLLC
+ * contact-wave sign, solver/core/hllc.py:231-238, whose quotient is read only
+ * through that comparison). IEEE semantics of the quotient: +-0 for n = +-0 or
+ * an infinite d, NaN for NaN n or inf/inf, otherwise the sign of n times the sign
+ * of d, where a negative quotient that underflows rounds to -0 (which compares
+ * >= 0). That last case needs |n / d| <= 2^-150; when |n| > |d| 2^-100 it cannot
+ * happen, and otherwise the quotient itself is formed. */
+RB_HD int rb_quotient_nonneg(float n, float d) {
+  if (!(n == n)) return 0;
+  if (n == 0.0f) return 1;
+  if (d > 3.4028234663852886e38f || d < -3.4028234663852886e38f) {
+    const int n_inf = n > 3.4028234663852886e38f || n < -3.4028234663852886e38f;
+    return n_inf ? 0 : 1;
+  }
+  if ((n > 0.0f) == (d > 0.0f)) return 1;
+  const float an = n < 0.0f ? -n : n, ad = d < 0.0f ? -d : d;
+  if (an > ad * 0x1p-100f) return 0;
+  return n / d >= 0.0f;
 }
 
 #endif /* RB_DETMATH_H */

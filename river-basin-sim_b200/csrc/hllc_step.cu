@@ -84,10 +84,13 @@ __device__ __forceinline__ void hllc_flux(float hl, float ul, float vtl, float h
     fh = (sr * fh_l - sl * fh_r + sl * sr * (hr - hl)) * inv;
     fmn = (sr * fmn_l - sl * fmn_r + sl * sr * (hr * ur - hl * ul)) * inv;
   }
+  // The contact speed s_star is read only through s_star >= 0 (hllc.py:231-238), so
+  // its sign is decided exactly without the division (rb_quotient_nonneg).
   const float den_s = hr * (ur - sr) - hl * (ul - sl);
-  float s_star = 0.5f * (ul + ur);
-  if (fabsf(den_s) > 1.0e-12f) s_star = (sl * hr * (ur - sr) - sr * hl * (ul - sl)) / den_s;
-  const float vt = s_star >= 0.0f ? vtl : vtr;
+  const bool star_nonneg = fabsf(den_s) > 1.0e-12f
+                               ? rb_quotient_nonneg(sl * hr * (ur - sr) - sr * hl * (ul - sl), den_s) != 0
+                               : 0.5f * (ul + ur) >= 0.0f;
+  const float vt = star_nonneg ? vtl : vtr;
   f0 = fh;
   f1 = fmn;
   f2 = fh * vt;
@@ -298,55 +301,58 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       fl = f1;
   };
   if constexpr (FU == 1) {
-    // One face per work item: four cells along the normal.
-    for (int k = threadIdx.x; k < XH * XW; k += NT) {
-      const int a = k / XW, b = k - a * XW;
-      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-      if (gi < 0 || gi >= ny || gj < 0 || gj > nx) continue;
-      const int r = a + 2;  // cell row; stencil columns b .. b+3 (cells gj-2 .. gj+1)
+    // One face per work item: four cells along the normal. x- and y-faces share
+    // one loop, so the last pass over the block is partly filled once, not twice.
+    constexpr int NXF = XH * XW, NF = XH * XW + YH * YW;
+    for (int k = threadIdx.x; k < NF; k += NT) {
       float fh, fl, fr, ft;
-      const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
-      if (kind == RB_BC_OPEN) {
-        const Cell c0{s_h[r][b], s_u[r][b], s_v[r][b], s_z[r][b]};
-        const Cell c1{s_h[r][b + 1], s_u[r][b + 1], s_v[r][b + 1], s_z[r][b + 1]};
-        const Cell c2{s_h[r][b + 2], s_u[r][b + 2], s_v[r][b + 2], s_z[r][b + 2]};
-        const Cell c3{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
-        face_flux(recon(c0, c1, c2), recon(c1, c2, c3), fh, fl, fr, ft);
-      } else {
-        const int ce = gj == 0 ? b + 2 : b + 1;  // the edge cell: column 0 or nx-1
-        edge_flux(kind, gj == 0, Cell{s_h[r][ce], s_u[r][ce], s_v[r][ce], s_z[r][ce]}, gj == 0 ? stage_w : stage_e,
-                  fh, fl, fr, ft);
-      }
-      s_fxh[a][b] = fh;
-      if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
-        s_fxl[a - 1][b - 1] = fl;
-        s_fxr[a - 1][b - 1] = fr;
-        s_fxt[a - 1][b - 1] = ft;
-      }
-    }
-    for (int k = threadIdx.x; k < YH * YW; k += NT) {
-      const int a = k / YW, b = k - a * YW;
-      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-      if (gj < 0 || gj >= nx || gi < 0 || gi > ny) continue;
-      const int c = b + 2;  // cell column; stencil rows a .. a+3 (cells gi-2 .. gi+1)
-      float fh, fl, fr, ft;
-      const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
-      if (kind == RB_BC_OPEN) {
-        const Cell c0{s_h[a][c], s_v[a][c], s_u[a][c], s_z[a][c]};
-        const Cell c1{s_h[a + 1][c], s_v[a + 1][c], s_u[a + 1][c], s_z[a + 1][c]};
-        const Cell c2{s_h[a + 2][c], s_v[a + 2][c], s_u[a + 2][c], s_z[a + 2][c]};
-        const Cell c3{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
-        face_flux(recon(c0, c1, c2), recon(c1, c2, c3), fh, fl, fr, ft);
-      } else {
-        const int re = gi == 0 ? a + 2 : a + 1;  // the edge cell: row 0 or ny-1
-        edge_flux(kind, gi == 0, Cell{s_h[re][c], s_v[re][c], s_u[re][c], s_z[re][c]}, gi == 0 ? stage_n : stage_s,
-                  fh, fl, fr, ft);
-      }
-      s_fyh[a][b] = fh;
-      if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
-        s_fyl[a - 1][b - 1] = fl;
-        s_fyr[a - 1][b - 1] = fr;
-        s_fyt[a - 1][b - 1] = ft;
+      if (k < NXF) {
+        const int a = k / XW, b = k - a * XW;
+        const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+        if (gi < 0 || gi >= ny || gj < 0 || gj > nx) continue;
+        const int r = a + 2;  // cell row; stencil columns b .. b+3 (cells gj-2 .. gj+1)
+        const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
+        if (kind == RB_BC_OPEN) {
+          const Cell c0{s_h[r][b], s_u[r][b], s_v[r][b], s_z[r][b]};
+          const Cell c1{s_h[r][b + 1], s_u[r][b + 1], s_v[r][b + 1], s_z[r][b + 1]};
+          const Cell c2{s_h[r][b + 2], s_u[r][b + 2], s_v[r][b + 2], s_z[r][b + 2]};
+          const Cell c3{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
+          face_flux(recon(c0, c1, c2), recon(c1, c2, c3), fh, fl, fr, ft);
+        } else {
+          const int ce = gj == 0 ? b + 2 : b + 1;  // the edge cell: column 0 or nx-1
+          edge_flux(kind, gj == 0, Cell{s_h[r][ce], s_u[r][ce], s_v[r][ce], s_z[r][ce]},
+                    gj == 0 ? stage_w : stage_e, fh, fl, fr, ft);
+        }
+        s_fxh[a][b] = fh;
+        if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
+          s_fxl[a - 1][b - 1] = fl;
+          s_fxr[a - 1][b - 1] = fr;
+          s_fxt[a - 1][b - 1] = ft;
+        }
+      } else {  // y-faces: normal velocity v, transverse u (hllc.py:357-424)
+        const int ky = k - NXF;
+        const int a = ky / YW, b = ky - a * YW;
+        const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+        if (gj < 0 || gj >= nx || gi < 0 || gi > ny) continue;
+        const int c = b + 2;  // cell column; stencil rows a .. a+3 (cells gi-2 .. gi+1)
+        const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
+        if (kind == RB_BC_OPEN) {
+          const Cell c0{s_h[a][c], s_v[a][c], s_u[a][c], s_z[a][c]};
+          const Cell c1{s_h[a + 1][c], s_v[a + 1][c], s_u[a + 1][c], s_z[a + 1][c]};
+          const Cell c2{s_h[a + 2][c], s_v[a + 2][c], s_u[a + 2][c], s_z[a + 2][c]};
+          const Cell c3{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
+          face_flux(recon(c0, c1, c2), recon(c1, c2, c3), fh, fl, fr, ft);
+        } else {
+          const int re = gi == 0 ? a + 2 : a + 1;  // the edge cell: row 0 or ny-1
+          edge_flux(kind, gi == 0, Cell{s_h[re][c], s_v[re][c], s_u[re][c], s_z[re][c]},
+                    gi == 0 ? stage_n : stage_s, fh, fl, fr, ft);
+        }
+        s_fyh[a][b] = fh;
+        if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
+          s_fyl[a - 1][b - 1] = fl;
+          s_fyr[a - 1][b - 1] = fr;
+          s_fyt[a - 1][b - 1] = ft;
+        }
       }
     }
   } else {
@@ -453,36 +459,39 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
   // 4. limit the tile's mass faces by their donor (hllc.py:739-773); bank the
   //    limited boundary flux of open / fixed_stage edges (hllc.py:638-677).
   double loss = 0.0;
-  for (int k = threadIdx.x; k < TY * (TX + 1); k += NT) {
-    const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
-    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-    if (gi >= ny || gj > nx) continue;
-    float q = s_fxh[a][b];
-    if (q > 0.0f) {
-      if (gj >= 1) q = q * s_beta[a][b - 1];
-    } else if (q < 0.0f) {
-      if (gj <= nx - 1) q = q * s_beta[a][b];
-    }
-    s_fxh[a][b] = q;
-    if (p.ledger != nullptr) {
-      if (gj == 0 && p.bc[RB_EDGE_WEST] != RB_BC_CLOSED) loss -= wt * (double)q;
-      if (gj == nx && (b <= TX || gj == nx) && p.bc[RB_EDGE_EAST] != RB_BC_CLOSED) loss += wt * (double)q;
-    }
-  }
-  for (int k = threadIdx.x; k < (TY + 1) * TX; k += NT) {
-    const int a = 1 + k / TX, b = 1 + (k - (a - 1) * TX);
-    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-    if (gj >= nx || gi > ny) continue;
-    float q = s_fyh[a][b];
-    if (q > 0.0f) {
-      if (gi >= 1) q = q * s_beta[a - 1][b];
-    } else if (q < 0.0f) {
-      if (gi <= ny - 1) q = q * s_beta[a][b];
-    }
-    s_fyh[a][b] = q;
-    if (p.ledger != nullptr) {
-      if (gi == 0 && p.bc[RB_EDGE_NORTH] != RB_BC_CLOSED) loss -= wt * (double)q;
-      if (gi == ny && p.bc[RB_EDGE_SOUTH] != RB_BC_CLOSED) loss += wt * (double)q;
+  constexpr int NLX = TY * (TX + 1), NL = TY * (TX + 1) + (TY + 1) * TX;
+  for (int k = threadIdx.x; k < NL; k += NT) {
+    if (k < NLX) {
+      const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
+      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+      if (gi >= ny || gj > nx) continue;
+      float q = s_fxh[a][b];
+      if (q > 0.0f) {
+        if (gj >= 1) q = q * s_beta[a][b - 1];
+      } else if (q < 0.0f) {
+        if (gj <= nx - 1) q = q * s_beta[a][b];
+      }
+      s_fxh[a][b] = q;
+      if (p.ledger != nullptr) {
+        if (gj == 0 && p.bc[RB_EDGE_WEST] != RB_BC_CLOSED) loss -= wt * (double)q;
+        if (gj == nx && p.bc[RB_EDGE_EAST] != RB_BC_CLOSED) loss += wt * (double)q;
+      }
+    } else {
+      const int ky = k - NLX;
+      const int a = 1 + ky / TX, b = 1 + (ky - (a - 1) * TX);
+      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+      if (gj >= nx || gi > ny) continue;
+      float q = s_fyh[a][b];
+      if (q > 0.0f) {
+        if (gi >= 1) q = q * s_beta[a - 1][b];
+      } else if (q < 0.0f) {
+        if (gi <= ny - 1) q = q * s_beta[a][b];
+      }
+      s_fyh[a][b] = q;
+      if (p.ledger != nullptr) {
+        if (gi == 0 && p.bc[RB_EDGE_NORTH] != RB_BC_CLOSED) loss -= wt * (double)q;
+        if (gi == ny && p.bc[RB_EDGE_SOUTH] != RB_BC_CLOSED) loss += wt * (double)q;
+      }
     }
   }
   __syncthreads();

@@ -280,81 +280,87 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
 
   // 2. unlimited face updates (local_inertial.py:72-129); boundary faces stay 0,
   //    which is the closed boundary (boundaries.py:223-241).
-  for (int k = threadIdx.x; k < XH * XW; k += NT) {
-    const int a = k / XW, b = k - a * XW;
-    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-    float q = 0.0f;
-    if constexpr (!CH) {
-      if (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1) {
-        const float eta_l = s_eta[a + 1][b], eta_r = s_eta[a + 1][b + 1];
-        const float h_flow = rmax(eta_l, eta_r) - rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
-        if (!(h_flow < kHDry)) {
-          const float qo = s_qx[a][b];  // previous discharge, staged above
-          const float n_face = 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]);
+  // x- and y-faces share one loop, so the last pass over the block is partly
+  // filled once, not twice.
+  constexpr int NXF = XH * XW, NF = XH * XW + YH * YW;
+  for (int kk = threadIdx.x; kk < NF; kk += NT) {
+    if (kk < NXF) {
+      const int k = kk;
+      const int a = k / XW, b = k - a * XW;
+      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+      float q = 0.0f;
+      if constexpr (!CH) {
+        if (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1) {
+          const float eta_l = s_eta[a + 1][b], eta_r = s_eta[a + 1][b + 1];
+          const float h_flow = rmax(eta_l, eta_r) - rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
+          if (!(h_flow < kHDry)) {
+            const float qo = s_qx[a][b];  // previous discharge, staged above
+            const float n_face = 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]);
+            const float slope = (eta_r - eta_l) / dx;
+            const float num = qo - kG * h_flow * dt * slope;
+            const float den = manning_denominator(qo, h_flow, n_face, kG, dt);
+            q = num / den;
+          }
+        }
+      } else {  // local_inertial.py:338-384 update_qx_channels
+        float qc = 0.0f, qf = 0.0f;
+        if (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1) {
+          const int r = a + 1, cl = b, cr = b + 1;
+          const float eta_l = s_eta[r][cl], eta_r = s_eta[r][cr];
+          const float eta_max = rmax(eta_l, eta_r);
           const float slope = (eta_r - eta_l) / dx;
-          const float num = qo - kG * h_flow * dt * slope;
-          const float den = manning_denominator(qo, h_flow, n_face, kG, dt);
-          q = num / den;
+          const float z_bank = rmax(s_z[r][cl], s_z[r][cr]);
+          qf = floodplain_flux(S.ch.qxf[a][b], eta_max, slope, z_bank, 0.5f * (s_n[r][cl] + s_n[r][cr]), dt);
+          const float w_face = rmin(S.ch.w[r][cl], S.ch.w[r][cr]);
+          const float z_ch = rmax(s_z[r][cl] - S.ch.d[r][cl], s_z[r][cr] - S.ch.d[r][cr]);
+          qc = channel_flux(S.ch.qxc[a][b], eta_max, slope, w_face, z_bank, z_ch,
+                            0.5f * (S.ch.cn[r][cl] + S.ch.cn[r][cr]), dt);
+          const float frac = w_face / dx;
+          q = qf * (1.0f - frac) + qc * frac;
         }
+        S.ch.qxc[a][b] = qc;
+        S.ch.qxf[a][b] = qf;
       }
-    } else {  // local_inertial.py:338-384 update_qx_channels
-      float qc = 0.0f, qf = 0.0f;
-      if (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1) {
-        const int r = a + 1, cl = b, cr = b + 1;
-        const float eta_l = s_eta[r][cl], eta_r = s_eta[r][cr];
-        const float eta_max = rmax(eta_l, eta_r);
-        const float slope = (eta_r - eta_l) / dx;
-        const float z_bank = rmax(s_z[r][cl], s_z[r][cr]);
-        qf = floodplain_flux(S.ch.qxf[a][b], eta_max, slope, z_bank, 0.5f * (s_n[r][cl] + s_n[r][cr]), dt);
-        const float w_face = rmin(S.ch.w[r][cl], S.ch.w[r][cr]);
-        const float z_ch = rmax(s_z[r][cl] - S.ch.d[r][cl], s_z[r][cr] - S.ch.d[r][cr]);
-        qc = channel_flux(S.ch.qxc[a][b], eta_max, slope, w_face, z_bank, z_ch,
-                          0.5f * (S.ch.cn[r][cl] + S.ch.cn[r][cr]), dt);
-        const float frac = w_face / dx;
-        q = qf * (1.0f - frac) + qc * frac;
-      }
-      S.ch.qxc[a][b] = qc;
-      S.ch.qxf[a][b] = qf;
-    }
-    s_qx[a][b] = q;
-  }
-  for (int k = threadIdx.x; k < YH * YW; k += NT) {
-    const int a = k / YW, b = k - a * YW;
-    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-    float q = 0.0f;
-    if constexpr (!CH) {
-      if (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx) {
-        const float eta_t = s_eta[a][b + 1], eta_b = s_eta[a + 1][b + 1];
-        const float h_flow = rmax(eta_t, eta_b) - rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
-        if (!(h_flow < kHDry)) {
-          const float qo = s_qy[a][b];
-          const float n_face = 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]);
+      s_qx[a][b] = q;
+    } else {
+      const int k = kk - NXF;
+      const int a = k / YW, b = k - a * YW;
+      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+      float q = 0.0f;
+      if constexpr (!CH) {
+        if (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx) {
+          const float eta_t = s_eta[a][b + 1], eta_b = s_eta[a + 1][b + 1];
+          const float h_flow = rmax(eta_t, eta_b) - rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
+          if (!(h_flow < kHDry)) {
+            const float qo = s_qy[a][b];
+            const float n_face = 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]);
+            const float slope = (eta_b - eta_t) / dx;
+            const float num = qo - kG * h_flow * dt * slope;
+            const float den = manning_denominator(qo, h_flow, n_face, kG, dt);
+            q = num / den;
+          }
+        }
+      } else {  // local_inertial.py:387-427 update_qy_channels
+        float qc = 0.0f, qf = 0.0f;
+        if (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx) {
+          const int c = b + 1, rt = a, rb = a + 1;
+          const float eta_t = s_eta[rt][c], eta_b = s_eta[rb][c];
+          const float eta_max = rmax(eta_t, eta_b);
           const float slope = (eta_b - eta_t) / dx;
-          const float num = qo - kG * h_flow * dt * slope;
-          const float den = manning_denominator(qo, h_flow, n_face, kG, dt);
-          q = num / den;
+          const float z_bank = rmax(s_z[rt][c], s_z[rb][c]);
+          qf = floodplain_flux(S.ch.qyf[a][b], eta_max, slope, z_bank, 0.5f * (s_n[rt][c] + s_n[rb][c]), dt);
+          const float w_face = rmin(S.ch.w[rt][c], S.ch.w[rb][c]);
+          const float z_ch = rmax(s_z[rt][c] - S.ch.d[rt][c], s_z[rb][c] - S.ch.d[rb][c]);
+          qc = channel_flux(S.ch.qyc[a][b], eta_max, slope, w_face, z_bank, z_ch,
+                            0.5f * (S.ch.cn[rt][c] + S.ch.cn[rb][c]), dt);
+          const float frac = w_face / dx;
+          q = qf * (1.0f - frac) + qc * frac;
         }
+        S.ch.qyc[a][b] = qc;
+        S.ch.qyf[a][b] = qf;
       }
-    } else {  // local_inertial.py:387-427 update_qy_channels
-      float qc = 0.0f, qf = 0.0f;
-      if (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx) {
-        const int c = b + 1, rt = a, rb = a + 1;
-        const float eta_t = s_eta[rt][c], eta_b = s_eta[rb][c];
-        const float eta_max = rmax(eta_t, eta_b);
-        const float slope = (eta_b - eta_t) / dx;
-        const float z_bank = rmax(s_z[rt][c], s_z[rb][c]);
-        qf = floodplain_flux(S.ch.qyf[a][b], eta_max, slope, z_bank, 0.5f * (s_n[rt][c] + s_n[rb][c]), dt);
-        const float w_face = rmin(S.ch.w[rt][c], S.ch.w[rb][c]);
-        const float z_ch = rmax(s_z[rt][c] - S.ch.d[rt][c], s_z[rb][c] - S.ch.d[rb][c]);
-        qc = channel_flux(S.ch.qyc[a][b], eta_max, slope, w_face, z_bank, z_ch,
-                          0.5f * (S.ch.cn[rt][c] + S.ch.cn[rb][c]), dt);
-        const float frac = w_face / dx;
-        q = qf * (1.0f - frac) + qc * frac;
-      }
-      S.ch.qyc[a][b] = qc;
-      S.ch.qyf[a][b] = qf;
+      s_qy[a][b] = q;
     }
-    s_qy[a][b] = q;
   }
   __syncthreads();
 
@@ -377,39 +383,43 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
     __syncthreads();
 
     // 4. scale each interior face of the tile by its donor's beta (:242-263).
-    for (int k = threadIdx.x; k < TY * (TX + 1); k += NT) {
-      const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
-      const int gj = x0 - 1 + b;
-      if (gj >= 1 && gj <= nx - 1) {
-        const float q = s_qx[a][b];
-        if constexpr (!CH) {
-          if (q > 0.0f)
-            s_qx[a][b] = q * s_beta[a][b - 1];
-          else if (q < 0.0f)
-            s_qx[a][b] = q * s_beta[a][b];
-        } else if (!(q == 0.0f)) {  // local_inertial.py:430-452 limit_qx_channels
-          const float bb = q < 0.0f ? s_beta[a][b] : s_beta[a][b - 1];
-          s_qx[a][b] = q * bb;
-          S.ch.qxc[a][b] = S.ch.qxc[a][b] * bb;
-          S.ch.qxf[a][b] = S.ch.qxf[a][b] * bb;
+    constexpr int NXF_ = TY * (TX + 1), NF_ = TY * (TX + 1) + (TY + 1) * TX;
+    for (int kk = threadIdx.x; kk < NF_; kk += NT) {
+      if (kk < NXF_) {
+        const int k = kk;
+        const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
+        const int gj = x0 - 1 + b;
+        if (gj >= 1 && gj <= nx - 1) {
+          const float q = s_qx[a][b];
+          if constexpr (!CH) {
+            if (q > 0.0f)
+              s_qx[a][b] = q * s_beta[a][b - 1];
+            else if (q < 0.0f)
+              s_qx[a][b] = q * s_beta[a][b];
+          } else if (!(q == 0.0f)) {  // local_inertial.py:430-452 limit_qx_channels
+            const float bb = q < 0.0f ? s_beta[a][b] : s_beta[a][b - 1];
+            s_qx[a][b] = q * bb;
+            S.ch.qxc[a][b] = S.ch.qxc[a][b] * bb;
+            S.ch.qxf[a][b] = S.ch.qxf[a][b] * bb;
+          }
         }
-      }
-    }
-    for (int k = threadIdx.x; k < (TY + 1) * TX; k += NT) {
-      const int a = 1 + k / TX, b = 1 + (k - (a - 1) * TX);
-      const int gi = y0 - 1 + a;
-      if (gi >= 1 && gi <= ny - 1) {
-        const float q = s_qy[a][b];
-        if constexpr (!CH) {
-          if (q > 0.0f)
-            s_qy[a][b] = q * s_beta[a - 1][b];
-          else if (q < 0.0f)
-            s_qy[a][b] = q * s_beta[a][b];
-        } else if (!(q == 0.0f)) {  // local_inertial.py:455-472 limit_qy_channels
-          const float bb = q < 0.0f ? s_beta[a][b] : s_beta[a - 1][b];
-          s_qy[a][b] = q * bb;
-          S.ch.qyc[a][b] = S.ch.qyc[a][b] * bb;
-          S.ch.qyf[a][b] = S.ch.qyf[a][b] * bb;
+      } else {
+        const int k = kk - NXF_;
+        const int a = 1 + k / TX, b = 1 + (k - (a - 1) * TX);
+        const int gi = y0 - 1 + a;
+        if (gi >= 1 && gi <= ny - 1) {
+          const float q = s_qy[a][b];
+          if constexpr (!CH) {
+            if (q > 0.0f)
+              s_qy[a][b] = q * s_beta[a - 1][b];
+            else if (q < 0.0f)
+              s_qy[a][b] = q * s_beta[a][b];
+          } else if (!(q == 0.0f)) {  // local_inertial.py:455-472 limit_qy_channels
+            const float bb = q < 0.0f ? s_beta[a][b] : s_beta[a - 1][b];
+            s_qy[a][b] = q * bb;
+            S.ch.qyc[a][b] = S.ch.qyc[a][b] * bb;
+            S.ch.qyf[a][b] = S.ch.qyf[a][b] * bb;
+          }
         }
       }
     }
@@ -417,74 +427,79 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
   }
 
   // 5. write the tile's faces; integrate bedload on them (sediment.py:218-273).
-  for (int k = threadIdx.x; k < TY * (TX + 1); k += NT) {
-    const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
-    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-    if (gi >= ny || gj > nx || (b == TX + 1 && gj != nx)) continue;
-    const size_t fid = (size_t)gi * (nx + 1) + gj;
-    const float q = s_qx[a][b];
-    qx_out[fid] = q;
-    if constexpr (CH) {
-      p.qxcb[cur ^ 1][fid] = S.ch.qxc[a][b];
-      p.qxfb[cur ^ 1][fid] = S.ch.qxf[a][b];
-      if (p.d50 != nullptr && gj >= 1 && gj <= nx - 1) {  // sediment.py:308-342
-        const int r = a + 1, cl = b, cr = b + 1;
-        const size_t ci = (size_t)gi * nx + gj - 1;
-        const float qs = combined_capacity(
-            S.ch.qxc[a][b], S.ch.qxf[a][b], rmax(s_eta[r][cl], s_eta[r][cr]), rmax(s_z[r][cl], s_z[r][cr]),
-            rmax(s_z[r][cl] - S.ch.d[r][cl], s_z[r][cr] - S.ch.d[r][cr]), rmin(S.ch.w[r][cl], S.ch.w[r][cr]),
-            0.5f * (s_n[r][cl] + s_n[r][cr]), 0.5f * (S.ch.cn[r][cl] + S.ch.cn[r][cr]),
-            0.5f * (p.d50[ci] + p.d50[ci + 1]), dx);
+  // x- and y-faces in one loop, as in the face update.
+  constexpr int NXW = TY * (TX + 1), NW = TY * (TX + 1) + (TY + 1) * TX;
+  for (int kk = threadIdx.x; kk < NW; kk += NT) {
+    if (kk < NXW) {
+      const int k = kk;
+      const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
+      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+      if (gi >= ny || gj > nx || (b == TX + 1 && gj != nx)) continue;
+      const size_t fid = (size_t)gi * (nx + 1) + gj;
+      const float q = s_qx[a][b];
+      qx_out[fid] = q;
+      if constexpr (CH) {
+        p.qxcb[cur ^ 1][fid] = S.ch.qxc[a][b];
+        p.qxfb[cur ^ 1][fid] = S.ch.qxf[a][b];
+        if (p.d50 != nullptr && gj >= 1 && gj <= nx - 1) {  // sediment.py:308-342
+          const int r = a + 1, cl = b, cr = b + 1;
+          const size_t ci = (size_t)gi * nx + gj - 1;
+          const float qs = combined_capacity(
+              S.ch.qxc[a][b], S.ch.qxf[a][b], rmax(s_eta[r][cl], s_eta[r][cr]), rmax(s_z[r][cl], s_z[r][cr]),
+              rmax(s_z[r][cl] - S.ch.d[r][cl], s_z[r][cr] - S.ch.d[r][cr]), rmin(S.ch.w[r][cl], S.ch.w[r][cr]),
+              0.5f * (s_n[r][cl] + s_n[r][cr]), 0.5f * (S.ch.cn[r][cl] + S.ch.cn[r][cr]),
+              0.5f * (p.d50[ci] + p.d50[ci + 1]), dx);
+          float tot = p.qs_int_x[fid], comp = p.qs_comp_x[fid];
+          kahan_add(tot, comp, qs * dt);
+          p.qs_int_x[fid] = tot;
+          p.qs_comp_x[fid] = comp;
+        }
+      } else if (p.d50 != nullptr && gj >= 1 && gj <= nx - 1) {
+        const float eta_max = rmax(s_eta[a + 1][b], s_eta[a + 1][b + 1]);
+        const float z_bank = rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
+        const float h_face = eta_max - z_bank;
+        const size_t cl = (size_t)gi * nx + gj - 1;
+        const float qs = face_capacity(q, h_face, h_face, 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]),
+                                       0.5f * (p.d50[cl] + p.d50[cl + 1]));
         float tot = p.qs_int_x[fid], comp = p.qs_comp_x[fid];
         kahan_add(tot, comp, qs * dt);
         p.qs_int_x[fid] = tot;
         p.qs_comp_x[fid] = comp;
       }
-    } else if (p.d50 != nullptr && gj >= 1 && gj <= nx - 1) {
-      const float eta_max = rmax(s_eta[a + 1][b], s_eta[a + 1][b + 1]);
-      const float z_bank = rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
-      const float h_face = eta_max - z_bank;
-      const size_t cl = (size_t)gi * nx + gj - 1;
-      const float qs = face_capacity(q, h_face, h_face, 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]),
-                                     0.5f * (p.d50[cl] + p.d50[cl + 1]));
-      float tot = p.qs_int_x[fid], comp = p.qs_comp_x[fid];
-      kahan_add(tot, comp, qs * dt);
-      p.qs_int_x[fid] = tot;
-      p.qs_comp_x[fid] = comp;
-    }
-  }
-  for (int k = threadIdx.x; k < (TY + 1) * TX; k += NT) {
-    const int a = 1 + k / TX, b = 1 + (k - (a - 1) * TX);
-    const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-    if (gj >= nx || gi > ny || (a == TY + 1 && gi != ny)) continue;
-    const size_t fid = (size_t)gi * nx + gj;
-    const float q = s_qy[a][b];
-    qy_out[fid] = q;
-    if constexpr (CH) {
-      p.qycb[cur ^ 1][fid] = S.ch.qyc[a][b];
-      p.qyfb[cur ^ 1][fid] = S.ch.qyf[a][b];
-      if (p.d50 != nullptr && gi >= 1 && gi <= ny - 1) {  // sediment.py:345-377
-        const int c = b + 1, rt = a, rb = a + 1;
-        const float qs = combined_capacity(
-            S.ch.qyc[a][b], S.ch.qyf[a][b], rmax(s_eta[rt][c], s_eta[rb][c]), rmax(s_z[rt][c], s_z[rb][c]),
-            rmax(s_z[rt][c] - S.ch.d[rt][c], s_z[rb][c] - S.ch.d[rb][c]), rmin(S.ch.w[rt][c], S.ch.w[rb][c]),
-            0.5f * (s_n[rt][c] + s_n[rb][c]), 0.5f * (S.ch.cn[rt][c] + S.ch.cn[rb][c]),
-            0.5f * (p.d50[fid - nx] + p.d50[fid]), dx);
+    } else {
+      const int k = kk - NXW;
+      const int a = 1 + k / TX, b = 1 + (k - (a - 1) * TX);
+      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+      if (gj >= nx || gi > ny || (a == TY + 1 && gi != ny)) continue;
+      const size_t fid = (size_t)gi * nx + gj;
+      const float q = s_qy[a][b];
+      qy_out[fid] = q;
+      if constexpr (CH) {
+        p.qycb[cur ^ 1][fid] = S.ch.qyc[a][b];
+        p.qyfb[cur ^ 1][fid] = S.ch.qyf[a][b];
+        if (p.d50 != nullptr && gi >= 1 && gi <= ny - 1) {  // sediment.py:345-377
+          const int c = b + 1, rt = a, rb = a + 1;
+          const float qs = combined_capacity(
+              S.ch.qyc[a][b], S.ch.qyf[a][b], rmax(s_eta[rt][c], s_eta[rb][c]), rmax(s_z[rt][c], s_z[rb][c]),
+              rmax(s_z[rt][c] - S.ch.d[rt][c], s_z[rb][c] - S.ch.d[rb][c]), rmin(S.ch.w[rt][c], S.ch.w[rb][c]),
+              0.5f * (s_n[rt][c] + s_n[rb][c]), 0.5f * (S.ch.cn[rt][c] + S.ch.cn[rb][c]),
+              0.5f * (p.d50[fid - nx] + p.d50[fid]), dx);
+          float tot = p.qs_int_y[fid], comp = p.qs_comp_y[fid];
+          kahan_add(tot, comp, qs * dt);
+          p.qs_int_y[fid] = tot;
+          p.qs_comp_y[fid] = comp;
+        }
+      } else if (p.d50 != nullptr && gi >= 1 && gi <= ny - 1) {
+        const float eta_max = rmax(s_eta[a][b + 1], s_eta[a + 1][b + 1]);
+        const float z_bank = rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
+        const float h_face = eta_max - z_bank;
+        const float qs = face_capacity(q, h_face, h_face, 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]),
+                                       0.5f * (p.d50[fid - nx] + p.d50[fid]));
         float tot = p.qs_int_y[fid], comp = p.qs_comp_y[fid];
         kahan_add(tot, comp, qs * dt);
         p.qs_int_y[fid] = tot;
         p.qs_comp_y[fid] = comp;
       }
-    } else if (p.d50 != nullptr && gi >= 1 && gi <= ny - 1) {
-      const float eta_max = rmax(s_eta[a][b + 1], s_eta[a + 1][b + 1]);
-      const float z_bank = rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
-      const float h_face = eta_max - z_bank;
-      const float qs = face_capacity(q, h_face, h_face, 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]),
-                                     0.5f * (p.d50[fid - nx] + p.d50[fid]));
-      float tot = p.qs_int_y[fid], comp = p.qs_comp_y[fid];
-      kahan_add(tot, comp, qs * dt);
-      p.qs_int_y[fid] = tot;
-      p.qs_comp_y[fid] = comp;
     }
   }
 
