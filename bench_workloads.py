@@ -118,6 +118,19 @@ def li_rain_512(args):
             "mass_max_rel_error": ledger.max_rel_error, "roofline": roof}  # fmt: skip
 
 
+def li_rain_2048(args):
+    """The rain-on-grid step at 2048^2 (inputs larger than L2): the LI kernel's roofline."""
+    n, dx = 2048, 10.0
+    rng = np.random.default_rng(1)
+    bed = _bumps(n, n, dx, rng, 40, (0.5, 5.0), (50.0, 1200.0))
+    st = rbsim.State.from_bed(bed, dx, depth=(0.5 + 0.1 * rng.random((n, n))).astype(np.float32), manning=0.03)
+    st.arm_source_compensation()
+    st.set_open_boundaries({e: "open" for e in ("north", "south", "east", "west")})
+    roof = _kernel_roofline(st, "local_inertial", args.steps, 40)
+    return {"workload": "li_rain_2048", "metric": "Gcell-updates/s", "value": roof["gcell_per_s_step"],
+            "steps": args.steps, "roofline": roof}  # fmt: skip
+
+
 def reach_inputs(n=8192, dx=5.0, seed=3):
     rng = np.random.default_rng(seed)
     yy, xx = np.mgrid[0:n, 0:n].astype(np.float32)
@@ -243,6 +256,6 @@ def serve(args):
 
 def run(args):
     torch.cuda.set_device(0)
-    fn = {"li_rain_512": li_rain_512, "li_reach_8192": li_reach_8192, "ensemble_256": ensemble_256,
-          "serve": serve}[args.workload]  # fmt: skip
+    fn = {"li_rain_512": li_rain_512, "li_rain_2048": li_rain_2048, "li_reach_8192": li_reach_8192,
+          "ensemble_256": ensemble_256, "serve": serve}[args.workload]  # fmt: skip
     return fn(args)

@@ -273,6 +273,11 @@ int rb_ensemble_read(const rb_ensemble_layout *L, void *ens, rb_clock_state *out
  * 512 threads). */
 int rb_hllc_set_kernel_variant(int32_t variant);
 int rb_hllc_kernel_variants(int32_t *count);
+/* The same for the local-inertial step (tile 32 x 16, 32 x 32, 64 x 16, 32 x 8, and
+ * 32 x 16 held to 48 registers; a state with sub-grid channels always uses 32 x 16).
+ * The library starts with variant 1 (32 x 32 tiles, 512 threads). */
+int rb_li_set_kernel_variant(int32_t variant);
+int rb_li_kernel_variants(int32_t *count);
 
 /* --- reservoir release (solver/processes/reservoir.py) -------------------------
  * Boxes are inclusive (r0, c0, r1, c1), as Structure.pool / .outlet. h is the

@@ -396,6 +396,19 @@ int rb_hllc_clock_start(const rb_hllc_fields* f, int32_t cur, const rb_clock_con
   return RB_OK;
 }
 
+int rb_li_set_kernel_variant(int32_t variant) {
+  if (!rb::li_set_kernel_variant(variant))
+    return fail(RB_ERR_ARG, "rb_li_set_kernel_variant: variant %d is not in [0, %d)", variant,
+                rb::li_kernel_variant_count());
+  return RB_OK;
+}
+
+int rb_li_kernel_variants(int32_t* count) {
+  if (count == nullptr) return fail(RB_ERR_ARG, "rb_li_kernel_variants: null argument");
+  *count = rb::li_kernel_variant_count();
+  return RB_OK;
+}
+
 int rb_hllc_set_kernel_variant(int32_t variant) {
   if (!rb::hllc_set_kernel_variant(variant))
     return fail(RB_ERR_ARG, "rb_hllc_set_kernel_variant: variant %d is not in [0, %d)", variant,

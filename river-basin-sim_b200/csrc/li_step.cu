@@ -31,6 +31,7 @@
 // reads (4 B each), + d50 and the four transport accumulators (36 B) when
 // morphology is armed. Infiltration and open-edge losses go to one float64 ledger
 // slot per tile instead of a per-cell float64 field.
+#include <atomic>
 #include <cfloat>
 
 #include "rb_common.cuh"
@@ -128,8 +129,8 @@ struct LiSmem : LiGeom<TX, TY> {
   using G = LiGeom<TX, TY>;
   float h[G::RH][G::RW], z[G::RH][G::RW], n[G::RH][G::RW], eta[G::RH][G::RW];
   float qx[G::XH][G::XW], qy[G::YH][G::YW], beta[G::BH][G::BW];
-  double red[8];
-  float redf[8];
+  double red[16];
+  float redf[16];
   LiChanSmem<TX, TY, CH> ch;
 };
 
@@ -137,7 +138,7 @@ struct LiSmem : LiGeom<TX, TY> {
 // Called by every thread of the block; returns uniformly.
 template <int TX, int TY, int NT, bool CH = false>
 __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_t slot, LiSmem<TX, TY, CH>& S) {
-  static_assert(NT / 32 <= 8, "reduction scratch sized for <= 8 warps");
+  static_assert(NT / 32 <= 16, "reduction scratch sized for <= 16 warps");
   using SM = LiSmem<TX, TY, CH>;
   constexpr int RW = SM::RW, RH = SM::RH, XW = SM::XW, XH = SM::XH, YW = SM::YW, YH = SM::YH;
   constexpr int BW = SM::BW, BH = SM::BH;
@@ -575,34 +576,57 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
   __syncthreads();  // the shared tile is reused by the caller's next tile
 }
 
-template <int TX, int TY, int NT, bool CH>
-__global__ void __launch_bounds__(NT) li_step_kernel(const LiParams p) {
+// The single-domain step kernel. MINB is __launch_bounds__' resident-block hint (it
+// caps registers at 65536 / (MINB * NT)).
+template <int TX, int TY, int NT, bool CH, int MINB>
+__global__ void __launch_bounds__(NT, MINB) li_step_kernel(const LiParams p) {
   __shared__ LiSmem<TX, TY, CH> S;
   li_tile<TX, TY, NT, CH>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
 
-template <int TX, int TY, int NT>
+template <int TX, int TY, int NT, bool CH, int MINB>
 static cudaError_t launch_li(const LiParams& p, cudaStream_t s) {
   const dim3 grid((p.nx + TX - 1) / TX, (p.ny + TY - 1) / TY);
-  if (p.cw != nullptr)
-    li_step_kernel<TX, TY, NT, true><<<grid, NT, 0, s>>>(p);
-  else
-    li_step_kernel<TX, TY, NT, false><<<grid, NT, 0, s>>>(p);
+  li_step_kernel<TX, TY, NT, CH, MINB><<<grid, NT, 0, s>>>(p);
   return cudaGetLastError();
 }
 
-cudaError_t li_step_launch(const LiParams& p, cudaStream_t s) {
-  return launch_li<LI_TX, LI_TY, LI_NT>(p, s);
+// Tile variants of the single-domain step (sub-grid channels always use 32 x 16);
+// all compute the same bits. The default is the fastest measured on B200 for the
+// 2048^2 and 4096^2 rain-on-grid steps (ms per 2048^2 step: 0.158, 0.142, 0.145,
+// 0.208, 0.149 for variants 0..4).
+struct LiKernelVariant {
+  int tx, ty, nt;
+};
+static const LiKernelVariant kLiVariants[] = {{32, 16, 256}, {32, 32, 512}, {64, 16, 512}, {32, 8, 256}, {32, 16, 256}};
+constexpr int kNumLiVariants = (int)(sizeof(kLiVariants) / sizeof(kLiVariants[0]));
+constexpr int kDefaultLiVariant = 1;
+static std::atomic<int> g_li_variant{kDefaultLiVariant};
+
+int li_kernel_variant_count() { return kNumLiVariants; }
+bool li_set_kernel_variant(int v) {
+  if (v < 0 || v >= kNumLiVariants) return false;
+  g_li_variant.store(v);
+  return true;
 }
 
-int li_tiles(int ny, int nx) { return ((nx + LI_TX - 1) / LI_TX) * ((ny + LI_TY - 1) / LI_TY); }
+cudaError_t li_step_launch(const LiParams& p, cudaStream_t s) {
+  if (p.cw != nullptr) return launch_li<32, 16, 256, true, 1>(p, s);
+  switch (g_li_variant.load()) {
+    case 0: return launch_li<32, 16, 256, false, 1>(p, s);
+    case 2: return launch_li<64, 16, 512, false, 3>(p, s);
+    case 3: return launch_li<32, 8, 256, false, 1>(p, s);
+    case 4: return launch_li<32, 16, 256, false, 5>(p, s);  // at most 48 registers
+    default: return launch_li<32, 32, 512, false, 3>(p, s);
+  }
+}
 
 // Ensemble: a persistent grid walks the (domain, local tile) work-list of every
 // local-inertial domain; a tile of a domain whose clock is not active returns at
 // its first instruction. Each domain's tiles, ledger slots and clock are its own,
 // so a domain's result does not depend on what else is in the batch.
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT) ens_li_kernel(const LiParams* __restrict__ P, const int2* __restrict__ map,
+__global__ void __launch_bounds__(NT, 4) ens_li_kernel(const LiParams* __restrict__ P, const int2* __restrict__ map,
                                                      long long total) {
   __shared__ LiSmem<TX, TY> S;
   for (long long t = blockIdx.x; t < total; t += gridDim.x) {

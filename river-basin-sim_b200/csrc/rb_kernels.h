@@ -108,7 +108,6 @@ cudaError_t clock_commit_many_launch(DevClock* clocks, int n, cudaStream_t s);
 cudaError_t clock_target_many_launch(DevClock* clocks, int n, const double* t_target, const int* max_steps,
                                      cudaStream_t s);
 cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s);
-int li_tiles(int ny, int nx);
 void li_variant_tile(int variant, int* tx, int* ty);
 void hllc_variant_tile(int variant, int* tx, int* ty);
 int ens_li_grid_size(int variant);
@@ -118,6 +117,8 @@ cudaError_t ens_hllc_launch(int variant, int grid, int stage, const HllcParams* 
                             cudaStream_t s);
 void set_last_error(const char* msg);  // the message rb_last_error returns on this thread
 int hllc_tiles(int ny, int nx);
+int li_kernel_variant_count();
+bool li_set_kernel_variant(int v);
 int hllc_kernel_variant_count();
 bool hllc_set_kernel_variant(int v);
 void hllc_prepare_device();

@@ -122,6 +122,8 @@ SIGNATURES = {
     "rb_ensemble_set_targets": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, _P, _P, _P]),
     "rb_ensemble_enqueue": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, ctypes.c_int32, _P]),
     "rb_ensemble_read": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, _P, _P]),
+    "rb_li_set_kernel_variant": (ctypes.c_int, [ctypes.c_int32]),
+    "rb_li_kernel_variants": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
     "rb_hllc_set_kernel_variant": (ctypes.c_int, [ctypes.c_int32]),
     "rb_hllc_kernel_variants": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
     "rb_li_clock_reseed": (ctypes.c_int, [ctypes.POINTER(LiFields), ctypes.c_int32, _P, _P]),

@@ -45,10 +45,29 @@ def _ptr(t) -> int | None:
 
 
 def _f32(a, shape, device) -> torch.Tensor:
+    """A float32 device copy of a host or device array (numpy, or a torch tensor:
+    a pinned host tensor copies at full bus speed)."""
+    if isinstance(a, torch.Tensor):
+        if tuple(a.shape) != tuple(shape):
+            raise ValueError(f"field shape {tuple(a.shape)} != {shape}")
+        out = torch.empty(shape, dtype=torch.float32, device=device)
+        out.copy_(a)
+        return out
     arr = np.ascontiguousarray(a, dtype=np.float32)
     if arr.shape != shape:
         raise ValueError(f"field shape {arr.shape} != {shape}")
-    return torch.from_numpy(arr.copy()).to(device)
+    if not arr.flags.writeable:  # torch.from_numpy wants a writable buffer
+        arr = arr.copy()
+    return torch.from_numpy(arr).to(device)
+
+
+def _scalar_or_field(v, shape, device, name) -> torch.Tensor:
+    if isinstance(v, torch.Tensor) or not np.isscalar(v):
+        sh = tuple(v.shape) if isinstance(v, torch.Tensor) else np.shape(v)
+        if tuple(sh) != tuple(shape):
+            raise ValueError(f"{name} shape {tuple(sh)} != bed shape {shape}")
+        return _f32(v, shape, device)
+    return torch.full(shape, float(v), dtype=torch.float32, device=device)
 
 
 class _Pair:
@@ -153,18 +172,15 @@ class State:
     def from_bed(cls, bed, dx, *, depth=0.0, manning=0.035, device="cuda") -> State:
         """state.py:179-226: fields from a bed array; depth / manning scalar or field."""
         dev = _device(device)
-        bed = np.ascontiguousarray(bed, dtype=np.float32)
-        ny, nx = bed.shape
+        if not isinstance(bed, torch.Tensor):
+            bed = np.ascontiguousarray(bed, dtype=np.float32)
+        if len(bed.shape) != 2:
+            raise ValueError(f"bed must be 2-D, got shape {tuple(bed.shape)}")
+        ny, nx = (int(v) for v in bed.shape)
         grid = Grid(ny=ny, nx=nx, dx=float(dx))
-        h0 = (np.full((ny, nx), float(depth), np.float32) if np.isscalar(depth)
-              else np.ascontiguousarray(depth, dtype=np.float32))  # fmt: skip
-        if h0.shape != (ny, nx):
-            raise ValueError(f"depth shape {h0.shape} != bed shape {(ny, nx)}")
-        n0 = (np.full((ny, nx), float(manning), np.float32) if np.isscalar(manning)
-              else np.ascontiguousarray(manning, dtype=np.float32))  # fmt: skip
-        if n0.shape != (ny, nx):
-            raise ValueError(f"manning shape {n0.shape} != bed shape {(ny, nx)}")
-        return cls(grid, dev, _f32(h0, (ny, nx), dev), _f32(bed, (ny, nx), dev), _f32(n0, (ny, nx), dev))
+        shape = (ny, nx)
+        return cls(grid, dev, _scalar_or_field(depth, shape, dev, "depth"), _f32(bed, shape, dev),
+                   _scalar_or_field(manning, shape, dev, "manning"))  # fmt: skip
 
     # --- double-buffered fields ---------------------------------------------- #
     def _get(self, pair):

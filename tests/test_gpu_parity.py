@@ -194,3 +194,42 @@ def test_every_hllc_kernel_variant_matches_oracle_bitwise(shape):
             _compare(run_case(case, GpuAPI()), want, f"hllc{shape} variant {v}")
     finally:
         _lib.check(L.rb_hllc_set_kernel_variant(4))  # the library's default
+
+
+@pytest.mark.parametrize("shape", [(333, 517), (1, 700), (37, 3)])
+def test_every_li_kernel_variant_matches_oracle_bitwise(shape):
+    """The local-inertial step's tile variants are a speed choice only."""
+    import ctypes
+
+    from gpu_api import GpuAPI
+    from rbsim import _lib
+
+    case = _synthetic_li(*shape, seed=14)
+    case["steps"] = 15
+    want = _oracle_outputs(case)
+    L = _lib.lib()
+    n = ctypes.c_int32(0)
+    _lib.check(L.rb_li_kernel_variants(ctypes.byref(n)))
+    try:
+        for v in range(n.value):
+            _lib.check(L.rb_li_set_kernel_variant(v))
+            _compare(run_case(case, GpuAPI()), want, f"li{shape} variant {v}")
+    finally:
+        _lib.check(L.rb_li_set_kernel_variant(1))  # the library's default
+
+
+def test_li_reach_8192_matches_oracle_bitwise():
+    """The full-size 8192 x 8192 reach configuration (67 M cells: V valley with a
+    meandering channel, lognormal roughness, infiltration, eight inflow cells, an open
+    downstream edge, bedload with an Exner activation), two steps, bit for bit."""
+    from bench_workloads import reach_inputs
+    from gpu_api import GpuAPI
+
+    z, manning, infil, inflows, depth = reach_inputs(8192, 5.0)
+    n = z.shape[0]
+    case = dict(scheme="local_inertial", bed=z, dx=5.0, depth=depth, manning=manning, infil=infil,
+                inflows=[(inf.cell, inf.hydrograph) for inf in inflows], boundaries={"east": "open"},
+                sediment=dict(d50=np.full((n, n), 0.002, np.float32), porosity=0.4, every=2,
+                              dz_lo=np.full((n, n), -np.inf, np.float32), dz_hi=np.full((n, n), np.inf, np.float32)),
+                steps=2, alpha=0.7, dt_max=30.0)  # fmt: skip
+    _compare(run_case(case, GpuAPI()), _oracle_outputs(case), "reach8192")
