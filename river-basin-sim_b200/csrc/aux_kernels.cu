@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(RED_NT) wavespeed_kernel(const float* __restri
     const float hh = h[k];
     const float c = sqrtf(kG * rmax(hh, 0.0f));
     float s = c;
-    if (hh > kHDry) s = rmax(fabsf(hu[k]) / hh, fabsf(hv[k]) / hh) + c;
+    if (hh > kHDry) s = rmax(div_pos(fabsf(hu[k]), hh), div_pos(fabsf(hv[k]), hh)) + c;
     m = s > m ? s : m;
   }
   block_max_to<RED_NT>(m, key, s_w);

@@ -229,8 +229,8 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       const float hh = h_s[id];
       float u = 0.0f, v = 0.0f;
       if (hh > kHDry) {
-        u = hu_s[id] / hh;
-        v = hv_s[id] / hh;
+        u = div_pos(hu_s[id], hh);
+        v = div_pos(hv_s[id], hh);
       }
       s_h[r][c] = hh;
       s_u[r][c] = u;
@@ -263,8 +263,8 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
         const float hh = lh[i];
         float u = 0.0f, v = 0.0f;
         if (hh > kHDry) {
-          u = lhu[i] / hh;
-          v = lhv[i] / hh;
+          u = div_pos(lhu[i], hh);
+          v = div_pos(lhv[i], hh);
         }
         s_h[r][c] = hh;
         s_u[r][c] = u;
@@ -569,9 +569,14 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
         hu = 0.5f * (g_hun[i] + g_hus[i] + dt * dhu);
         hv = 0.5f * (g_hvn[i] + g_hvs[i] + dt * dhv);
         const float mom = sqrtf(hu * hu + hv * hv);
-        const float denom = manning_denominator(mom, hh, g_n[i], g, dt);
-        hu = hu / denom;
-        hv = hv / denom;
+        // friction (hllc.py:912-939): a zero friction numerator (n = 0 or still
+        // water) makes the denominator exactly 1, so hu and hv stand as they are
+        const float f = g * dt * g_n[i] * g_n[i] * mom;
+        if (!(f == 0.0f)) {
+          const float denom = 1.0f + f / rb_pow73f(hh);
+          hu = (hu == 0.0f && denom > 0.0f) ? hu : hu / denom;
+          hv = (hv == 0.0f && denom > 0.0f) ? hv : hv / denom;
+        }
       }
       if (rain_mode == 1) {
         float comp = p.h_comp[id];
@@ -603,9 +608,9 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       // hllc.py:948-966 _reduce_wavespeed on the new state
       const float cw = sqrtf(g * rmax(hh, 0.0f));
       float s = cw;
-      if (hh > kHDry) s = rmax(fabsf(hu) / hh, fabsf(hv) / hh) + cw;
+      if (hh > kHDry) s = rmax(div_pos(fabsf(hu), hh), div_pos(fabsf(hv), hh)) + cw;
       smax = s > smax ? s : smax;
-      bad |= !(fabsf(hh) <= FLT_MAX);
+      bad |= !(fabsf(hh) <= FLT_MAX) || !(fabsf(hu) <= FLT_MAX) || !(fabsf(hv) <= FLT_MAX);
     }
   }
 

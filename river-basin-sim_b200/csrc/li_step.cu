@@ -42,8 +42,8 @@ namespace rb {
 // sediment.py:161-207 kinematic_shear / shields_number / mpm_capacity / face_capacity.
 __device__ __forceinline__ float face_capacity(float q, float h, float radius, float n, float d50) {
   if (h < kHDry || d50 <= 0.0f || q == 0.0f) return 0.0f;
-  const float tau = kG * n * n * q * q / (h * h * rb_pow13f(radius));
-  const float theta = tau / (1.65f * kG * d50);
+  const float tau = div_pos(kG * n * n * q * q, h * h * rb_pow13f(radius));
+  const float theta = div_pos(tau, 1.65f * kG * d50);
   float qs;
   if (theta <= 0.047f) {
     qs = 0.0f;
@@ -62,14 +62,9 @@ __device__ __forceinline__ float drain(float h_edge, float q_out, float dxdt) {
   return h_edge - removed;
 }
 
-// friction.py:35-58 manning_denominator_radius (hydraulic radius R = A/P).
-__device__ __forceinline__ float manning_denominator_radius(float q_prev, float h_flow, float radius, float n,
-                                                            float g, float dt) {
-  return 1.0f + g * dt * n * n * fabsf(q_prev) / (h_flow * rb_pow43f(radius));
-}
-
-// local_inertial.py:294-320 _channel_flux with channels.py:120-135: the channel
-// component of a face, per unit channel width.
+// local_inertial.py:294-320 _channel_flux with channels.py:120-135 and the
+// hydraulic-radius Manning denominator of friction.py:35-58: the channel component
+// of a face, per unit channel width.
 __device__ __forceinline__ float channel_flux(float q_prev, float eta_max, float slope, float w_face, float z_bank,
                                               float z_ch, float n_ch, float dt) {
   if (w_face <= 0.0f) return 0.0f;
@@ -77,8 +72,11 @@ __device__ __forceinline__ float channel_flux(float q_prev, float eta_max, float
   if (h_ch < kHDry) return 0.0f;
   const float radius = w_face * h_ch / (w_face + 2.0f * h_ch);
   const float num = q_prev - kG * h_ch * dt * slope;
-  const float den = manning_denominator_radius(q_prev, h_ch, radius, n_ch, kG, dt);
-  return num / den;
+  // zero dividends as in manning_divide: a zero friction numerator makes den exactly 1
+  const float f = kG * dt * n_ch * n_ch * fabsf(q_prev);
+  if (f == 0.0f) return num;
+  const float den = 1.0f + f / (h_ch * rb_pow43f(radius));
+  return (num == 0.0f && den > 0.0f) ? num : num / den;
 }
 
 // local_inertial.py:323-336 _floodplain_flux: the plain face update above the banks.
@@ -87,8 +85,7 @@ __device__ __forceinline__ float floodplain_flux(float q_prev, float eta_max, fl
   const float h_fp = eta_max - z_bank;
   if (h_fp < kHDry) return 0.0f;
   const float num = q_prev - kG * h_fp * dt * slope;
-  const float den = manning_denominator(q_prev, h_fp, n_fp, kG, dt);
-  return num / den;
+  return manning_divide(num, q_prev, h_fp, n_fp, kG, dt);
 }
 
 // sediment.py:276-305 _combined_capacity: bedload per unit cell width of a
@@ -297,10 +294,9 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
           if (!(h_flow < kHDry)) {
             const float qo = s_qx[a][b];  // previous discharge, staged above
             const float n_face = 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]);
-            const float slope = (eta_r - eta_l) / dx;
+            const float slope = div_pos(eta_r - eta_l, dx);
             const float num = qo - kG * h_flow * dt * slope;
-            const float den = manning_denominator(qo, h_flow, n_face, kG, dt);
-            q = num / den;
+            q = manning_divide(num, qo, h_flow, n_face, kG, dt);
           }
         }
       } else {  // local_inertial.py:338-384 update_qx_channels
@@ -309,7 +305,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
           const int r = a + 1, cl = b, cr = b + 1;
           const float eta_l = s_eta[r][cl], eta_r = s_eta[r][cr];
           const float eta_max = rmax(eta_l, eta_r);
-          const float slope = (eta_r - eta_l) / dx;
+          const float slope = div_pos(eta_r - eta_l, dx);
           const float z_bank = rmax(s_z[r][cl], s_z[r][cr]);
           qf = floodplain_flux(S.ch.qxf[a][b], eta_max, slope, z_bank, 0.5f * (s_n[r][cl] + s_n[r][cr]), dt);
           const float w_face = rmin(S.ch.w[r][cl], S.ch.w[r][cr]);
@@ -335,10 +331,9 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
           if (!(h_flow < kHDry)) {
             const float qo = s_qy[a][b];
             const float n_face = 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]);
-            const float slope = (eta_b - eta_t) / dx;
+            const float slope = div_pos(eta_b - eta_t, dx);
             const float num = qo - kG * h_flow * dt * slope;
-            const float den = manning_denominator(qo, h_flow, n_face, kG, dt);
-            q = num / den;
+            q = manning_divide(num, qo, h_flow, n_face, kG, dt);
           }
         }
       } else {  // local_inertial.py:387-427 update_qy_channels
@@ -347,7 +342,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
           const int c = b + 1, rt = a, rb = a + 1;
           const float eta_t = s_eta[rt][c], eta_b = s_eta[rb][c];
           const float eta_max = rmax(eta_t, eta_b);
-          const float slope = (eta_b - eta_t) / dx;
+          const float slope = div_pos(eta_b - eta_t, dx);
           const float z_bank = rmax(s_z[rt][c], s_z[rb][c]);
           qf = floodplain_flux(S.ch.qyf[a][b], eta_max, slope, z_bank, 0.5f * (s_n[rt][c] + s_n[rb][c]), dt);
           const float w_face = rmin(S.ch.w[rt][c], S.ch.w[rb][c]);
