@@ -12,9 +12,10 @@ here.
   device: K steps on the device-resident clock (dt, fill_span and rain gating in
   a one-thread plan kernel), replayed as one CUDA graph, timed with CUDA events
   between a barrier + synchronize on each side (max over ranks).
-* ``e2e``: the same metric through the public API from host arrays: the initial
-  fields are uploaded (State.from_bed), K steps run through DeviceClock, and the
-  final depth is read back, all inside the timed region. ``e2e.per_step_api`` is
+* ``e2e``: the same metric through the public API from host memory: the bed and
+  initial depth are copied in from pinned host buffers (State.from_bed), K steps
+  run through DeviceClock, and the final depth is copied back to a pinned buffer,
+  all inside the timed region. ``e2e.per_step_api`` is
   the same through the reference-shaped ``compute_dt`` / ``step`` loop, which reads
   dt back to the host every step as the reference does.
 * ``roofline``: the step's kernels against the measured HBM copy bandwidth, from
@@ -52,6 +53,9 @@ ALPHA = 0.45
 DT_MAX = 30.0
 T_END = 30.0  # simulated horizon of the dam-break configuration
 BYTES_PER_CELL_STEP = 32  # read h, hu, hv, z, n (20 B) + write h, hu, hv (12 B)
+# DRAM bytes (read + write) of one step's two stage launches in one ncu capture of this
+# workload (profiles/hllc_stage_kernel_dambreak_2048.md): 86.6 MB + 165.9 MB.
+NCU_DRAM_BYTES_PER_STEP = 252.4e6
 WORKLOAD = "hllc_dambreak_2048x2048"
 CPU_BAND_ROWS = 256  # the CPU sample: a full-width band of the same dam break
 
@@ -343,7 +347,11 @@ def main(argv=None) -> int:
                                      "replayed as one CUDA graph"},
             "gpu_launches": 3 * K,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / pk["hbm_gbs"], "traffic": None, "peak_source": pk["source"],
+                         "frac": achieved / pk["hbm_gbs"], "traffic": NCU_DRAM_BYTES_PER_STEP,
+                         "traffic_note": "DRAM bytes read + written by stage 1 + stage 2 of one step, from one "
+                                         "ncu capture (profiles/hllc_stage_kernel_dambreak_2048.md); the "
+                                         "algorithmic bytes per step are 134 MB",
+                         "peak_source": pk["source"],
                          "kernel": "hllc_stage_kernel stage 1 + stage 2 (one SSP-RK2 step)",
                          "kernel_ms_mean": mean_kernel_ms,
                          "kernel_timing": f"CUDA events around each stage launch, {len(stage1_ms)} clocked steps "
