@@ -220,7 +220,7 @@ def ensemble_256(args):
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     # the probe replays are real steps of the run; the batch continues from where they stopped
-    best, timings, t_reached = autotune(make, probe_replays=1, candidates=[(0, 0), (1, 0), (2, 0)])
+    best, timings, t_reached = autotune(make, probe_replays=1, candidates=[(0, 0), (1, 0), (2, 0), (3, 0)])
     ens = make(*best, t_reached, graph_steps=32)
     replays = ens.run_until(horizon)
     torch.cuda.synchronize()

@@ -568,14 +568,19 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       if (hh > kHDry) {
         hu = 0.5f * (g_hun[i] + g_hus[i] + dt * dhu);
         hv = 0.5f * (g_hvn[i] + g_hvs[i] + dt * dhv);
-        const float mom = sqrtf(hu * hu + hv * hv);
-        // friction (hllc.py:912-939): a zero friction numerator (n = 0 or still
-        // water) makes the denominator exactly 1, so hu and hv stand as they are
-        const float f = g * dt * g_n[i] * g_n[i] * mom;
-        if (!(f == 0.0f)) {
-          const float denom = 1.0f + f / rb_pow73f(hh);
-          hu = (hu == 0.0f && denom > 0.0f) ? hu : hu / denom;
-          hv = (hv == 0.0f && denom > 0.0f) ? hv : hv / denom;
+        // friction (hllc.py:912-939): the numerator g dt n^2 |q| is zero, and the
+        // denominator exactly 1 so hu and hv stand as they are, whenever n = 0 with a
+        // finite |q|^2 or the water is still with a finite g dt n^2; neither the
+        // square root nor the power is needed then
+        const float m2 = hu * hu + hv * hv;
+        const float k = g * dt * g_n[i] * g_n[i];
+        if (!((k == 0.0f && m2 <= FLT_MAX) || (m2 == 0.0f && k <= FLT_MAX))) {
+          const float f = k * sqrtf(m2);
+          if (!(f == 0.0f)) {
+            const float denom = 1.0f + f / rb_pow73f(hh);
+            hu = (hu == 0.0f && denom > 0.0f) ? hu : hu / denom;
+            hv = (hv == 0.0f && denom > 0.0f) ? hv : hv / denom;
+          }
         }
       }
       if (rain_mode == 1) {
@@ -606,7 +611,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       p.hub[cur ^ 1][id] = hu;
       p.hvb[cur ^ 1][id] = hv;
       // hllc.py:948-966 _reduce_wavespeed on the new state
-      const float cw = sqrtf(g * rmax(hh, 0.0f));
+      const float cw = sqrt_z(g * rmax(hh, 0.0f));
       float s = cw;
       if (hh > kHDry) s = rmax(div_pos(fabsf(hu), hh), div_pos(fabsf(hv), hh)) + cw;
       smax = s > smax ? s : smax;

@@ -621,7 +621,7 @@ cudaError_t li_step_launch(const LiParams& p, cudaStream_t s) {
 // its first instruction. Each domain's tiles, ledger slots and clock are its own,
 // so a domain's result does not depend on what else is in the batch.
 template <int TX, int TY, int NT>
-__global__ void __launch_bounds__(NT, 4) ens_li_kernel(const LiParams* __restrict__ P, const int2* __restrict__ map,
+__global__ void __launch_bounds__(NT, NT >= 512 ? 2 : 4) ens_li_kernel(const LiParams* __restrict__ P, const int2* __restrict__ map,
                                                      long long total) {
   __shared__ LiSmem<TX, TY> S;
   for (long long t = blockIdx.x; t < total; t += gridDim.x) {
@@ -642,8 +642,8 @@ static int ens_li_grid() {
 }
 
 void li_variant_tile(int variant, int* tx, int* ty) {
-  static const int T[3][2] = {{32, 16}, {32, 8}, {64, 8}};
-  const int v = variant < 0 || variant > 2 ? 0 : variant;
+  static const int T[4][2] = {{32, 16}, {32, 8}, {64, 8}, {32, 32}};
+  const int v = variant < 0 || variant > 3 ? 0 : variant;
   *tx = T[v][0];
   *ty = T[v][1];
 }
@@ -652,6 +652,7 @@ int ens_li_grid_size(int variant) {
   switch (variant) {
     case 1: return ens_li_grid<32, 8, 256>();
     case 2: return ens_li_grid<64, 8, 256>();
+    case 3: return ens_li_grid<32, 32, 512>();
     default: return ens_li_grid<32, 16, 256>();
   }
 }
@@ -662,6 +663,7 @@ cudaError_t ens_li_launch(int variant, int grid, const LiParams* P, const int2* 
   switch (variant) {
     case 1: ens_li_kernel<32, 8, 256><<<g, 256, 0, s>>>(P, map, total); break;
     case 2: ens_li_kernel<64, 8, 256><<<g, 256, 0, s>>>(P, map, total); break;
+    case 3: ens_li_kernel<32, 32, 512><<<g, 512, 0, s>>>(P, map, total); break;
     default: ens_li_kernel<32, 16, 256><<<g, 256, 0, s>>>(P, map, total); break;
   }
   return cudaGetLastError();

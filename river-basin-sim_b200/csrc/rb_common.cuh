@@ -31,12 +31,16 @@ __device__ __forceinline__ void kahan_add(float& total, float& comp, float inc) 
   total = t;
 }
 
-// Zero dividends. The IEEE single-precision division takes its slow path when the
+// Zero operands. The IEEE single-precision division takes its slow path when the
 // dividend is zero (about 3x the cost on B200), and still water, dry neighbours and
 // frictionless beds make zero dividends common. For a divisor y > 0 (finite or +inf,
 // never NaN) the quotient of +-0 is that same +-0, so returning x unchanged is the
 // division's exact result. Callers guarantee y > 0.
 __device__ __forceinline__ float div_pos(float x, float y) { return x == 0.0f ? x : x / y; }
+
+// The IEEE square root of a zero argument also leaves its fast path (about 1.6x the
+// cost); sqrt(+-0) is that same +-0.
+__device__ __forceinline__ float sqrt_z(float x) { return x == 0.0f ? x : sqrtf(x); }
 
 // channels.py:58-70 eta_subgrid: the storage curve h -> eta.
 __device__ __forceinline__ float eta_subgrid(float h, float z, float w, float d, float dx) {

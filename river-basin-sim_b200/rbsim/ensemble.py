@@ -24,7 +24,7 @@ import torch
 from . import _lib
 from .state import State
 
-LI_VARIANTS = (0, 1, 2)
+LI_VARIANTS = (0, 1, 2, 3)  # tiles 32x16, 32x8, 64x8, 32x32 (512 threads)
 HLLC_VARIANTS = (0, 1)
 
 
