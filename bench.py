@@ -56,6 +56,9 @@ BYTES_PER_CELL_STEP = 32  # read h, hu, hv, z, n (20 B) + write h, hu, hv (12 B)
 # DRAM bytes (read + write) of one step's two stage launches in one ncu capture of this
 # workload (profiles/hllc_stage_kernel_dambreak_2048.md): 86.6 MB + 165.9 MB.
 NCU_DRAM_BYTES_PER_STEP = 252.4e6
+# The stage kernels are issue-bound: share of issue slots busy in the same capture
+# (stage 1 79.6 %, stage 2 77.4 %).
+NCU_ISSUE_ACTIVE = (0.796, 0.774)
 WORKLOAD = "hllc_dambreak_2048x2048"
 CPU_BAND_ROWS = 256  # the CPU sample: a full-width band of the same dam break
 
@@ -200,7 +203,8 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="rbsim", choices=["rbsim", "reference"])
     ap.add_argument("--workload", default="hllc_dambreak",
-                    choices=["hllc_dambreak", "li_rain_512", "li_rain_2048", "li_reach_8192", "ensemble_256", "serve"],
+                    choices=["hllc_dambreak", "li_rain_512", "li_rain_2048", "hllc_lake_2048", "li_reach_8192",
+                             "ensemble_256", "serve"],
                     help="hllc_dambreak is the headline; the others measure the remaining configurations")
     ap.add_argument("--rates", default="2,10,50", help="serve: arrival rates, requests/s")
     ap.add_argument("--requests", type=int, default=16, help="serve: requests per rate")
@@ -208,7 +212,9 @@ def main(argv=None) -> int:
     if args.workload != "hllc_dambreak" and args.impl == "rbsim":
         import bench_workloads
 
-        print(json.dumps(bench_workloads.run(args)))
+        out = bench_workloads.run(args)
+        if int(os.environ.get("RANK", "0")) == 0:
+            print(json.dumps(out))
         return 0
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -352,6 +358,9 @@ def main(argv=None) -> int:
                                          "ncu capture (profiles/hllc_stage_kernel_dambreak_2048.md); the "
                                          "algorithmic bytes per step are 134 MB",
                          "peak_source": pk["source"],
+                         "issue_bound": {"issue_slots_busy_stage1": NCU_ISSUE_ACTIVE[0],
+                                         "issue_slots_busy_stage2": NCU_ISSUE_ACTIVE[1],
+                                         "source": "ncu capture in profiles/hllc_stage_kernel_dambreak_2048.md"},
                          "kernel": "hllc_stage_kernel stage 1 + stage 2 (one SSP-RK2 step)",
                          "kernel_ms_mean": mean_kernel_ms,
                          "kernel_timing": f"CUDA events around each stage launch, {len(stage1_ms)} clocked steps "

@@ -10,6 +10,12 @@
   hydrograph split over the 8 inlet channel cells, MPM bedload (d50 2 mm), open
   downstream edge; the first K steps (the full 12 h is ~10^5 steps), fused step
   roofline at 72 B/cell-step.
+* ``li_rain_2048``: the rain-on-grid step at 2048 x 2048 (inputs larger than L2),
+  the LI kernel's roofline point.
+* ``hllc_lake_2048``: HLLC lake at rest, 2048 x 2048, dx 1 m, surface 2 m over
+  seeded Gaussian bumps (amplitude 0.5-3.5 m, sigma 10-80 m) that pierce it, n 0.03,
+  closed walls: the well-balanced case with dry islands and shorelines. Reports
+  throughput and the largest |u|, |v| after the timed steps (round-off level).
 * ``ensemble_256``: 256 local-inertial domains, sides log-uniform in [128, 2048],
   each with its own rain U(10, 100) mm/h and Manning U(0.02, 0.06), to 1800 s:
   the batched ensemble (autotuned tiles) against the plain per-domain loop
@@ -131,6 +137,37 @@ def li_rain_2048(args):
             "steps": args.steps, "roofline": roof}  # fmt: skip
 
 
+def hllc_lake_2048(args):
+    from rbsim.schemes import hllc
+
+    n, dx = 2048, 1.0
+    rng = np.random.default_rng(2)
+    bed = _bumps(n, n, dx, rng, 40, (0.5, 3.5), (10.0, 80.0), slope=0.0)
+    depth = np.maximum(2.0 - bed, 0.0).astype(np.float32)
+    st = rbsim.State.from_bed(bed, dx, depth=depth, manning=0.03)
+    hllc.arm_hllc(st)
+    K = args.steps
+    clk = DeviceClock(st, "hllc_fv", alpha=0.45, dt_max=30.0, sync_times=[600.0], graph_steps=K)
+    clk.run_until(600.0, max_steps=K)  # capture + warm
+    torch.cuda.synchronize()
+    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clk.set_target(600.0, K)
+    start.record()
+    clk._replay()
+    stop.record()
+    torch.cuda.synchronize()
+    clk.read()
+    ms = start.elapsed_time(stop) / K
+    u, v = st.velocities_numpy()
+    h = st.h.cpu().numpy()
+    speed = np.maximum(np.abs(u), np.abs(v))
+    deep = h > 0.1
+    return {"workload": "hllc_lake_2048", "metric": "Gcell-updates/s", "value": n * n / (ms / 1e3) / 1e9,
+            "ms_per_step": ms, "steps": K, "dry_fraction": float((h < 1e-3).mean()),
+            "max_speed_after": float(speed.max()),
+            "max_speed_where_deeper_than_0.1m": float(speed[deep].max()) if deep.any() else 0.0}  # fmt: skip
+
+
 def reach_inputs(n=8192, dx=5.0, seed=3):
     rng = np.random.default_rng(seed)
     yy, xx = np.mgrid[0:n, 0:n].astype(np.float32)
@@ -176,8 +213,16 @@ def _ensemble_members(n=256, seed=5):
 
 
 def ensemble_256(args):
+    """Config 4. Under torchrun each rank takes its share of the 256 domains (whole
+    domains, longest first onto the least-loaded rank); solves/s is all domains over
+    the slowest rank's time."""
+    from rbsim import replicas
+
     horizon = 1800.0
-    spec = _ensemble_members()
+    rank, world = replicas.rank_world()
+    all_spec = _ensemble_members()
+    mine = replicas.shard_units([float(b.size) for b, _, _ in all_spec], world)[rank]
+    spec = [all_spec[i] for i in mine]
     cells = sum(b.size for b, _, _ in spec)
 
     def fresh():
@@ -227,14 +272,18 @@ def ensemble_256(args):
     batched_wall = time.perf_counter() - t0
     steps = sum(c.steps for c in ens.clock)
     same = all(np.array_equal(sts[k].h.cpu().numpy(), plain_h[k]) for k in range(len(plain_h)))
+    cell_updates = sum(c.steps * b.size for c, (b, _, _) in zip(ens.clock, spec, strict=True))
+    # whole job: every rank's domains over the slowest rank's time
+    job_rate, job_wall = replicas.whole_job_rate(float(len(spec)), batched_wall)
+    plain_rate, plain_job_wall = replicas.whole_job_rate(float(len(spec)), plain_wall)
     return {
-        "workload": "ensemble_256", "metric": "ensemble solves/s", "domains": len(spec), "cells": cells,
-        "batched": {"wall_s": batched_wall, "solves_per_s": len(spec) / batched_wall, "replays": replays,
+        "workload": "ensemble_256", "metric": "ensemble solves/s", "n_gpus": world, "domains": len(all_spec),
+        "domains_this_rank": len(spec), "cells_this_rank": cells,
+        "batched": {"wall_s": job_wall, "solves_per_s": job_rate, "replays": replays,
                     "tiles": {"li_variant": best[0]}, "autotune_ms_per_replay": {str(k): v for k, v in timings.items()},
-                    "gcell_per_s": cells * 0 + sum(c.steps * b.size for c, (b, _, _) in zip(ens.clock, spec)) /
-                    batched_wall / 1e9, "steps": steps},
-        "plain_loop": {"wall_s": plain_wall, "solves_per_s": len(spec) / plain_wall, "steps": plain_steps},
-        "speedup": plain_wall / batched_wall, "first_8_domains_bitwise_equal_to_plain": same,
+                    "gcell_per_s_this_rank": cell_updates / batched_wall / 1e9, "steps": steps},
+        "plain_loop": {"wall_s": plain_job_wall, "solves_per_s": plain_rate, "steps": plain_steps},
+        "speedup": plain_job_wall / job_wall, "first_8_domains_bitwise_equal_to_plain": same,
     }  # fmt: skip
 
 
@@ -255,7 +304,25 @@ def serve(args):
 
 
 def run(args):
-    torch.cuda.set_device(0)
-    fn = {"li_rain_512": li_rain_512, "li_rain_2048": li_rain_2048, "li_reach_8192": li_reach_8192,
-          "ensemble_256": ensemble_256, "serve": serve}[args.workload]  # fmt: skip
-    return fn(args)
+    """Run one workload. Under torchrun (WORLD_SIZE > 1) each rank drives its own GPU
+    and the workloads that shard (ensemble_256) split their units across ranks; the
+    others run one replica per rank."""
+    import os
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
+    fn = {"li_rain_512": li_rain_512, "li_rain_2048": li_rain_2048, "hllc_lake_2048": hllc_lake_2048,
+          "li_reach_8192": li_reach_8192, "ensemble_256": ensemble_256, "serve": serve}[args.workload]  # fmt: skip
+    try:
+        return fn(args)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
