@@ -54,7 +54,7 @@ DT_MAX = 30.0
 T_END = 30.0  # simulated horizon of the dam-break configuration
 BYTES_PER_CELL_STEP = 32  # read h, hu, hv, z, n (20 B) + write h, hu, hv (12 B)
 # DRAM bytes (read + write) of one step's two stage launches in one ncu capture of this
-# workload (profiles/hllc_stage_kernel_dambreak_2048.md): 86.6 MB + 165.9 MB.
+# workload (--set full, 2048^2 dam break, stage 1 + stage 2): 86.6 MB + 165.9 MB.
 NCU_DRAM_BYTES_PER_STEP = 252.4e6
 # The stage kernels are issue-bound: share of issue slots busy in the same capture
 # (stage 1 79.6 %, stage 2 77.4 %).
@@ -355,12 +355,11 @@ def main(argv=None) -> int:
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                          "frac": achieved / pk["hbm_gbs"], "traffic": NCU_DRAM_BYTES_PER_STEP,
                          "traffic_note": "DRAM bytes read + written by stage 1 + stage 2 of one step, from one "
-                                         "ncu capture (profiles/hllc_stage_kernel_dambreak_2048.md); the "
-                                         "algorithmic bytes per step are 134 MB",
+                                         "ncu capture of this workload; the algorithmic bytes per step are 134 MB",
                          "peak_source": pk["source"],
                          "issue_bound": {"issue_slots_busy_stage1": NCU_ISSUE_ACTIVE[0],
                                          "issue_slots_busy_stage2": NCU_ISSUE_ACTIVE[1],
-                                         "source": "ncu capture in profiles/hllc_stage_kernel_dambreak_2048.md"},
+                                         "source": "the same ncu capture"},
                          "kernel": "hllc_stage_kernel stage 1 + stage 2 (one SSP-RK2 step)",
                          "kernel_ms_mean": mean_kernel_ms,
                          "kernel_timing": f"CUDA events around each stage launch, {len(stage1_ms)} clocked steps "

@@ -7,10 +7,6 @@
 
 namespace rb {
 
-// Tile shapes (cells per CTA) and threads per CTA.
-constexpr int LI_TX = 32, LI_TY = 16, LI_NT = 256;
-constexpr int HLLC_TX = 32, HLLC_TY = 16, HLLC_NT = 256;
-
 // The device-resident clock (solver/scheduler.py:171-246 + compute_dt + the run
 // loop's rain gating and source ledger, run.py:369-388), one per workspace. The
 // plan kernel fills the per-step fields below from the state-derived reduction;
