@@ -166,4 +166,20 @@ RB_HD int rb_quotient_nonneg(float n, float d) {
   return n / d >= 0.0f;
 }
 
+/* x / 9.81f (the float32 gravity of solver/core/grid.py:43), the IEEE quotient
+ * bit for bit, without a division for x >= 2^-99: the method of Brisebarre, Muller
+ * and Raina for division by a constant ("Accelerating correctly rounded
+ * floating-point division when the divisor is known in advance", IEEE Trans.
+ * Computers 53(8), 2004), q = RN(x zh + RN(x zl)) with zh = RN(1/g) and
+ * zl = RN(1/g - zh), one multiply and one fused multiply-add. Whether it is
+ * correctly rounded depends on the divisor; for this one it was checked against
+ * the division for every float from 2^-99 to +inf. Below 2^-99 x zl underflows
+ * and the method can miss, and NaN and negative x are not its business: those
+ * take the division. The only use is the HLLC star-depth estimate
+ * (solver/core/hllc.py:224, hs * hs / g). */
+RB_HD float rb_div_g(float x) {
+  const float g = 9.81f, zh = 0x1.a1887ap-4f, zl = 0x1.dcb5p-38f;
+  return x >= 0x1p-99f ? fmaf(x, zh, x * zl) : x / g;
+}
+
 #endif /* RB_DETMATH_H */

@@ -40,9 +40,9 @@ __global__ void __launch_bounds__(RED_NT) wavespeed_kernel(const float* __restri
   float m = 0.0f;
   for (size_t k = (size_t)blockIdx.x * RED_NT + threadIdx.x; k < n; k += (size_t)gridDim.x * RED_NT) {
     const float hh = h[k];
-    const float c = sqrt_z(kG * rmax(hh, 0.0f));
-    float s = c;
-    if (hh > kHDry) s = rmax(div_pos(fabsf(hu[k]), hh), div_pos(fabsf(hv[k]), hh)) + c;
+    const float c = sqrtf(kG * rmax(hh, 0.0f));
+    const bool wet = hh > kHDry;
+    const float s = wet ? rmax(div_if(wet, fabsf(hu[k]), hh), div_if(wet, fabsf(hv[k]), hh)) + c : c;
     m = s > m ? s : m;
   }
   block_max_to<RED_NT>(m, key, s_w);

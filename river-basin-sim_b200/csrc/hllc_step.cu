@@ -62,7 +62,7 @@ __device__ __forceinline__ void hllc_flux(float hl, float ul, float vtl, float h
     sr = ul + 2.0f * cl;
   } else {
     const float hs = 0.5f * (cl + cr) + 0.25f * (ul - ur);
-    const float h_star = rmax(hs * hs / g, 0.0f);
+    const float h_star = rmax(rb_div_g(hs * hs), 0.0f);  // = hs * hs / g, bit for bit
     const float c_star = sqrtf(g * h_star);
     const float u_star = 0.5f * (ul + ur) + cl - cr;
     sl = rmin(ul - cl, u_star - c_star);
@@ -94,6 +94,22 @@ __device__ __forceinline__ void hllc_flux(float hl, float ul, float vtl, float h
   f0 = fh;
   f1 = fmn;
   f2 = fh * vt;
+}
+
+// hllc.py:262-282 _primitives: u = hu / h and v = hv / h on a wet cell, 0 on a dry
+// one. Still water (hu = hv = 0) is common, and its quotients are the zero momenta
+// themselves, so such cells branch around both divisions (a zero dividend would take
+// the division's slow path); a cell with one zero momentum divides 1 in its place.
+__device__ __forceinline__ void primitives(float h, float hu, float hv, float& u, float& v) {
+  const bool wet = h > kHDry;
+  u = wet ? hu : 0.0f;
+  v = wet ? hv : 0.0f;
+  if (wet && !(hu == 0.0f && hv == 0.0f)) {
+    const float qu = div_in_branch(opaque(hu == 0.0f ? 1.0f : hu), h);
+    const float qv = div_in_branch(opaque(hv == 0.0f ? 1.0f : hv), h);
+    if (hu != 0.0f) u = qu;
+    if (hv != 0.0f) v = qv;
+  }
 }
 
 // A cell of the stencil, in the face's frame: depth, normal and transverse
@@ -128,23 +144,48 @@ __device__ __forceinline__ Rec recon(const Cell& m, const Cell& c, const Cell& p
   return r;
 }
 
-// The face between a left cell's east values and a right cell's west values:
-// Audusse hydrostatic reconstruction and HLLC (hllc.py:344-354), with the left and
-// right bed-slope corrections of the normal momentum flux.
-__device__ __forceinline__ void face_flux(const Rec& L, const Rec& R, float& fh, float& fmn_l, float& fmn_r,
-                                          float& fmt) {
+// Any face of the face loop, between a left cell's east values and a right cell's
+// west values. An interior face (kind open: an inner face, or an open edge with its
+// transmissive clamped stencil) is the Audusse hydrostatic reconstruction and HLLC
+// (hllc.py:344-354) with the left and right bed-slope corrections of the normal
+// momentum flux. A closed or fixed_stage edge face is a ghost-state Riemann problem
+// on the edge cell e (hllc.py:439-628): a reflective wall mirrors e's normal
+// velocity (:442-521), a prescribed surface puts the ghost depth max(stage - z_e, 0)
+// on the outside (:537-628), and only the inward normal-momentum slot is read.
+// `low` is the edge at index 0 (west / north). Both kinds feed one HLLC solve, so
+// the solver is inlined once per loop rather than once per edge case; the operands
+// and every rounding are those of separate calls.
+__device__ __forceinline__ void any_face_flux(const Rec& L, const Rec& R, int kind, bool low, const Cell& e,
+                                              float stage, float& fh, float& fl, float& fr, float& ft) {
   const float g = kG;
   const float h_l = rmax(L.eE - L.zE, 0.0f);
   const float h_r = rmax(R.eW - R.zW, 0.0f);
   const float z_star = rmax(L.zE, R.zW);
   const float hl_star = rmax(L.eE - z_star, 0.0f);
   const float hr_star = rmax(R.eW - z_star, 0.0f);
+  float hl = hl_star, ul = L.nE, vl = L.tE, hr = hr_star, ur = R.nW, vr = R.tW;
+  const bool edge = kind != RB_BC_OPEN;
+  if (edge) {
+    const bool closed = kind == RB_BC_CLOSED;
+    const float h_g = rmax(stage - e.z, 0.0f);
+    hl = (!closed && low) ? h_g : e.h;
+    hr = (!closed && !low) ? h_g : e.h;
+    ul = (closed && low) ? -e.un : e.un;
+    ur = (closed && !low) ? -e.un : e.un;
+    vl = e.ut;
+    vr = e.ut;
+  }
   float f0, f1, f2;
-  hllc_flux(hl_star, L.nE, L.tE, hr_star, R.nW, R.tW, f0, f1, f2);
+  hllc_flux(hl, ul, vl, hr, ur, vr, f0, f1, f2);
   fh = f0;
-  fmn_l = f1 + 0.5f * g * (h_l * h_l - hl_star * hl_star);
-  fmn_r = f1 + 0.5f * g * (h_r * h_r - hr_star * hr_star);
-  fmt = f2;
+  ft = f2;
+  if (!edge) {
+    fl = f1 + 0.5f * g * (h_l * h_l - hl_star * hl_star);
+    fr = f1 + 0.5f * g * (h_r * h_r - hr_star * hr_star);
+  } else {
+    fl = low ? 0.0f : f1;
+    fr = low ? f1 : 0.0f;
+  }
 }
 
 template <int TX, int TY>
@@ -227,11 +268,8 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       const int gi = min(max(y0 - H + r, 0), ny - 1), gj = min(max(x0 - H + c, 0), nx - 1);
       const size_t id = (size_t)gi * nx + gj;
       const float hh = h_s[id];
-      float u = 0.0f, v = 0.0f;
-      if (hh > kHDry) {
-        u = div_pos(hu_s[id], hh);
-        v = div_pos(hv_s[id], hh);
-      }
+      float u, v;
+      primitives(hh, hu_s[id], hv_s[id], u, v);
       s_h[r][c] = hh;
       s_u[r][c] = u;
       s_v[r][c] = v;
@@ -261,11 +299,8 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       if (k < RH * RW) {
         const int r = k / RW, c = k - r * RW;
         const float hh = lh[i];
-        float u = 0.0f, v = 0.0f;
-        if (hh > kHDry) {
-          u = div_pos(lhu[i], hh);
-          v = div_pos(lhv[i], hh);
-        }
+        float u, v;
+        primitives(hh, lhu[i], lhv[i], u, v);
         s_h[r][c] = hh;
         s_u[r][c] = u;
         s_v[r][c] = v;
@@ -275,31 +310,9 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
   }
   __syncthreads();
 
-  // 2. face fluxes (hllc.py:285-424) with boundary corrections (:993-1109).
-  // An edge face (gj == 0 / nx, gi == 0 / ny) of a closed or fixed_stage edge is a
-  // ghost-state Riemann problem on the edge cell e; only the inward normal-momentum
-  // slot is read (hllc.py:439-440).
-  auto edge_flux = [&](int kind, bool low, const Cell& e, float stage, float& fh, float& fl, float& fr, float& ft) {
-    float f1;
-    if (kind == RB_BC_CLOSED) {  // reflective wall, hllc.py:442-521
-      if (low)
-        hllc_flux(e.h, -e.un, e.ut, e.h, e.un, e.ut, fh, f1, ft);
-      else
-        hllc_flux(e.h, e.un, e.ut, e.h, -e.un, e.ut, fh, f1, ft);
-    } else {  // prescribed surface, hllc.py:537-628
-      const float h_g = rmax(stage - e.z, 0.0f);
-      if (low)
-        hllc_flux(h_g, e.un, e.ut, e.h, e.un, e.ut, fh, f1, ft);
-      else
-        hllc_flux(e.h, e.un, e.ut, h_g, e.un, e.ut, fh, f1, ft);
-    }
-    fl = 0.0f;
-    fr = 0.0f;
-    if (low)
-      fr = f1;
-    else
-      fl = f1;
-  };
+  // 2. face fluxes (hllc.py:285-424) with boundary corrections (:993-1109); an edge
+  // face (gj == 0 / nx, gi == 0 / ny) of a closed or fixed_stage edge is the
+  // ghost-state problem of any_face_flux.
   if constexpr (FU == 1) {
     // One face per work item: four cells along the normal. x- and y-faces share
     // one loop, so the last pass over the block is partly filled once, not twice.
@@ -312,17 +325,14 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
         if (gi < 0 || gi >= ny || gj < 0 || gj > nx) continue;
         const int r = a + 2;  // cell row; stencil columns b .. b+3 (cells gj-2 .. gj+1)
         const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
-        if (kind == RB_BC_OPEN) {
-          const Cell c0{s_h[r][b], s_u[r][b], s_v[r][b], s_z[r][b]};
-          const Cell c1{s_h[r][b + 1], s_u[r][b + 1], s_v[r][b + 1], s_z[r][b + 1]};
-          const Cell c2{s_h[r][b + 2], s_u[r][b + 2], s_v[r][b + 2], s_z[r][b + 2]};
-          const Cell c3{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
-          face_flux(recon(c0, c1, c2), recon(c1, c2, c3), fh, fl, fr, ft);
-        } else {
-          const int ce = gj == 0 ? b + 2 : b + 1;  // the edge cell: column 0 or nx-1
-          edge_flux(kind, gj == 0, Cell{s_h[r][ce], s_u[r][ce], s_v[r][ce], s_z[r][ce]},
-                    gj == 0 ? stage_w : stage_e, fh, fl, fr, ft);
-        }
+        const Cell c0{s_h[r][b], s_u[r][b], s_v[r][b], s_z[r][b]};
+        const Cell c1{s_h[r][b + 1], s_u[r][b + 1], s_v[r][b + 1], s_z[r][b + 1]};
+        const Cell c2{s_h[r][b + 2], s_u[r][b + 2], s_v[r][b + 2], s_z[r][b + 2]};
+        const Cell c3{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
+        // at an edge the clamped stencil is in the staged region; the edge cell is
+        // column 0 (c2) or nx-1 (c1)
+        any_face_flux(recon(c0, c1, c2), recon(c1, c2, c3), kind, gj == 0, gj == 0 ? c2 : c1,
+                      gj == 0 ? stage_w : stage_e, fh, fl, fr, ft);
         s_fxh[a][b] = fh;
         if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
           s_fxl[a - 1][b - 1] = fl;
@@ -336,17 +346,13 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
         if (gj < 0 || gj >= nx || gi < 0 || gi > ny) continue;
         const int c = b + 2;  // cell column; stencil rows a .. a+3 (cells gi-2 .. gi+1)
         const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
-        if (kind == RB_BC_OPEN) {
-          const Cell c0{s_h[a][c], s_v[a][c], s_u[a][c], s_z[a][c]};
-          const Cell c1{s_h[a + 1][c], s_v[a + 1][c], s_u[a + 1][c], s_z[a + 1][c]};
-          const Cell c2{s_h[a + 2][c], s_v[a + 2][c], s_u[a + 2][c], s_z[a + 2][c]};
-          const Cell c3{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
-          face_flux(recon(c0, c1, c2), recon(c1, c2, c3), fh, fl, fr, ft);
-        } else {
-          const int re = gi == 0 ? a + 2 : a + 1;  // the edge cell: row 0 or ny-1
-          edge_flux(kind, gi == 0, Cell{s_h[re][c], s_v[re][c], s_u[re][c], s_z[re][c]},
-                    gi == 0 ? stage_n : stage_s, fh, fl, fr, ft);
-        }
+        const Cell c0{s_h[a][c], s_v[a][c], s_u[a][c], s_z[a][c]};
+        const Cell c1{s_h[a + 1][c], s_v[a + 1][c], s_u[a + 1][c], s_z[a + 1][c]};
+        const Cell c2{s_h[a + 2][c], s_v[a + 2][c], s_u[a + 2][c], s_z[a + 2][c]};
+        const Cell c3{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
+        // the edge cell: row 0 (c2) or ny-1 (c1)
+        any_face_flux(recon(c0, c1, c2), recon(c1, c2, c3), kind, gi == 0, gi == 0 ? c2 : c1,
+                      gi == 0 ? stage_n : stage_s, fh, fl, fr, ft);
         s_fyh[a][b] = fh;
         if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
           s_fyl[a - 1][b - 1] = fl;
@@ -379,10 +385,8 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
         if (b < XW && gj >= 0 && gj <= nx) {
           float fh, fl, fr, ft;
           const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
-          if (kind == RB_BC_OPEN)
-            face_flux(left, right, fh, fl, fr, ft);
-          else  // edge cell: column 0 (cp) or nx-1 (c0)
-            edge_flux(kind, gj == 0, gj == 0 ? cp : c0, gj == 0 ? stage_w : stage_e, fh, fl, fr, ft);
+          // edge cell: column 0 (cp) or nx-1 (c0)
+          any_face_flux(left, right, kind, gj == 0, gj == 0 ? cp : c0, gj == 0 ? stage_w : stage_e, fh, fl, fr, ft);
           s_fxh[a][b] = fh;
           if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
             s_fxl[a - 1][b - 1] = fl;
@@ -414,10 +418,8 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
         if (a < YH && gi >= 0 && gi <= ny) {
           float fh, fl, fr, ft;
           const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
-          if (kind == RB_BC_OPEN)
-            face_flux(left, right, fh, fl, fr, ft);
-          else  // edge cell: row 0 (cp) or ny-1 (c0)
-            edge_flux(kind, gi == 0, gi == 0 ? cp : c0, gi == 0 ? stage_n : stage_s, fh, fl, fr, ft);
+          // edge cell: row 0 (cp) or ny-1 (c0)
+          any_face_flux(left, right, kind, gi == 0, gi == 0 ? cp : c0, gi == 0 ? stage_n : stage_s, fh, fl, fr, ft);
           s_fyh[a][b] = fh;
           if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
             s_fyl[a - 1][b - 1] = fl;
@@ -450,53 +452,23 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       const float fb = s_fyh[a + 1][b];
       if (fb > 0.0f) q_out = q_out + fb;
       const float out_depth = dtdx * q_out;
-      if (out_depth > 0.0f) beta = rclamp(s_h[a + 2][b + 2] / out_depth, 0.0f, 1.0f);
+      const bool out = out_depth > 0.0f;
+      const float ratio = div_if(out, s_h[a + 2][b + 2], out_depth);
+      if (out) beta = rclamp(ratio, 0.0f, 1.0f);
     }
     s_beta[a][b] = beta;
   }
   __syncthreads();
 
-  // 4. limit the tile's mass faces by their donor (hllc.py:739-773); bank the
-  //    limited boundary flux of open / fixed_stage edges (hllc.py:638-677).
   double loss = 0.0;
-  constexpr int NLX = TY * (TX + 1), NL = TY * (TX + 1) + (TY + 1) * TX;
-  for (int k = threadIdx.x; k < NL; k += NT) {
-    if (k < NLX) {
-      const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
-      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-      if (gi >= ny || gj > nx) continue;
-      float q = s_fxh[a][b];
-      if (q > 0.0f) {
-        if (gj >= 1) q = q * s_beta[a][b - 1];
-      } else if (q < 0.0f) {
-        if (gj <= nx - 1) q = q * s_beta[a][b];
-      }
-      s_fxh[a][b] = q;
-      if (p.ledger != nullptr) {
-        if (gj == 0 && p.bc[RB_EDGE_WEST] != RB_BC_CLOSED) loss -= wt * (double)q;
-        if (gj == nx && p.bc[RB_EDGE_EAST] != RB_BC_CLOSED) loss += wt * (double)q;
-      }
-    } else {
-      const int ky = k - NLX;
-      const int a = 1 + ky / TX, b = 1 + (ky - (a - 1) * TX);
-      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-      if (gj >= nx || gi > ny) continue;
-      float q = s_fyh[a][b];
-      if (q > 0.0f) {
-        if (gi >= 1) q = q * s_beta[a - 1][b];
-      } else if (q < 0.0f) {
-        if (gi <= ny - 1) q = q * s_beta[a][b];
-      }
-      s_fyh[a][b] = q;
-      if (p.ledger != nullptr) {
-        if (gi == 0 && p.bc[RB_EDGE_NORTH] != RB_BC_CLOSED) loss -= wt * (double)q;
-        if (gi == ny && p.bc[RB_EDGE_SOUTH] != RB_BC_CLOSED) loss += wt * (double)q;
-      }
-    }
-  }
-  __syncthreads();
 
-  // 5. divergence + centred bed source (hllc.py:776-847) and the Heun update.
+  // 4. divergence + centred bed source (hllc.py:776-847) and the Heun update. Each
+  //    cell limits its four mass faces by their donor as it reads them
+  //    (hllc.py:739-773): a face shared by two cells is limited by both with the same
+  //    operands, so both see the same bits, and no pass over the faces and no barrier
+  //    sits between the beta and the update. The cell at a domain edge banks the
+  //    limited flux of its edge face if that edge is open or fixed_stage
+  //    (hllc.py:638-677).
   const float inv_dx = 1.0f / dx;
   const float g = kG;
   float smax = 0.0f;
@@ -530,8 +502,39 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
     if (k >= TX * TY || gi >= ny || gj >= nx) continue;
     const size_t id = (size_t)gi * nx + gj;
     const int R = r + H, Cc = c + H;  // this cell in the staged region
-    const float dh = -((s_fxh[r + 1][c + 2] - s_fxh[r + 1][c + 1]) + (s_fyh[r + 2][c + 1] - s_fyh[r + 1][c + 1])) *
-                     inv_dx;
+    // west / east faces: the donor of q > 0 is the cell to the west, of q < 0 the
+    // cell to the east, and a face with no donor cell inside the domain stays as is
+    float qw = s_fxh[r + 1][c + 1];
+    if (qw > 0.0f) {
+      if (gj >= 1) qw = qw * s_beta[r + 1][c];
+    } else if (qw < 0.0f) {
+      qw = qw * s_beta[r + 1][c + 1];
+    }
+    float qe = s_fxh[r + 1][c + 2];
+    if (qe > 0.0f) {
+      qe = qe * s_beta[r + 1][c + 1];
+    } else if (qe < 0.0f) {
+      if (gj + 1 <= nx - 1) qe = qe * s_beta[r + 1][c + 2];
+    }
+    float qn = s_fyh[r + 1][c + 1];
+    if (qn > 0.0f) {
+      if (gi >= 1) qn = qn * s_beta[r][c + 1];
+    } else if (qn < 0.0f) {
+      qn = qn * s_beta[r + 1][c + 1];
+    }
+    float qs = s_fyh[r + 2][c + 1];
+    if (qs > 0.0f) {
+      qs = qs * s_beta[r + 1][c + 1];
+    } else if (qs < 0.0f) {
+      if (gi + 1 <= ny - 1) qs = qs * s_beta[r + 2][c + 1];
+    }
+    if (p.ledger != nullptr) {
+      if (gj == 0 && p.bc[RB_EDGE_WEST] != RB_BC_CLOSED) loss -= wt * (double)qw;
+      if (gj == nx - 1 && p.bc[RB_EDGE_EAST] != RB_BC_CLOSED) loss += wt * (double)qe;
+      if (gi == 0 && p.bc[RB_EDGE_NORTH] != RB_BC_CLOSED) loss -= wt * (double)qn;
+      if (gi == ny - 1 && p.bc[RB_EDGE_SOUTH] != RB_BC_CLOSED) loss += wt * (double)qs;
+    }
+    const float dh = -((qe - qw) + (qs - qn)) * inv_dx;
     const float hg = s_h[R][Cc];
     const float wx = dryfactor(hg, s_h[R][Cc - 1], s_h[R][Cc + 1]);
     const float wy = dryfactor(hg, s_h[R - 1][Cc], s_h[R + 1][Cc]);
@@ -578,8 +581,8 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
           const float f = k * sqrtf(m2);
           if (!(f == 0.0f)) {
             const float denom = 1.0f + f / rb_pow73f(hh);
-            hu = (hu == 0.0f && denom > 0.0f) ? hu : hu / denom;
-            hv = (hv == 0.0f && denom > 0.0f) ? hv : hv / denom;
+            hu = div_pos(hu, denom);
+            hv = div_pos(hv, denom);
           }
         }
       }
@@ -611,9 +614,9 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       p.hub[cur ^ 1][id] = hu;
       p.hvb[cur ^ 1][id] = hv;
       // hllc.py:948-966 _reduce_wavespeed on the new state
-      const float cw = sqrt_z(g * rmax(hh, 0.0f));
-      float s = cw;
-      if (hh > kHDry) s = rmax(div_pos(fabsf(hu), hh), div_pos(fabsf(hv), hh)) + cw;
+      const float cw = sqrtf(g * rmax(hh, 0.0f));
+      const bool wet = hh > kHDry;
+      const float s = wet ? rmax(div_if(wet, fabsf(hu), hh), div_if(wet, fabsf(hv), hh)) + cw : cw;
       smax = s > smax ? s : smax;
       bad |= !(fabsf(hh) <= FLT_MAX) || !(fabsf(hu) <= FLT_MAX) || !(fabsf(hv) <= FLT_MAX);
     }

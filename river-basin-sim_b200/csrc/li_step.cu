@@ -70,13 +70,13 @@ __device__ __forceinline__ float channel_flux(float q_prev, float eta_max, float
   if (w_face <= 0.0f) return 0.0f;
   const float h_ch = rmin(eta_max, z_bank) - z_ch;
   if (h_ch < kHDry) return 0.0f;
-  const float radius = w_face * h_ch / (w_face + 2.0f * h_ch);
+  const float radius = div_pos(w_face * h_ch, w_face + 2.0f * h_ch);
   const float num = q_prev - kG * h_ch * dt * slope;
   // zero dividends as in manning_divide: a zero friction numerator makes den exactly 1
   const float f = kG * dt * n_ch * n_ch * fabsf(q_prev);
   if (f == 0.0f) return num;
   const float den = 1.0f + f / (h_ch * rb_pow43f(radius));
-  return (num == 0.0f && den > 0.0f) ? num : num / den;
+  return div_pos(num, den);
 }
 
 // local_inertial.py:323-336 _floodplain_flux: the plain face update above the banks.
@@ -99,7 +99,7 @@ __device__ __forceinline__ float combined_capacity(float q_ch, float q_fp, float
     const float h_ch = rmin(eta_max, z_bank) - z_ch;
     if (h_ch >= kHDry) qs_ch = face_capacity(q_ch, h_ch, w_face * h_ch / (w_face + 2.0f * h_ch), n_ch, d50);
   }
-  const float frac = w_face / dx;
+  const float frac = div_pos(w_face, dx);
   return qs_fp * (1.0f - frac) + qs_ch * frac;
 }
 
@@ -312,7 +312,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
           const float z_ch = rmax(s_z[r][cl] - S.ch.d[r][cl], s_z[r][cr] - S.ch.d[r][cr]);
           qc = channel_flux(S.ch.qxc[a][b], eta_max, slope, w_face, z_bank, z_ch,
                             0.5f * (S.ch.cn[r][cl] + S.ch.cn[r][cr]), dt);
-          const float frac = w_face / dx;
+          const float frac = div_pos(w_face, dx);
           q = qf * (1.0f - frac) + qc * frac;
         }
         S.ch.qxc[a][b] = qc;
@@ -349,7 +349,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
           const float z_ch = rmax(s_z[rt][c] - S.ch.d[rt][c], s_z[rb][c] - S.ch.d[rb][c]);
           qc = channel_flux(S.ch.qyc[a][b], eta_max, slope, w_face, z_bank, z_ch,
                             0.5f * (S.ch.cn[rt][c] + S.ch.cn[rb][c]), dt);
-          const float frac = w_face / dx;
+          const float frac = div_pos(w_face, dx);
           q = qf * (1.0f - frac) + qc * frac;
         }
         S.ch.qyc[a][b] = qc;
@@ -374,7 +374,9 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
       const float qb = s_qy[a + 1][b];
       if (qb > 0.0f) q_out = q_out + qb;
       const float out_depth = dtdx * q_out;
-      s_beta[a][b] = out_depth > 0.0f ? rclamp(s_h[a + 1][b + 1] / out_depth, 0.0f, 1.0f) : 1.0f;
+      const bool out = out_depth > 0.0f;
+      const float ratio = div_if(out, s_h[a + 1][b + 1], out_depth);
+      s_beta[a][b] = out ? rclamp(ratio, 0.0f, 1.0f) : 1.0f;
     }
     __syncthreads();
 

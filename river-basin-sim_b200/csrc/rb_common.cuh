@@ -32,23 +32,52 @@ __device__ __forceinline__ void kahan_add(float& total, float& comp, float inc) 
 }
 
 // Zero operands. The IEEE single-precision division takes its slow path when the
-// dividend is zero (about 3x the cost on B200), and still water, dry neighbours and
-// frictionless beds make zero dividends common. For a divisor y > 0 (finite or +inf,
-// never NaN) the quotient of +-0 is that same +-0, so returning x unchanged is the
-// division's exact result. Callers guarantee y > 0.
-__device__ __forceinline__ float div_pos(float x, float y) { return x == 0.0f ? x : x / y; }
+// dividend is zero (about 3x the cost of the fast path on B200) or the divisor is.
+// Still water, dry neighbours and frictionless beds make such operands common, and
+// a guard in the source does not keep them away: the compiler evaluates a guarded
+// division unconditionally and selects the result, so a discarded quotient of a
+// dry cell still pays the slow path. The helpers below give the division 1 in place of an
+// operand that would send it down the slow path, and select the exact result
+// themselves (0 / y = 0 with the dividend's sign for y > 0).
+// `opaque` hides the substituted operand from the optimizer, which would otherwise
+// fold the two selects back into the original division; the move itself compiles to
+// nothing.
+__device__ __forceinline__ float opaque(float v) {
+  float r;
+  asm("mov.b32 %0, %1;" : "=f"(r) : "f"(v));
+  return r;
+}
 
-// The IEEE square root of a zero argument also leaves its fast path (about 1.6x the
-// cost); sqrt(+-0) is that same +-0.
-__device__ __forceinline__ float sqrt_z(float x) { return x == 0.0f ? x : sqrtf(x); }
+// x / y, bit for bit, for any x and y.
+__device__ __forceinline__ float div_pos(float x, float y) {
+  const bool same = x == 0.0f && y > 0.0f;  // the quotient is x itself
+  const float q = opaque(same ? 1.0f : x) / y;
+  return same ? x : q;
+}
+
+// use ? x / y : 0, where the division of an unused lane divides by 1 (its divisor,
+// e.g. the depth of a dry cell, may be 0).
+__device__ __forceinline__ float div_if(bool use, float x, float y) {
+  const float q = div_pos(x, opaque(use ? y : 1.0f));
+  return use ? q : 0.0f;
+}
+
+// The IEEE quotient x / y as inline PTX, which the compiler cannot evaluate ahead
+// of the branch that guards it: for divisions that a data-dependent branch is meant
+// to skip, where an ordinary '/' would be computed for every lane regardless.
+__device__ __forceinline__ float div_in_branch(float x, float y) {
+  float q;
+  asm volatile("div.rn.f32 %0, %1, %2;" : "=f"(q) : "f"(x), "f"(y));
+  return q;
+}
 
 // channels.py:58-70 eta_subgrid: the storage curve h -> eta.
 __device__ __forceinline__ float eta_subgrid(float h, float z, float w, float d, float dx) {
   float eta = h + z;
   if (w > 0.0f && d > 0.0f) {
-    const float h_bf = w * d / dx;
+    const float h_bf = div_pos(w * d, dx);
     if (h <= h_bf)
-      eta = z - d + div_pos(h * dx, w);
+      eta = z - d + div_pos(h * dx, opaque(w > 0.0f ? w : 1.0f));
     else
       eta = z + (h - h_bf);
   }
@@ -59,9 +88,9 @@ __device__ __forceinline__ float eta_subgrid(float h, float z, float w, float d,
 __device__ __forceinline__ float column_depth(float h, float w, float d, float dx) {
   float col = h;
   if (w > 0.0f && d > 0.0f) {
-    const float h_bf = w * d / dx;
+    const float h_bf = div_pos(w * d, dx);
     if (h <= h_bf)
-      col = div_pos(h * dx, w);
+      col = div_pos(h * dx, opaque(w > 0.0f ? w : 1.0f));
     else
       col = d + (h - h_bf);
   }
@@ -80,7 +109,7 @@ __device__ __forceinline__ float manning_divide(float num, float q_prev, float h
   const float f = g * dt * n * n * fabsf(q_prev);
   if (f == 0.0f) return num;
   const float den = 1.0f + f / rb_pow73f(h_flow);
-  return (num == 0.0f && den > 0.0f) ? num : num / den;
+  return div_pos(num, den);
 }
 
 // Float key whose unsigned order is the float order for values >= 0.

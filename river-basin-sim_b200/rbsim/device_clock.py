@@ -25,7 +25,7 @@ import math
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, graphs
 from .scheduler import EPS_T
 from .state import State
 
@@ -111,13 +111,7 @@ class DeviceClock:
             self._enqueue(self.graph_steps, self.state.stream)
             return
         if self._graph is None:
-            g = torch.cuda.CUDAGraph()
-            s = torch.cuda.Stream(self.state.device)
-            s.wait_stream(torch.cuda.current_stream(self.state.device))
-            with torch.cuda.graph(g, stream=s):
-                self._enqueue(self.graph_steps, s.cuda_stream)
-            torch.cuda.current_stream(self.state.device).wait_stream(s)
-            self._graph = g
+            self._graph = graphs.capture(self.state.device, lambda s: self._enqueue(self.graph_steps, s))
         self._graph.replay()
 
     def set_target(self, t_target: float, max_steps: int = 2**31 - 1) -> None:

@@ -21,7 +21,7 @@ import math
 import numpy as np
 import torch
 
-from . import _lib
+from . import _lib, graphs
 from .state import State
 
 LI_VARIANTS = (0, 1, 2, 3)  # tiles 32x16, 32x8, 64x8, 32x32 (512 threads)
@@ -94,14 +94,10 @@ class Ensemble:
 
     def replay(self) -> None:
         if self._graph is None:
-            g = torch.cuda.CUDAGraph()
-            s = torch.cuda.Stream(self.device)
-            s.wait_stream(torch.cuda.current_stream(self.device))
-            with torch.cuda.graph(g, stream=s):
-                _lib.check(self._L.rb_ensemble_enqueue(ctypes.byref(self.layout), self._ws.data_ptr(),
-                                                       self.graph_steps, s.cuda_stream))  # fmt: skip
-            torch.cuda.current_stream(self.device).wait_stream(s)
-            self._graph = g
+            self._graph = graphs.capture(
+                self.device,
+                lambda s: _lib.check(self._L.rb_ensemble_enqueue(ctypes.byref(self.layout), self._ws.data_ptr(),
+                                                                 self.graph_steps, s)))  # fmt: skip
         self._graph.replay()
 
     def read(self):
