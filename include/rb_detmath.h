@@ -145,6 +145,20 @@ RB_HD float rb_pow15f(float x) {
   return (float)(d * sqrt(d));
 }
 
+/* n / d, the IEEE quotient, on a path the caller takes rarely. On the device it is
+ * inline PTX, which the compiler cannot evaluate ahead of the branch that guards it
+ * (an ordinary division would be computed on every lane and selected, and would
+ * cost its full price, or its slow path for a zero operand, on all of them). */
+RB_HD float rb_div_rare(float n, float d) {
+#if defined(__CUDA_ARCH__)
+  float q;
+  asm volatile("div.rn.f32 %0, %1, %2;" : "=f"(q) : "f"(n), "f"(d));
+  return q;
+#else
+  return n / d;
+#endif
+}
+
 /* (n / d >= 0.0f) for a float quotient, without the division in all but a rare
  * case, for any n and any non-NaN d with |d| > 1e-12 (the only use: the HLLC
  * contact-wave sign, solver/core/hllc.py:231-238, whose quotient is read only
@@ -163,7 +177,7 @@ RB_HD int rb_quotient_nonneg(float n, float d) {
   if ((n > 0.0f) == (d > 0.0f)) return 1;
   const float an = n < 0.0f ? -n : n, ad = d < 0.0f ? -d : d;
   if (an > ad * 0x1p-100f) return 0;
-  return n / d >= 0.0f;
+  return rb_div_rare(n, d) >= 0.0f;
 }
 
 /* x / 9.81f (the float32 gravity of solver/core/grid.py:43), the IEEE quotient
@@ -179,7 +193,8 @@ RB_HD int rb_quotient_nonneg(float n, float d) {
  * (solver/core/hllc.py:224, hs * hs / g). */
 RB_HD float rb_div_g(float x) {
   const float g = 9.81f, zh = 0x1.a1887ap-4f, zl = 0x1.dcb5p-38f;
-  return x >= 0x1p-99f ? fmaf(x, zh, x * zl) : x / g;
+  if (x >= 0x1p-99f) return fmaf(x, zh, x * zl);
+  return rb_div_rare(x, g);
 }
 
 #endif /* RB_DETMATH_H */
