@@ -379,62 +379,37 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
       s_beta[a][b] = out ? rclamp(ratio, 0.0f, 1.0f) : 1.0f;
     }
     __syncthreads();
-
-    // 4. scale each interior face of the tile by its donor's beta (:242-263).
-    constexpr int NXF_ = TY * (TX + 1), NF_ = TY * (TX + 1) + (TY + 1) * TX;
-    for (int kk = threadIdx.x; kk < NF_; kk += NT) {
-      if (kk < NXF_) {
-        const int k = kk;
-        const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
-        const int gj = x0 - 1 + b;
-        if (gj >= 1 && gj <= nx - 1) {
-          const float q = s_qx[a][b];
-          if constexpr (!CH) {
-            if (q > 0.0f)
-              s_qx[a][b] = q * s_beta[a][b - 1];
-            else if (q < 0.0f)
-              s_qx[a][b] = q * s_beta[a][b];
-          } else if (!(q == 0.0f)) {  // local_inertial.py:430-452 limit_qx_channels
-            const float bb = q < 0.0f ? s_beta[a][b] : s_beta[a][b - 1];
-            s_qx[a][b] = q * bb;
-            S.ch.qxc[a][b] = S.ch.qxc[a][b] * bb;
-            S.ch.qxf[a][b] = S.ch.qxf[a][b] * bb;
-          }
-        }
-      } else {
-        const int k = kk - NXF_;
-        const int a = 1 + k / TX, b = 1 + (k - (a - 1) * TX);
-        const int gi = y0 - 1 + a;
-        if (gi >= 1 && gi <= ny - 1) {
-          const float q = s_qy[a][b];
-          if constexpr (!CH) {
-            if (q > 0.0f)
-              s_qy[a][b] = q * s_beta[a - 1][b];
-            else if (q < 0.0f)
-              s_qy[a][b] = q * s_beta[a][b];
-          } else if (!(q == 0.0f)) {  // local_inertial.py:455-472 limit_qy_channels
-            const float bb = q < 0.0f ? s_beta[a][b] : s_beta[a - 1][b];
-            s_qy[a][b] = q * bb;
-            S.ch.qyc[a][b] = S.ch.qyc[a][b] * bb;
-            S.ch.qyf[a][b] = S.ch.qyf[a][b] * bb;
-          }
-        }
-      }
-    }
-    __syncthreads();
   }
 
-  // 5. write the tile's faces; integrate bedload on them (sediment.py:218-273).
-  // x- and y-faces in one loop, as in the face update.
+  // 4. scale each interior face of the tile by its donor's beta (:242-263), write
+  //    the tile's faces and integrate bedload on them (sediment.py:218-273). x- and
+  //    y-faces in one loop, as in the face update. The limited discharge goes back
+  //    to shared memory for the continuity below; the east (south) face of a tile
+  //    is limited here but written by the next tile, except at the domain's edge.
   constexpr int NXW = TY * (TX + 1), NW = TY * (TX + 1) + (TY + 1) * TX;
   for (int kk = threadIdx.x; kk < NW; kk += NT) {
     if (kk < NXW) {
       const int k = kk;
       const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
       const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-      if (gi >= ny || gj > nx || (b == TX + 1 && gj != nx)) continue;
+      if (gi >= ny || gj > nx) continue;
+      float q = s_qx[a][b];
+      if (limit && gj >= 1 && gj <= nx - 1) {
+        if constexpr (!CH) {
+          if (q > 0.0f)
+            q = q * s_beta[a][b - 1];
+          else if (q < 0.0f)
+            q = q * s_beta[a][b];
+        } else if (!(q == 0.0f)) {  // local_inertial.py:430-452 limit_qx_channels
+          const float bb = q < 0.0f ? s_beta[a][b] : s_beta[a][b - 1];
+          q = q * bb;
+          S.ch.qxc[a][b] = S.ch.qxc[a][b] * bb;
+          S.ch.qxf[a][b] = S.ch.qxf[a][b] * bb;
+        }
+        s_qx[a][b] = q;
+      }
+      if (b == TX + 1 && gj != nx) continue;
       const size_t fid = (size_t)gi * (nx + 1) + gj;
-      const float q = s_qx[a][b];
       qx_out[fid] = q;
       if constexpr (CH) {
         p.qxcb[cur ^ 1][fid] = S.ch.qxc[a][b];
@@ -468,9 +443,24 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
       const int k = kk - NXW;
       const int a = 1 + k / TX, b = 1 + (k - (a - 1) * TX);
       const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-      if (gj >= nx || gi > ny || (a == TY + 1 && gi != ny)) continue;
+      if (gj >= nx || gi > ny) continue;
+      float q = s_qy[a][b];
+      if (limit && gi >= 1 && gi <= ny - 1) {
+        if constexpr (!CH) {
+          if (q > 0.0f)
+            q = q * s_beta[a - 1][b];
+          else if (q < 0.0f)
+            q = q * s_beta[a][b];
+        } else if (!(q == 0.0f)) {  // local_inertial.py:455-472 limit_qy_channels
+          const float bb = q < 0.0f ? s_beta[a][b] : s_beta[a - 1][b];
+          q = q * bb;
+          S.ch.qyc[a][b] = S.ch.qyc[a][b] * bb;
+          S.ch.qyf[a][b] = S.ch.qyf[a][b] * bb;
+        }
+        s_qy[a][b] = q;
+      }
+      if (a == TY + 1 && gi != ny) continue;
       const size_t fid = (size_t)gi * nx + gj;
-      const float q = s_qy[a][b];
       qy_out[fid] = q;
       if constexpr (CH) {
         p.qycb[cur ^ 1][fid] = S.ch.qyc[a][b];
@@ -501,7 +491,9 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
     }
   }
 
-  // 6. continuity, areal sources, infiltration, open-edge sinks, per tile cell.
+  __syncthreads();
+
+  // 5. continuity, areal sources, infiltration, open-edge sinks, per tile cell.
   const float rain_dt = rain_cont * dt;
   double loss = 0.0;
   float hmax = 0.0f;
