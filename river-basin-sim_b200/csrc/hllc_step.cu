@@ -725,16 +725,30 @@ int hllc_tiles(int ny, int nx) {
 
 // Ensemble: one Heun stage over the (domain, local tile) work-list of every HLLC
 // domain (stage 2 of any domain starts only after stage 1 of all of them, as the
-// single-domain step requires for its own tiles).
+// single-domain step requires for its own tiles). Three resident blocks per SM
+// (at most 80 registers) measured fastest: 0.479 ms per step for 16 domains of
+// 512 x 512 against 0.552 with no register bound and 0.517 with four blocks (which
+// spills).
 template <int TX, int TY, int NT, int STAGE>
-__global__ void __launch_bounds__(NT) ens_hllc_kernel(const HllcParams* __restrict__ P, const int2* __restrict__ map,
-                                                       long long total) {
+__global__ void __launch_bounds__(NT, 768 / NT) ens_hllc_kernel(const HllcParams* __restrict__ P,
+                                                                 const int2* __restrict__ map, long long total) {
   __shared__ HllcSmem<TX, TY> S;
+  // The work item's domain parameters are staged in shared memory: read from there,
+  // the dozens of pointers and scalars need not stay in registers through the tile.
+  __shared__ __align__(16) HllcParams sp;
+  static_assert(sizeof(HllcParams) % 4 == 0, "parameters copied as 32-bit words");
+  constexpr int NW = (int)(sizeof(HllcParams) / 4);
+  static_assert(NW <= NT, "one word per thread");
   for (long long t = blockIdx.x; t < total; t += gridDim.x) {
     const int2 m = map[t];
-    const HllcParams& p = P[m.x];
-    const int tiles_x = (p.nx + TX - 1) / TX;
-    hllc_tile<TX, TY, NT, STAGE>(p, m.y % tiles_x, m.y / tiles_x, (size_t)m.y, S);
+    // every thread is done with the previous item's parameters (a tile of a domain
+    // whose clock is inactive returns without a barrier)
+    __syncthreads();
+    if (threadIdx.x < NW)
+      reinterpret_cast<unsigned*>(&sp)[threadIdx.x] = reinterpret_cast<const unsigned*>(P + m.x)[threadIdx.x];
+    __syncthreads();
+    const int tiles_x = (sp.nx + TX - 1) / TX;
+    hllc_tile<TX, TY, NT, STAGE>(sp, m.y % tiles_x, m.y / tiles_x, (size_t)m.y, S);
   }
 }
 
