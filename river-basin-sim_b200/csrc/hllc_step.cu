@@ -120,14 +120,17 @@ struct Cell {
 
 // MUSCL-minmod reconstruction of one cell to its two faces along the normal
 // (hllc.py:325-342): the east ("E", +1/2) and west ("W", -1/2) values of the water
-// surface, bed, normal and transverse velocity, first order at a dry-adjacent cell.
+// surface, bed, normal and transverse velocity, first order at a dry-adjacent cell;
+// and sz = dryfactor * minmod of the bed, the slope of the cell's centred bed
+// source (hllc.py:805-813, the same operands).
 struct Rec {
-  float eE, zE, nE, tE, eW, zW, nW, tW;
+  float eE, zE, nE, tE, eW, zW, nW, tW, sz;
 };
 
 __device__ __forceinline__ Rec recon(const Cell& m, const Cell& c, const Cell& p) {
   const float em = m.h + m.z, ec = c.h + c.z, ep = p.h + p.z;
-  const float hw = 0.5f * dryfactor(c.h, m.h, p.h);
+  const float dry = dryfactor(c.h, m.h, p.h);
+  const float hw = 0.5f * dry;
   const float me = minmod(ec - em, ep - ec);
   const float mz = minmod(c.z - m.z, p.z - c.z);
   const float mn = minmod(c.un - m.un, p.un - c.un);
@@ -141,6 +144,7 @@ __device__ __forceinline__ Rec recon(const Cell& m, const Cell& c, const Cell& p
   r.nW = c.un - hw * mn;
   r.tE = c.ut + hw * mt;
   r.tW = c.ut - hw * mt;
+  r.sz = dry * mz;
   return r;
 }
 
@@ -154,15 +158,20 @@ __device__ __forceinline__ Rec recon(const Cell& m, const Cell& c, const Cell& p
 // on the outside (:537-628), and only the inward normal-momentum slot is read.
 // `low` is the edge at index 0 (west / north). Both kinds feed one HLLC solve, so
 // the solver is inlined once per loop rather than once per edge case; the operands
-// and every rounding are those of separate calls.
+// and every rounding are those of separate calls. h_l and h_r, the left cell's
+// reconstructed depth at its east face and the right cell's at its west face, are
+// also the depths of those cells' centred bed source (hllc.py:805-813).
 __device__ __forceinline__ void any_face_flux(const Rec& L, const Rec& R, int kind, bool low, const Cell& e,
-                                              float stage, float& fh, float& fl, float& fr, float& ft) {
+                                              float stage, float& fh, float& fl, float& fr, float& ft,
+                                              float& h_l_out, float& h_r_out) {
   const float g = kG;
   const float h_l = rmax(L.eE - L.zE, 0.0f);
   const float h_r = rmax(R.eW - R.zW, 0.0f);
   const float z_star = rmax(L.zE, R.zW);
   const float hl_star = rmax(L.eE - z_star, 0.0f);
   const float hr_star = rmax(R.eW - z_star, 0.0f);
+  h_l_out = h_l;
+  h_r_out = h_r;
   float hl = hl_star, ul = L.nE, vl = L.tE, hr = hr_star, ur = R.nW, vr = R.tW;
   const bool edge = kind != RB_BC_OPEN;
   if (edge) {
@@ -200,6 +209,9 @@ struct HllcSmem {
   float fxl[TY][TX + 1], fxr[TY][TX + 1], fxt[TY][TX + 1];  // tile x-faces
   float fyl[TY + 1][TX], fyr[TY + 1][TX], fyt[TY + 1][TX];  // tile y-faces
   float beta[BH][BW];
+  // per tile cell, from the face phase: the reconstructed depths at the cell's east
+  // (hp) and west (hm) faces and the bed slope sz, along x and along y
+  float hpx[TY][TX], hmx[TY][TX], szx[TY][TX], hpy[TY][TX], hmy[TY][TX], szy[TY][TX];
   double red[16];
   float redf[16];
 };
@@ -313,6 +325,28 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
   // 2. face fluxes (hllc.py:285-424) with boundary corrections (:993-1109); an edge
   // face (gj == 0 / nx, gi == 0 / ny) of a closed or fixed_stage edge is the
   // ghost-state problem of any_face_flux.
+  // The face phase also keeps, for each tile cell, the reconstructed depths of its
+  // east / west (south / north) faces and its bed slope: x-face (a, b) has its left
+  // cell at tile (a - 1, b - 2) and its right cell at (a - 1, b - 1); y-face (a, b)
+  // its upper cell at (a - 2, b - 1) and its lower cell at (a - 1, b - 1).
+  auto keep_x = [&](int a, int b, float h_l, float h_r, float sz_l) {
+    if (a >= 1 && a <= TY) {
+      if (b >= 2 && b <= TX + 1) {
+        S.hpx[a - 1][b - 2] = h_l;
+        S.szx[a - 1][b - 2] = sz_l;
+      }
+      if (b >= 1 && b <= TX) S.hmx[a - 1][b - 1] = h_r;
+    }
+  };
+  auto keep_y = [&](int a, int b, float h_l, float h_r, float sz_l) {
+    if (b >= 1 && b <= TX) {
+      if (a >= 2 && a <= TY + 1) {
+        S.hpy[a - 2][b - 1] = h_l;
+        S.szy[a - 2][b - 1] = sz_l;
+      }
+      if (a >= 1 && a <= TY) S.hmy[a - 1][b - 1] = h_r;
+    }
+  };
   if constexpr (FU == 1) {
     // One face per work item: four cells along the normal. x- and y-faces share
     // one loop, so the last pass over the block is partly filled once, not twice.
@@ -331,8 +365,11 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
         const Cell c3{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
         // at an edge the clamped stencil is in the staged region; the edge cell is
         // column 0 (c2) or nx-1 (c1)
-        any_face_flux(recon(c0, c1, c2), recon(c1, c2, c3), kind, gj == 0, gj == 0 ? c2 : c1,
-                      gj == 0 ? stage_w : stage_e, fh, fl, fr, ft);
+        const Rec L = recon(c0, c1, c2);
+        float h_l, h_r;
+        any_face_flux(L, recon(c1, c2, c3), kind, gj == 0, gj == 0 ? c2 : c1, gj == 0 ? stage_w : stage_e, fh, fl,
+                      fr, ft, h_l, h_r);
+        keep_x(a, b, h_l, h_r, L.sz);
         s_fxh[a][b] = fh;
         if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
           s_fxl[a - 1][b - 1] = fl;
@@ -351,8 +388,11 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
         const Cell c2{s_h[a + 2][c], s_v[a + 2][c], s_u[a + 2][c], s_z[a + 2][c]};
         const Cell c3{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
         // the edge cell: row 0 (c2) or ny-1 (c1)
-        any_face_flux(recon(c0, c1, c2), recon(c1, c2, c3), kind, gi == 0, gi == 0 ? c2 : c1,
-                      gi == 0 ? stage_n : stage_s, fh, fl, fr, ft);
+        const Rec L = recon(c0, c1, c2);
+        float h_l, h_r;
+        any_face_flux(L, recon(c1, c2, c3), kind, gi == 0, gi == 0 ? c2 : c1, gi == 0 ? stage_n : stage_s, fh, fl,
+                      fr, ft, h_l, h_r);
+        keep_y(a, b, h_l, h_r, L.sz);
         s_fyh[a][b] = fh;
         if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
           s_fyl[a - 1][b - 1] = fl;
@@ -386,7 +426,10 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
           float fh, fl, fr, ft;
           const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
           // edge cell: column 0 (cp) or nx-1 (c0)
-          any_face_flux(left, right, kind, gj == 0, gj == 0 ? cp : c0, gj == 0 ? stage_w : stage_e, fh, fl, fr, ft);
+          float h_l, h_r;
+          any_face_flux(left, right, kind, gj == 0, gj == 0 ? cp : c0, gj == 0 ? stage_w : stage_e, fh, fl, fr, ft,
+                        h_l, h_r);
+          keep_x(a, b, h_l, h_r, left.sz);
           s_fxh[a][b] = fh;
           if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
             s_fxl[a - 1][b - 1] = fl;
@@ -419,7 +462,10 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
           float fh, fl, fr, ft;
           const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
           // edge cell: row 0 (cp) or ny-1 (c0)
-          any_face_flux(left, right, kind, gi == 0, gi == 0 ? cp : c0, gi == 0 ? stage_n : stage_s, fh, fl, fr, ft);
+          float h_l, h_r;
+          any_face_flux(left, right, kind, gi == 0, gi == 0 ? cp : c0, gi == 0 ? stage_n : stage_s, fh, fl, fr, ft,
+                        h_l, h_r);
+          keep_y(a, b, h_l, h_r, left.sz);
           s_fyh[a][b] = fh;
           if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
             s_fyl[a - 1][b - 1] = fl;
@@ -536,23 +582,15 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
     }
     const float dh = -((qe - qw) + (qs - qn)) * inv_dx;
     const float hg = s_h[R][Cc];
-    const float wx = dryfactor(hg, s_h[R][Cc - 1], s_h[R][Cc + 1]);
-    const float wy = dryfactor(hg, s_h[R - 1][Cc], s_h[R + 1][Cc]);
-    const float zc = s_z[R][Cc];
-    const float ec = hg + zc;
-    const float sz_x = wx * minmod(zc - s_z[R][Cc - 1], s_z[R][Cc + 1] - zc);
-    const float se_x =
-        wx * minmod(ec - (s_h[R][Cc - 1] + s_z[R][Cc - 1]), (s_h[R][Cc + 1] + s_z[R][Cc + 1]) - ec);
-    const float hp_x = rmax((ec + 0.5f * se_x) - (zc + 0.5f * sz_x), 0.0f);
-    const float hm_x = rmax((ec - 0.5f * se_x) - (zc - 0.5f * sz_x), 0.0f);
-    const float src_x = -g * 0.5f * (hp_x + hm_x) * sz_x;
+    // the centred bed source (hllc.py:805-813): the cell's reconstructed depths at
+    // its two faces and its bed slope, as the face phase computed them (the
+    // reference's hp = max((eta + se/2) - (z + sz/2), 0) is the reconstruction's
+    // east depth bit for bit, hm its west depth)
+    const float sz_x = S.szx[r][c];
+    const float src_x = -g * 0.5f * (S.hpx[r][c] + S.hmx[r][c]) * sz_x;
     const float dhu = (-((s_fxl[r][c + 1] - s_fxr[r][c]) + (s_fyt[r + 1][c] - s_fyt[r][c])) + src_x) * inv_dx;
-    const float sz_y = wy * minmod(zc - s_z[R - 1][Cc], s_z[R + 1][Cc] - zc);
-    const float se_y =
-        wy * minmod(ec - (s_h[R - 1][Cc] + s_z[R - 1][Cc]), (s_h[R + 1][Cc] + s_z[R + 1][Cc]) - ec);
-    const float hp_y = rmax((ec + 0.5f * se_y) - (zc + 0.5f * sz_y), 0.0f);
-    const float hm_y = rmax((ec - 0.5f * se_y) - (zc - 0.5f * sz_y), 0.0f);
-    const float src_y = -g * 0.5f * (hp_y + hm_y) * sz_y;
+    const float sz_y = S.szy[r][c];
+    const float src_y = -g * 0.5f * (S.hpy[r][c] + S.hmy[r][c]) * sz_y;
     const float dhv = (-((s_fyl[r + 1][c] - s_fyr[r][c]) + (s_fxt[r][c + 1] - s_fxt[r][c])) + src_y) * inv_dx;
 
     if (STAGE == 1) {  // hllc.py:850-878
