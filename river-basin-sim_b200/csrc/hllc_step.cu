@@ -22,6 +22,7 @@
 // buffer of the caller's double-buffered (h, hu, hv).
 #include <atomic>
 #include <cfloat>
+#include <type_traits>
 
 #include "rb_common.cuh"
 #include "rb_kernels.h"
@@ -350,57 +351,72 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
   if constexpr (FU == 1) {
     // One face per work item: four cells along the normal. x- and y-faces share
     // one loop, so the last pass over the block is partly filled once, not twice.
+    // A tile whose faces (and the ring's) are all inner faces of the domain runs an
+    // instantiation without bounds checks and with the boundary kind fixed at
+    // "open", so the edge-ghost code compiles away; the others run the general one.
     constexpr int NXF = XH * XW, NF = XH * XW + YH * YW;
-    for (int k = threadIdx.x; k < NF; k += NT) {
-      float fh, fl, fr, ft;
-      if (k < NXF) {
-        const int a = k / XW, b = k - a * XW;
-        const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-        if (gi < 0 || gi >= ny || gj < 0 || gj > nx) continue;
-        const int r = a + 2;  // cell row; stencil columns b .. b+3 (cells gj-2 .. gj+1)
-        const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
-        const Cell c0{s_h[r][b], s_u[r][b], s_v[r][b], s_z[r][b]};
-        const Cell c1{s_h[r][b + 1], s_u[r][b + 1], s_v[r][b + 1], s_z[r][b + 1]};
-        const Cell c2{s_h[r][b + 2], s_u[r][b + 2], s_v[r][b + 2], s_z[r][b + 2]};
-        const Cell c3{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
-        // at an edge the clamped stencil is in the staged region; the edge cell is
-        // column 0 (c2) or nx-1 (c1)
-        const Rec L = recon(c0, c1, c2);
-        float h_l, h_r;
-        any_face_flux(L, recon(c1, c2, c3), kind, gj == 0, gj == 0 ? c2 : c1, gj == 0 ? stage_w : stage_e, fh, fl,
-                      fr, ft, h_l, h_r);
-        keep_x(a, b, h_l, h_r, L.sz);
-        s_fxh[a][b] = fh;
-        if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
-          s_fxl[a - 1][b - 1] = fl;
-          s_fxr[a - 1][b - 1] = fr;
-          s_fxt[a - 1][b - 1] = ft;
-        }
-      } else {  // y-faces: normal velocity v, transverse u (hllc.py:357-424)
-        const int ky = k - NXF;
-        const int a = ky / YW, b = ky - a * YW;
-        const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-        if (gj < 0 || gj >= nx || gi < 0 || gi > ny) continue;
-        const int c = b + 2;  // cell column; stencil rows a .. a+3 (cells gi-2 .. gi+1)
-        const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
-        const Cell c0{s_h[a][c], s_v[a][c], s_u[a][c], s_z[a][c]};
-        const Cell c1{s_h[a + 1][c], s_v[a + 1][c], s_u[a + 1][c], s_z[a + 1][c]};
-        const Cell c2{s_h[a + 2][c], s_v[a + 2][c], s_u[a + 2][c], s_z[a + 2][c]};
-        const Cell c3{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
-        // the edge cell: row 0 (c2) or ny-1 (c1)
-        const Rec L = recon(c0, c1, c2);
-        float h_l, h_r;
-        any_face_flux(L, recon(c1, c2, c3), kind, gi == 0, gi == 0 ? c2 : c1, gi == 0 ? stage_n : stage_s, fh, fl,
-                      fr, ft, h_l, h_r);
-        keep_y(a, b, h_l, h_r, L.sz);
-        s_fyh[a][b] = fh;
-        if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
-          s_fyl[a - 1][b - 1] = fl;
-          s_fyr[a - 1][b - 1] = fr;
-          s_fyt[a - 1][b - 1] = ft;
+    auto face_loop = [&](auto inner_tag) {
+      constexpr bool INNER = decltype(inner_tag)::value;
+      for (int k = threadIdx.x; k < NF; k += NT) {
+        float fh, fl, fr, ft;
+        if (k < NXF) {
+          const int a = k / XW, b = k - a * XW;
+          const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+          if (!INNER && (gi < 0 || gi >= ny || gj < 0 || gj > nx)) continue;
+          const int r = a + 2;  // cell row; stencil columns b .. b+3 (cells gj-2 .. gj+1)
+          const int kind =
+              INNER ? RB_BC_OPEN : (gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN));
+          const Cell c0{s_h[r][b], s_u[r][b], s_v[r][b], s_z[r][b]};
+          const Cell c1{s_h[r][b + 1], s_u[r][b + 1], s_v[r][b + 1], s_z[r][b + 1]};
+          const Cell c2{s_h[r][b + 2], s_u[r][b + 2], s_v[r][b + 2], s_z[r][b + 2]};
+          const Cell c3{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
+          // at an edge the clamped stencil is in the staged region; the edge cell is
+          // column 0 (c2) or nx-1 (c1)
+          const Rec L = recon(c0, c1, c2);
+          float h_l, h_r;
+          any_face_flux(L, recon(c1, c2, c3), kind, gj == 0, gj == 0 ? c2 : c1, gj == 0 ? stage_w : stage_e, fh,
+                        fl, fr, ft, h_l, h_r);
+          keep_x(a, b, h_l, h_r, L.sz);
+          s_fxh[a][b] = fh;
+          if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
+            s_fxl[a - 1][b - 1] = fl;
+            s_fxr[a - 1][b - 1] = fr;
+            s_fxt[a - 1][b - 1] = ft;
+          }
+        } else {  // y-faces: normal velocity v, transverse u (hllc.py:357-424)
+          const int ky = k - NXF;
+          const int a = ky / YW, b = ky - a * YW;
+          const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+          if (!INNER && (gj < 0 || gj >= nx || gi < 0 || gi > ny)) continue;
+          const int c = b + 2;  // cell column; stencil rows a .. a+3 (cells gi-2 .. gi+1)
+          const int kind =
+              INNER ? RB_BC_OPEN : (gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN));
+          const Cell c0{s_h[a][c], s_v[a][c], s_u[a][c], s_z[a][c]};
+          const Cell c1{s_h[a + 1][c], s_v[a + 1][c], s_u[a + 1][c], s_z[a + 1][c]};
+          const Cell c2{s_h[a + 2][c], s_v[a + 2][c], s_u[a + 2][c], s_z[a + 2][c]};
+          const Cell c3{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
+          // the edge cell: row 0 (c2) or ny-1 (c1)
+          const Rec L = recon(c0, c1, c2);
+          float h_l, h_r;
+          any_face_flux(L, recon(c1, c2, c3), kind, gi == 0, gi == 0 ? c2 : c1, gi == 0 ? stage_n : stage_s, fh,
+                        fl, fr, ft, h_l, h_r);
+          keep_y(a, b, h_l, h_r, L.sz);
+          s_fyh[a][b] = fh;
+          if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
+            s_fyl[a - 1][b - 1] = fl;
+            s_fyr[a - 1][b - 1] = fr;
+            s_fyt[a - 1][b - 1] = ft;
+          }
         }
       }
-    }
+    };
+    // x-faces span columns x0-1 .. x0+TX+1 and rows y0-1 .. y0+TY, y-faces columns
+    // x0-1 .. x0+TX and rows y0-1 .. y0+TY+1: all inner faces when these hold
+    const bool inner = x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= nx && y0 + TY + 2 <= ny;
+    if (inner)
+      face_loop(std::true_type{});
+    else
+      face_loop(std::false_type{});
   } else {
     // FU consecutive faces per work item along the normal, each cell reconstructed
     // once in a rolling window: the reference's face-local eta_l / eta_r are the
