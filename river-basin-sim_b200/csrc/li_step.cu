@@ -33,6 +33,7 @@
 // slot per tile instead of a per-cell float64 field.
 #include <atomic>
 #include <cfloat>
+#include <type_traits>
 
 #include "rb_common.cuh"
 #include "rb_kernels.h"
@@ -281,83 +282,94 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
   // x- and y-faces share one loop, so the last pass over the block is partly
   // filled once, not twice.
   constexpr int NXF = XH * XW, NF = XH * XW + YH * YW;
-  for (int kk = threadIdx.x; kk < NF; kk += NT) {
-    if (kk < NXF) {
-      const int k = kk;
-      const int a = k / XW, b = k - a * XW;
-      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-      float q = 0.0f;
-      if constexpr (!CH) {
-        if (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1) {
-          const float eta_l = s_eta[a + 1][b], eta_r = s_eta[a + 1][b + 1];
-          const float h_flow = rmax(eta_l, eta_r) - rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
-          if (!(h_flow < kHDry)) {
-            const float qo = s_qx[a][b];  // previous discharge, staged above
-            const float n_face = 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]);
+  // A tile whose faces (and the ring's) are all inner faces of the domain runs an
+  // instantiation without the bounds checks.
+  auto face_loop = [&](auto inner_tag) {
+    constexpr bool INNER = decltype(inner_tag)::value;
+    for (int kk = threadIdx.x; kk < NF; kk += NT) {
+      if (kk < NXF) {
+        const int k = kk;
+        const int a = k / XW, b = k - a * XW;
+        const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+        float q = 0.0f;
+        if constexpr (!CH) {
+          if (INNER || (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1)) {
+            const float eta_l = s_eta[a + 1][b], eta_r = s_eta[a + 1][b + 1];
+            const float h_flow = rmax(eta_l, eta_r) - rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
+            if (!(h_flow < kHDry)) {
+              const float qo = s_qx[a][b];  // previous discharge, staged above
+              const float n_face = 0.5f * (s_n[a + 1][b] + s_n[a + 1][b + 1]);
+              const float slope = div_pos(eta_r - eta_l, dx);
+              const float num = qo - kG * h_flow * dt * slope;
+              q = manning_divide(num, qo, h_flow, n_face, kG, dt);
+            }
+          }
+        } else {  // local_inertial.py:338-384 update_qx_channels
+          float qc = 0.0f, qf = 0.0f;
+          if (INNER || (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1)) {
+            const int r = a + 1, cl = b, cr = b + 1;
+            const float eta_l = s_eta[r][cl], eta_r = s_eta[r][cr];
+            const float eta_max = rmax(eta_l, eta_r);
             const float slope = div_pos(eta_r - eta_l, dx);
-            const float num = qo - kG * h_flow * dt * slope;
-            q = manning_divide(num, qo, h_flow, n_face, kG, dt);
+            const float z_bank = rmax(s_z[r][cl], s_z[r][cr]);
+            qf = floodplain_flux(S.ch.qxf[a][b], eta_max, slope, z_bank, 0.5f * (s_n[r][cl] + s_n[r][cr]), dt);
+            const float w_face = rmin(S.ch.w[r][cl], S.ch.w[r][cr]);
+            const float z_ch = rmax(s_z[r][cl] - S.ch.d[r][cl], s_z[r][cr] - S.ch.d[r][cr]);
+            qc = channel_flux(S.ch.qxc[a][b], eta_max, slope, w_face, z_bank, z_ch,
+                              0.5f * (S.ch.cn[r][cl] + S.ch.cn[r][cr]), dt);
+            const float frac = div_pos(w_face, dx);
+            q = qf * (1.0f - frac) + qc * frac;
           }
+          S.ch.qxc[a][b] = qc;
+          S.ch.qxf[a][b] = qf;
         }
-      } else {  // local_inertial.py:338-384 update_qx_channels
-        float qc = 0.0f, qf = 0.0f;
-        if (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1) {
-          const int r = a + 1, cl = b, cr = b + 1;
-          const float eta_l = s_eta[r][cl], eta_r = s_eta[r][cr];
-          const float eta_max = rmax(eta_l, eta_r);
-          const float slope = div_pos(eta_r - eta_l, dx);
-          const float z_bank = rmax(s_z[r][cl], s_z[r][cr]);
-          qf = floodplain_flux(S.ch.qxf[a][b], eta_max, slope, z_bank, 0.5f * (s_n[r][cl] + s_n[r][cr]), dt);
-          const float w_face = rmin(S.ch.w[r][cl], S.ch.w[r][cr]);
-          const float z_ch = rmax(s_z[r][cl] - S.ch.d[r][cl], s_z[r][cr] - S.ch.d[r][cr]);
-          qc = channel_flux(S.ch.qxc[a][b], eta_max, slope, w_face, z_bank, z_ch,
-                            0.5f * (S.ch.cn[r][cl] + S.ch.cn[r][cr]), dt);
-          const float frac = div_pos(w_face, dx);
-          q = qf * (1.0f - frac) + qc * frac;
-        }
-        S.ch.qxc[a][b] = qc;
-        S.ch.qxf[a][b] = qf;
-      }
-      s_qx[a][b] = q;
-    } else {
-      const int k = kk - NXF;
-      const int a = k / YW, b = k - a * YW;
-      const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-      float q = 0.0f;
-      if constexpr (!CH) {
-        if (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx) {
-          const float eta_t = s_eta[a][b + 1], eta_b = s_eta[a + 1][b + 1];
-          const float h_flow = rmax(eta_t, eta_b) - rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
-          if (!(h_flow < kHDry)) {
-            const float qo = s_qy[a][b];
-            const float n_face = 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]);
+        s_qx[a][b] = q;
+      } else {
+        const int k = kk - NXF;
+        const int a = k / YW, b = k - a * YW;
+        const int gi = y0 - 1 + a, gj = x0 - 1 + b;
+        float q = 0.0f;
+        if constexpr (!CH) {
+          if (INNER || (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx)) {
+            const float eta_t = s_eta[a][b + 1], eta_b = s_eta[a + 1][b + 1];
+            const float h_flow = rmax(eta_t, eta_b) - rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
+            if (!(h_flow < kHDry)) {
+              const float qo = s_qy[a][b];
+              const float n_face = 0.5f * (s_n[a][b + 1] + s_n[a + 1][b + 1]);
+              const float slope = div_pos(eta_b - eta_t, dx);
+              const float num = qo - kG * h_flow * dt * slope;
+              q = manning_divide(num, qo, h_flow, n_face, kG, dt);
+            }
+          }
+        } else {  // local_inertial.py:387-427 update_qy_channels
+          float qc = 0.0f, qf = 0.0f;
+          if (INNER || (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx)) {
+            const int c = b + 1, rt = a, rb = a + 1;
+            const float eta_t = s_eta[rt][c], eta_b = s_eta[rb][c];
+            const float eta_max = rmax(eta_t, eta_b);
             const float slope = div_pos(eta_b - eta_t, dx);
-            const float num = qo - kG * h_flow * dt * slope;
-            q = manning_divide(num, qo, h_flow, n_face, kG, dt);
+            const float z_bank = rmax(s_z[rt][c], s_z[rb][c]);
+            qf = floodplain_flux(S.ch.qyf[a][b], eta_max, slope, z_bank, 0.5f * (s_n[rt][c] + s_n[rb][c]), dt);
+            const float w_face = rmin(S.ch.w[rt][c], S.ch.w[rb][c]);
+            const float z_ch = rmax(s_z[rt][c] - S.ch.d[rt][c], s_z[rb][c] - S.ch.d[rb][c]);
+            qc = channel_flux(S.ch.qyc[a][b], eta_max, slope, w_face, z_bank, z_ch,
+                              0.5f * (S.ch.cn[rt][c] + S.ch.cn[rb][c]), dt);
+            const float frac = div_pos(w_face, dx);
+            q = qf * (1.0f - frac) + qc * frac;
           }
+          S.ch.qyc[a][b] = qc;
+          S.ch.qyf[a][b] = qf;
         }
-      } else {  // local_inertial.py:387-427 update_qy_channels
-        float qc = 0.0f, qf = 0.0f;
-        if (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx) {
-          const int c = b + 1, rt = a, rb = a + 1;
-          const float eta_t = s_eta[rt][c], eta_b = s_eta[rb][c];
-          const float eta_max = rmax(eta_t, eta_b);
-          const float slope = div_pos(eta_b - eta_t, dx);
-          const float z_bank = rmax(s_z[rt][c], s_z[rb][c]);
-          qf = floodplain_flux(S.ch.qyf[a][b], eta_max, slope, z_bank, 0.5f * (s_n[rt][c] + s_n[rb][c]), dt);
-          const float w_face = rmin(S.ch.w[rt][c], S.ch.w[rb][c]);
-          const float z_ch = rmax(s_z[rt][c] - S.ch.d[rt][c], s_z[rb][c] - S.ch.d[rb][c]);
-          qc = channel_flux(S.ch.qyc[a][b], eta_max, slope, w_face, z_bank, z_ch,
-                            0.5f * (S.ch.cn[rt][c] + S.ch.cn[rb][c]), dt);
-          const float frac = div_pos(w_face, dx);
-          q = qf * (1.0f - frac) + qc * frac;
-        }
-        S.ch.qyc[a][b] = qc;
-        S.ch.qyf[a][b] = qf;
+        s_qy[a][b] = q;
       }
-      s_qy[a][b] = q;
     }
-  }
+  };
+  // x-faces span columns x0-1 .. x0+TX+1 and rows y0-1 .. y0+TY, y-faces columns
+  // x0-1 .. x0+TX and rows y0-1 .. y0+TY+1: all inner faces when these hold
+  if (x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= nx && y0 + TY + 2 <= ny)
+    face_loop(std::true_type{});
+  else
+    face_loop(std::false_type{});
   __syncthreads();
 
   // 3. donor-cell beta on the tile plus a 1-cell ring (local_inertial.py:197-239).
