@@ -269,8 +269,8 @@ int rb_ensemble_read(const rb_ensemble_layout *L, void *ens, rb_clock_state *out
  * kernel's variants (tile shape, block size, faces per work item, load batching).
  * Every variant computes bit-identical results; this is a speed knob only, read at
  * each launch (a captured graph keeps the variant it was captured with). The
- * library starts with the variant measured fastest on B200 (4: 32 x 32 tiles,
- * 512 threads). */
+ * library starts with the variant measured fastest on B200 (6: 32 x 32 tiles,
+ * 640 threads). */
 int rb_hllc_set_kernel_variant(int32_t variant);
 int rb_hllc_kernel_variants(int32_t *count);
 /* The same for the local-inertial step (tile 32 x 16, 32 x 32, 64 x 16, 32 x 8, and

@@ -213,8 +213,8 @@ struct HllcSmem {
   // per tile cell, from the face phase: the reconstructed depths at the cell's east
   // (hp) and west (hm) faces and the bed slope sz, along x and along y
   float hpx[TY][TX], hmx[TY][TX], szx[TY][TX], hpy[TY][TX], hmy[TY][TX], szy[TY][TX];
-  double red[16];
-  float redf[16];
+  double red[32];  // one slot per warp of a block of up to 1024 threads
+  float redf[32];
 };
 
 // One Heun stage of tile (bx, by) of domain p; ledger slot `slot`. Called by every
@@ -224,7 +224,7 @@ struct HllcSmem {
 // divisions. Every choice computes the same bits.
 template <int TX, int TY, int NT, int STAGE, int FU = 1, int LP = 1>
 __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, size_t slot, HllcSmem<TX, TY>& S) {
-  static_assert(NT / 32 <= 16, "reduction scratch sized for <= 16 warps");
+  static_assert(NT / 32 <= 32, "reduction scratch sized for <= 32 warps");
   using SM = HllcSmem<TX, TY>;
   constexpr int H = SM::H, RW = SM::RW, RH = SM::RH, XW = SM::XW, XH = SM::XH, YW = SM::YW, YH = SM::YH;
   constexpr int BW = SM::BW, BH = SM::BH;
@@ -689,9 +689,10 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
 
 // The single-domain stage kernel. Shared memory is dynamic (a 32 x 32 tile needs
 // more than the 48 KB a static array may take); __launch_bounds__ asks for two
-// resident 512-thread blocks (or four of 256) per SM, i.e. at most 64 registers.
+// resident blocks of 512 threads or more (four of 256) per SM: at most 64 registers
+// a thread for 512, 51 for 640.
 template <int TX, int TY, int NT, int STAGE, int FU, int LP>
-__global__ void __launch_bounds__(NT, 1024 / NT) hllc_stage_kernel(const HllcParams p) {
+__global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT) hllc_stage_kernel(const HllcParams p) {
   extern __shared__ __align__(16) unsigned char hllc_smem_raw[];
   auto& S = *reinterpret_cast<HllcSmem<TX, TY>*>(hllc_smem_raw);
   hllc_tile<TX, TY, NT, STAGE, FU, LP>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S);
@@ -728,17 +729,20 @@ static cudaError_t launch_hllc(const HllcParams& p, int stage, cudaStream_t s) {
 
 // Kernel variants of the single-domain stage: tile, block size, faces per work item,
 // load batching. All compute the same bits; they differ only in speed. The default
-// is the fastest measured on B200 for the 2048 x 2048 dam break (ms per step, plan
-// included: 0.604, 0.517, 0.522, 0.556, 0.504, 0.511 for variants 0..5).
+// (6: 32 x 32 tiles, 640 threads, two blocks and 40 warps per SM, 44-48 registers)
+// is the fastest measured on B200: 0.316 ms per 2048 x 2048 dam-break step against
+// 0.326 for 512 threads, 0.337 for 576, 0.323 for 608, 0.328 for 768 and 0.348 for
+// 800 (which spills at its 40-register bound). The 2380 face work items of a tile
+// fill 3.7 passes of 640 threads against 4.6 of 512.
 struct HllcKernelVariant {
   int tx, ty, nt, fu, lp;
 };
 static const HllcKernelVariant kHllcVariants[] = {
     {32, 16, 256, 1, 0}, {32, 16, 256, 1, 1}, {32, 16, 256, 3, 1},
-    {32, 16, 256, 2, 1}, {32, 32, 512, 1, 1}, {64, 16, 512, 1, 1},
+    {32, 16, 256, 2, 1}, {32, 32, 512, 1, 1}, {64, 16, 512, 1, 1}, {32, 32, 640, 1, 1},
 };
 constexpr int kNumHllcVariants = (int)(sizeof(kHllcVariants) / sizeof(kHllcVariants[0]));
-constexpr int kDefaultHllcVariant = 4;
+constexpr int kDefaultHllcVariant = 6;
 static std::atomic<int> g_hllc_variant{kDefaultHllcVariant};
 
 int hllc_kernel_variant_count() { return kNumHllcVariants; }
@@ -752,6 +756,7 @@ void hllc_prepare_device() {
   prepare_hllc<32, 16, 256, 2, 1>();
   prepare_hllc<32, 32, 512, 1, 1>();
   prepare_hllc<64, 16, 512, 1, 1>();
+  prepare_hllc<32, 32, 640, 1, 1>();
 }
 bool hllc_set_kernel_variant(int v) {
   if (v < 0 || v >= kNumHllcVariants) return false;
@@ -766,7 +771,8 @@ cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s) {
     case 3: return launch_hllc<32, 16, 256, 2, 1>(p, stage, s);
     case 5: return launch_hllc<64, 16, 512, 1, 1>(p, stage, s);
     case 0: return launch_hllc<32, 16, 256, 1, 0>(p, stage, s);
-    default: return launch_hllc<32, 32, 512, 1, 1>(p, stage, s);
+    case 4: return launch_hllc<32, 32, 512, 1, 1>(p, stage, s);
+    default: return launch_hllc<32, 32, 640, 1, 1>(p, stage, s);
   }
 }
 

@@ -219,7 +219,7 @@ def test_every_hllc_kernel_variant_matches_oracle_bitwise(shape):
             _lib.check(L.rb_hllc_set_kernel_variant(v))
             _compare(run_case(case, GpuAPI()), want, f"hllc{shape} variant {v}")
     finally:
-        _lib.check(L.rb_hllc_set_kernel_variant(4))  # the library's default
+        _lib.check(L.rb_hllc_set_kernel_variant(6))  # the library's default
 
 
 @pytest.mark.parametrize("shape", [(333, 517), (1, 700), (37, 3)])
