@@ -146,6 +146,7 @@ def hllc_lake_2048(args):
     depth = np.maximum(2.0 - bed, 0.0).astype(np.float32)
     st = rbsim.State.from_bed(bed, dx, depth=depth, manning=0.03)
     hllc.arm_hllc(st)
+    v0 = st.volume_sum()
     K = args.steps
     clk = DeviceClock(st, "hllc_fv", alpha=0.45, dt_max=30.0, sync_times=[600.0], graph_steps=K)
     clk.run_until(600.0, max_steps=K)  # capture + warm
@@ -158,14 +159,24 @@ def hllc_lake_2048(args):
     torch.cuda.synchronize()
     clk.read()
     ms = start.elapsed_time(stop) / K
-    u, v = st.velocities_numpy()
+
+    def at_rest():
+        u, v = st.velocities_numpy()
+        h = st.h.cpu().numpy()
+        speed = np.maximum(np.abs(u), np.abs(v))
+        deep = h > 0.1
+        return {"t_s": clk.t, "steps": clk.steps, "max_speed": float(speed.max()),
+                "max_speed_where_deeper_than_0.1m": float(speed[deep].max()) if deep.any() else 0.0,
+                "volume_rel_change": abs(st.volume_sum() - v0) / v0}  # fmt: skip
+
+    after_timed = at_rest()
+    # then on to the configuration's 600 s horizon (untimed), where its gate is read
+    clk.run_until(600.0)
+    horizon = at_rest()
     h = st.h.cpu().numpy()
-    speed = np.maximum(np.abs(u), np.abs(v))
-    deep = h > 0.1
     return {"workload": "hllc_lake_2048", "metric": "Gcell-updates/s", "value": n * n / (ms / 1e3) / 1e9,
             "ms_per_step": ms, "steps": K, "dry_fraction": float((h < 1e-3).mean()),
-            "max_speed_after": float(speed.max()),
-            "max_speed_where_deeper_than_0.1m": float(speed[deep].max()) if deep.any() else 0.0}  # fmt: skip
+            "after_timed_steps": after_timed, "at_600s": horizon}  # fmt: skip
 
 
 def reach_inputs(n=8192, dx=5.0, seed=3):
