@@ -239,7 +239,7 @@ int rb_clock_read(void *ws, void *stream, rb_clock_state *out);
  * (clocks, parameter blocks, tile maps) is caller-allocated, sized by the layout. */
 typedef struct rb_ensemble_layout {
   int32_t ndom, n_li, n_hllc;
-  int32_t li_variant, hllc_variant;  /* tile shapes: LI 0 = 32x16, 1 = 32x8, 2 = 64x8, 3 = 32x32; HLLC 0 = 32x16, 1 = 32x8 */
+  int32_t li_variant, hllc_variant;  /* tile shapes: LI 0 = 32x16, 1 = 32x8, 2 = 64x8, 3 = 32x32; HLLC 0 = 32x16, 1 = 32x8, 2 = 32x32 */
   int32_t li_grid, hllc_grid;        /* persistent grid sizes (set by rb_ensemble_init) */
   int32_t reserved;
   int64_t li_tiles, hllc_tiles;

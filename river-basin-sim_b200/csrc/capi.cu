@@ -538,7 +538,7 @@ static int64_t tiles_of(int ny, int nx, int tx, int ty) {
 int rb_ensemble_layout_make(int32_t ndom, const int32_t* scheme, const int32_t* ny, const int32_t* nx,
                             int32_t li_variant, int32_t hllc_variant, rb_ensemble_layout* out) {
   if (ndom < 1 || !scheme || !ny || !nx || !out) return fail(RB_ERR_ARG, "rb_ensemble_layout_make: bad argument");
-  if (li_variant < 0 || li_variant > 3 || hllc_variant < 0 || hllc_variant > 1)
+  if (li_variant < 0 || li_variant > 3 || hllc_variant < 0 || hllc_variant > 2)
     return fail(RB_ERR_ARG, "rb_ensemble_layout_make: unknown tile variant");
   rb_ensemble_layout L{};
   L.ndom = ndom;

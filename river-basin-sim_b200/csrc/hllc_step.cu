@@ -789,13 +789,11 @@ int hllc_tiles(int ny, int nx) {
 // (at most 80 registers) measured fastest: 0.479 ms per step for 16 domains of
 // 512 x 512 against 0.552 with no register bound and 0.517 with four blocks (which
 // spills).
+// The work item's domain parameters are staged in shared memory: read from there,
+// the dozens of pointers and scalars need not stay in registers through the tile.
 template <int TX, int TY, int NT, int STAGE>
-__global__ void __launch_bounds__(NT, 768 / NT) ens_hllc_kernel(const HllcParams* __restrict__ P,
-                                                                 const int2* __restrict__ map, long long total) {
-  __shared__ HllcSmem<TX, TY> S;
-  // The work item's domain parameters are staged in shared memory: read from there,
-  // the dozens of pointers and scalars need not stay in registers through the tile.
-  __shared__ __align__(16) HllcParams sp;
+__device__ __forceinline__ void ens_hllc_items(const HllcParams* __restrict__ P, const int2* __restrict__ map,
+                                               long long total, HllcSmem<TX, TY>& S, HllcParams& sp) {
   static_assert(sizeof(HllcParams) % 4 == 0, "parameters copied as 32-bit words");
   constexpr int NW = (int)(sizeof(HllcParams) / 4);
   static_assert(NW <= NT, "one word per thread");
@@ -812,6 +810,31 @@ __global__ void __launch_bounds__(NT, 768 / NT) ens_hllc_kernel(const HllcParams
   }
 }
 
+template <int TX, int TY, int NT, int STAGE>
+__global__ void __launch_bounds__(NT, 768 / NT) ens_hllc_kernel(const HllcParams* __restrict__ P,
+                                                                 const int2* __restrict__ map, long long total) {
+  __shared__ HllcSmem<TX, TY> S;
+  __shared__ __align__(16) HllcParams sp;
+  ens_hllc_items<TX, TY, NT, STAGE>(P, map, total, S, sp);
+}
+
+// The 32 x 32 tile of the single-domain default, with its shared memory (more than a
+// static array may take) dynamic: the tile, then the staged parameters. 512 threads
+// and two blocks per SM measured faster than 640 (whose 51-register bound spills
+// here): 9.9 Gcell-updates/s for 4 domains of 2048 x 2048 against 9.2 for the 32 x 16
+// variant.
+constexpr int kEnsWideNT = 512;
+constexpr size_t kEnsWideParamsAt = (sizeof(HllcSmem<32, 32>) + 15) / 16 * 16;
+constexpr size_t kEnsWideSmem = kEnsWideParamsAt + sizeof(HllcParams);
+template <int STAGE>
+__global__ void __launch_bounds__(kEnsWideNT, 2) ens_hllc_wide_kernel(const HllcParams* __restrict__ P,
+                                                                     const int2* __restrict__ map, long long total) {
+  extern __shared__ __align__(16) unsigned char ens_wide_smem[];
+  auto& S = *reinterpret_cast<HllcSmem<32, 32>*>(ens_wide_smem);
+  auto& sp = *reinterpret_cast<HllcParams*>(ens_wide_smem + kEnsWideParamsAt);
+  ens_hllc_items<32, 32, kEnsWideNT, STAGE>(P, map, total, S, sp);
+}
+
 template <int TX, int TY, int NT>
 static int ens_hllc_grid() {
   int dev = 0, sms = 0, per_sm = 0;
@@ -821,18 +844,39 @@ static int ens_hllc_grid() {
   return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
 }
 
-void hllc_variant_tile(int variant, int* tx, int* ty) {
-  *tx = 32;
-  *ty = variant == 1 ? 8 : 16;
+// Sets the wide kernel's shared-memory opt-in on the current device (outside any
+// stream capture: called while an ensemble layout is made) and sizes its grid.
+static int ens_hllc_wide_grid() {
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaFuncSetAttribute(ens_hllc_wide_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsWideSmem);
+  cudaFuncSetAttribute(ens_hllc_wide_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsWideSmem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_hllc_wide_kernel<2>, kEnsWideNT, kEnsWideSmem);
+  return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
 }
 
-int ens_hllc_grid_size(int variant) { return variant == 1 ? ens_hllc_grid<32, 8, 256>() : ens_hllc_grid<32, 16, 256>(); }
+// Ensemble HLLC variants: 0 = 32 x 16 tiles, 1 = 32 x 8 (256 threads), 2 = 32 x 32.
+void hllc_variant_tile(int variant, int* tx, int* ty) {
+  *tx = 32;
+  *ty = variant == 1 ? 8 : (variant == 2 ? 32 : 16);
+}
+
+int ens_hllc_grid_size(int variant) {
+  if (variant == 2) return ens_hllc_wide_grid();
+  return variant == 1 ? ens_hllc_grid<32, 8, 256>() : ens_hllc_grid<32, 16, 256>();
+}
 
 cudaError_t ens_hllc_launch(int variant, int grid, int stage, const HllcParams* P, const int2* map, long long total,
                             cudaStream_t s) {
   if (total <= 0) return cudaSuccess;
   const int g = (int)(total < grid ? total : grid);
-  if (variant == 1) {
+  if (variant == 2) {
+    if (stage == 1)
+      ens_hllc_wide_kernel<1><<<g, kEnsWideNT, kEnsWideSmem, s>>>(P, map, total);
+    else
+      ens_hllc_wide_kernel<2><<<g, kEnsWideNT, kEnsWideSmem, s>>>(P, map, total);
+  } else if (variant == 1) {
     if (stage == 1)
       ens_hllc_kernel<32, 8, 256, 1><<<g, 256, 0, s>>>(P, map, total);
     else

@@ -42,7 +42,7 @@ def _member(scheme, ny, nx, dx, seed):
     return st
 
 
-@pytest.mark.parametrize("variants", [(0, 0), (1, 1), (2, 0), (3, 1)])
+@pytest.mark.parametrize("variants", [(0, 0), (1, 1), (2, 0), (3, 1), (3, 2)])
 def test_members_equal_solo_runs(variants):
     from rbsim.device_clock import DeviceClock
     from rbsim.ensemble import Ensemble
