@@ -785,12 +785,9 @@ int hllc_tiles(int ny, int nx) {
 
 // Ensemble: one Heun stage over the (domain, local tile) work-list of every HLLC
 // domain (stage 2 of any domain starts only after stage 1 of all of them, as the
-// single-domain step requires for its own tiles). Three resident blocks per SM
-// (at most 80 registers) measured fastest: 0.479 ms per step for 16 domains of
-// 512 x 512 against 0.552 with no register bound and 0.517 with four blocks (which
-// spills).
-// The work item's domain parameters are staged in shared memory: read from there,
-// the dozens of pointers and scalars need not stay in registers through the tile.
+// single-domain step requires for its own tiles). The work item's domain parameters
+// are staged in shared memory: read from there, the dozens of pointers and scalars
+// need not stay in registers through the tile.
 template <int TX, int TY, int NT, int STAGE>
 __device__ __forceinline__ void ens_hllc_items(const HllcParams* __restrict__ P, const int2* __restrict__ map,
                                                long long total, HllcSmem<TX, TY>& S, HllcParams& sp) {
@@ -810,6 +807,9 @@ __device__ __forceinline__ void ens_hllc_items(const HllcParams* __restrict__ P,
   }
 }
 
+// 32 x 16 and 32 x 8 tiles, 256 threads. Three resident blocks per SM (at most 80
+// registers) measured fastest: 0.479 ms per step for 16 domains of 512 x 512 against
+// 0.552 with no register bound and 0.517 with four blocks (which spills).
 template <int TX, int TY, int NT, int STAGE>
 __global__ void __launch_bounds__(NT, 768 / NT) ens_hllc_kernel(const HllcParams* __restrict__ P,
                                                                  const int2* __restrict__ map, long long total) {
