@@ -119,6 +119,11 @@ struct Cell {
   float h, un, ut, z;
 };
 
+// A staged cell (h, u, v, z) in the frame of an x-face (normal u) or a y-face
+// (normal v).
+__device__ __forceinline__ Cell cell_x(const float4& q) { return Cell{q.x, q.y, q.z, q.w}; }
+__device__ __forceinline__ Cell cell_y(const float4& q) { return Cell{q.x, q.z, q.y, q.w}; }
+
 // MUSCL-minmod reconstruction of one cell to its two faces along the normal
 // (hllc.py:325-342): the east ("E", +1/2) and west ("W", -1/2) values of the water
 // surface, bed, normal and transverse velocity, first order at a dry-adjacent cell;
@@ -205,7 +210,9 @@ struct HllcSmem {
   static constexpr int XW = TX + 3, XH = TY + 2;  // x-face mass flux: cols x0-1..x0+TX+1, rows y0-1..y0+TY
   static constexpr int YW = TX + 2, YH = TY + 3;  // y-face mass flux: cols x0-1..x0+TX,   rows y0-1..y0+TY+1
   static constexpr int BW = TX + 2, BH = TY + 2;  // beta on the tile + ring
-  float h[RH][RW], u[RH][RW], v[RH][RW], z[RH][RW];
+  // the staged cells (h, u, v, z) as one 16-byte word each: a face reads its four
+  // stencil cells with four vector loads
+  float4 c[RH][RW];
   float fxh[XH][XW], fyh[YH][YW];
   float fxl[TY][TX + 1], fxr[TY][TX + 1], fxt[TY][TX + 1];  // tile x-faces
   float fyl[TY + 1][TX], fyr[TY + 1][TX], fyt[TY + 1][TX];  // tile y-faces
@@ -228,10 +235,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
   using SM = HllcSmem<TX, TY>;
   constexpr int H = SM::H, RW = SM::RW, RH = SM::RH, XW = SM::XW, XH = SM::XH, YW = SM::YW, YH = SM::YH;
   constexpr int BW = SM::BW, BH = SM::BH;
-  auto& s_h = S.h;
-  auto& s_u = S.u;
-  auto& s_v = S.v;
-  auto& s_z = S.z;
+  auto& s_c = S.c;
   auto& s_fxh = S.fxh;
   auto& s_fyh = S.fyh;
   auto& s_fxl = S.fxl;
@@ -283,10 +287,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       const float hh = h_s[id];
       float u, v;
       primitives(hh, hu_s[id], hv_s[id], u, v);
-      s_h[r][c] = hh;
-      s_u[r][c] = u;
-      s_v[r][c] = v;
-      s_z[r][c] = p.z[id];
+      s_c[r][c] = make_float4(hh, u, v, p.z[id]);
     }
   } else {
     // All of a thread's loads are issued before any of its divisions, so the
@@ -314,10 +315,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
         const float hh = lh[i];
         float u, v;
         primitives(hh, lhu[i], lhv[i], u, v);
-        s_h[r][c] = hh;
-        s_u[r][c] = u;
-        s_v[r][c] = v;
-        s_z[r][c] = lz[i];
+        s_c[r][c] = make_float4(hh, u, v, lz[i]);
       }
     }
   }
@@ -366,10 +364,10 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
           const int r = a + 2;  // cell row; stencil columns b .. b+3 (cells gj-2 .. gj+1)
           const int kind =
               INNER ? RB_BC_OPEN : (gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN));
-          const Cell c0{s_h[r][b], s_u[r][b], s_v[r][b], s_z[r][b]};
-          const Cell c1{s_h[r][b + 1], s_u[r][b + 1], s_v[r][b + 1], s_z[r][b + 1]};
-          const Cell c2{s_h[r][b + 2], s_u[r][b + 2], s_v[r][b + 2], s_z[r][b + 2]};
-          const Cell c3{s_h[r][b + 3], s_u[r][b + 3], s_v[r][b + 3], s_z[r][b + 3]};
+          const Cell c0 = cell_x(s_c[r][b]);
+          const Cell c1 = cell_x(s_c[r][b + 1]);
+          const Cell c2 = cell_x(s_c[r][b + 2]);
+          const Cell c3 = cell_x(s_c[r][b + 3]);
           // at an edge the clamped stencil is in the staged region; the edge cell is
           // column 0 (c2) or nx-1 (c1)
           const Rec L = recon(c0, c1, c2);
@@ -391,10 +389,10 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
           const int c = b + 2;  // cell column; stencil rows a .. a+3 (cells gi-2 .. gi+1)
           const int kind =
               INNER ? RB_BC_OPEN : (gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN));
-          const Cell c0{s_h[a][c], s_v[a][c], s_u[a][c], s_z[a][c]};
-          const Cell c1{s_h[a + 1][c], s_v[a + 1][c], s_u[a + 1][c], s_z[a + 1][c]};
-          const Cell c2{s_h[a + 2][c], s_v[a + 2][c], s_u[a + 2][c], s_z[a + 2][c]};
-          const Cell c3{s_h[a + 3][c], s_v[a + 3][c], s_u[a + 3][c], s_z[a + 3][c]};
+          const Cell c0 = cell_y(s_c[a][c]);
+          const Cell c1 = cell_y(s_c[a + 1][c]);
+          const Cell c2 = cell_y(s_c[a + 2][c]);
+          const Cell c3 = cell_y(s_c[a + 3][c]);
           // the edge cell: row 0 (c2) or ny-1 (c1)
           const Rec L = recon(c0, c1, c2);
           float h_l, h_r;
@@ -428,14 +426,14 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       if (gi < 0 || gi >= ny) continue;
       const int r = a + 2;
       const int b0 = g * FU;
-      Cell c0{s_h[r][b0 + 1], s_u[r][b0 + 1], s_v[r][b0 + 1], s_z[r][b0 + 1]};
-      Cell cp{s_h[r][b0 + 2], s_u[r][b0 + 2], s_v[r][b0 + 2], s_z[r][b0 + 2]};
-      Rec left = recon(Cell{s_h[r][b0], s_u[r][b0], s_v[r][b0], s_z[r][b0]}, c0, cp);
+      Cell c0 = cell_x(s_c[r][b0 + 1]);
+      Cell cp = cell_x(s_c[r][b0 + 2]);
+      Rec left = recon(cell_x(s_c[r][b0]), c0, cp);
 #pragma unroll
       for (int f = 0; f < FU; f++) {
         const int b = b0 + f;
         const int bb = b < XW ? b : XW - 1;  // a unit past the row end recomputes the last face, unstored
-        const Cell cn{s_h[r][bb + 3], s_u[r][bb + 3], s_v[r][bb + 3], s_z[r][bb + 3]};
+        const Cell cn = cell_x(s_c[r][bb + 3]);
         const Rec right = recon(c0, cp, cn);
         const int gj = x0 - 1 + b;
         if (b < XW && gj >= 0 && gj <= nx) {
@@ -464,14 +462,14 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       if (gj < 0 || gj >= nx) continue;
       const int c = b + 2;
       const int a0 = g * FU;
-      Cell c0{s_h[a0 + 1][c], s_v[a0 + 1][c], s_u[a0 + 1][c], s_z[a0 + 1][c]};
-      Cell cp{s_h[a0 + 2][c], s_v[a0 + 2][c], s_u[a0 + 2][c], s_z[a0 + 2][c]};
-      Rec left = recon(Cell{s_h[a0][c], s_v[a0][c], s_u[a0][c], s_z[a0][c]}, c0, cp);
+      Cell c0 = cell_y(s_c[a0 + 1][c]);
+      Cell cp = cell_y(s_c[a0 + 2][c]);
+      Rec left = recon(cell_y(s_c[a0][c]), c0, cp);
 #pragma unroll
       for (int f = 0; f < FU; f++) {
         const int a = a0 + f;
         const int aa = a < YH ? a : YH - 1;
-        const Cell cn{s_h[aa + 3][c], s_v[aa + 3][c], s_u[aa + 3][c], s_z[aa + 3][c]};
+        const Cell cn = cell_y(s_c[aa + 3][c]);
         const Rec right = recon(c0, cp, cn);
         const int gi = y0 - 1 + a;
         if (a < YH && gi >= 0 && gi <= ny) {
@@ -515,7 +513,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       if (fb > 0.0f) q_out = q_out + fb;
       const float out_depth = dtdx * q_out;
       const bool out = out_depth > 0.0f;
-      const float ratio = div_if(out, s_h[a + 2][b + 2], out_depth);
+      const float ratio = div_if(out, s_c[a + 2][b + 2].x, out_depth);
       if (out) beta = rclamp(ratio, 0.0f, 1.0f);
     }
     s_beta[a][b] = beta;
@@ -597,7 +595,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       if (gi == ny - 1 && p.bc[RB_EDGE_SOUTH] != RB_BC_CLOSED) loss += wt * (double)qs;
     }
     const float dh = -((qe - qw) + (qs - qn)) * inv_dx;
-    const float hg = s_h[R][Cc];
+    const float hg = s_c[R][Cc].x;
     // the centred bed source (hllc.py:805-813): the cell's reconstructed depths at
     // its two faces and its bed slope, as the face phase computed them (the
     // reference's hp = max((eta + se/2) - (z + sz/2), 0) is the reconstruction's
