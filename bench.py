@@ -54,11 +54,11 @@ DT_MAX = 30.0
 T_END = 30.0  # simulated horizon of the dam-break configuration
 BYTES_PER_CELL_STEP = 32  # read h, hu, hv, z, n (20 B) + write h, hu, hv (12 B)
 # DRAM bytes (read + write) of one step's two stage launches in one ncu capture of this
-# workload (--set full, 2048^2 dam break, stage 1 + stage 2): 89.8 MB + 164.7 MB.
-NCU_DRAM_BYTES_PER_STEP = 254.5e6
+# workload (--set full, 2048^2 dam break, stage 1 + stage 2): 88.4 MB + 164.7 MB.
+NCU_DRAM_BYTES_PER_STEP = 253.0e6
 # The stage kernels are issue-bound: share of issue slots busy in the same capture
-# (stage 1 83.8 %, stage 2 82.7 %).
-NCU_ISSUE_ACTIVE = (0.838, 0.827)
+# (stage 1 84.7 %, stage 2 83.9 %).
+NCU_ISSUE_ACTIVE = (0.847, 0.839)
 WORKLOAD = "hllc_dambreak_2048x2048"
 CPU_BAND_ROWS = 256  # the CPU sample: a full-width band of the same dam break
 
