@@ -99,3 +99,32 @@ def test_argument_errors_are_reported_without_touching_the_device():
     f.bc[:] = [2, 0, 0, 0]
     a.dt = 1.0
     assert L.rb_li_step(ctypes.byref(f), 0, ctypes.byref(a), ctypes.c_void_p(1), None) == _lib.RB_ERR_ARG
+
+
+def test_ensemble_layout_counts_each_variants_tiles():
+    """Host only: the ensemble layout sizes its work lists from the chosen tile shapes
+    (LI 32x16 / 32x8 / 64x8 / 32x32, HLLC 32x16 / 32x8 / 32x32) and refuses others."""
+    from rbsim import _lib
+
+    L = _lib.lib()
+    scheme = (ctypes.c_int32 * 3)(0, 1, 1)
+    ny = (ctypes.c_int32 * 3)(100, 70, 33)
+    nx = (ctypes.c_int32 * 3)(64, 65, 1)
+
+    def tiles(n_y, n_x, tx, ty):
+        return -(-n_x // tx) * -(-n_y // ty)
+
+    li_shapes = {0: (32, 16), 1: (32, 8), 2: (64, 8), 3: (32, 32)}
+    hllc_shapes = {0: (32, 16), 1: (32, 8), 2: (32, 32)}
+    for lv, (ltx, lty) in li_shapes.items():
+        for hv, (htx, hty) in hllc_shapes.items():
+            out = _lib.EnsembleLayout()
+            assert L.rb_ensemble_layout_make(3, scheme, ny, nx, lv, hv, ctypes.byref(out)) == 0
+            assert (out.n_li, out.n_hllc) == (1, 2)
+            assert out.li_tiles == tiles(100, 64, ltx, lty)
+            assert out.hllc_tiles == tiles(70, 65, htx, hty) + tiles(33, 1, htx, hty)
+            assert out.bytes > 0
+    out = _lib.EnsembleLayout()
+    assert L.rb_ensemble_layout_make(3, scheme, ny, nx, 0, 3, ctypes.byref(out)) == _lib.RB_ERR_ARG
+    assert "unknown tile variant" in _lib.last_error()
+    assert L.rb_ensemble_layout_make(3, scheme, ny, nx, 4, 0, ctypes.byref(out)) == _lib.RB_ERR_ARG
