@@ -647,6 +647,9 @@ int rb_ensemble_init(rb_ensemble_layout* L, void* ens, const int32_t* scheme, co
   }
   L->li_grid = rb::ens_li_grid_size(L->li_variant);
   L->hllc_grid = rb::ens_hllc_grid_size(L->hllc_variant);
+  if (L->n_hllc > 0 && L->hllc_grid < 1)
+    return fail(RB_ERR_CUDA, "rb_ensemble_init: the device cannot run HLLC tile variant %d (shared memory)",
+                L->hllc_variant);
   RB_CUDA(cudaMemcpyAsync(clocks, hc.data(), hc.size() * sizeof(rb::DevClock), cudaMemcpyHostToDevice, s), "ens clocks");
   if (!hli.empty())
     RB_CUDA(cudaMemcpyAsync(base + L->off_li, hli.data(), hli.size() * sizeof(rb::LiParams), cudaMemcpyHostToDevice, s),

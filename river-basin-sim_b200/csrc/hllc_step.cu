@@ -843,15 +843,23 @@ static int ens_hllc_grid() {
 }
 
 // Sets the wide kernel's shared-memory opt-in on the current device (outside any
-// stream capture: called while an ensemble layout is made) and sizes its grid.
+// stream capture: called while an ensemble is initialised) and sizes its grid; 0
+// when the device refuses the opt-in or cannot hold one block.
 static int ens_hllc_wide_grid() {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaFuncSetAttribute(ens_hllc_wide_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsWideSmem);
-  cudaFuncSetAttribute(ens_hllc_wide_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsWideSmem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_hllc_wide_kernel<2>, kEnsWideNT, kEnsWideSmem);
-  return (per_sm > 0 ? per_sm : 1) * (sms > 0 ? sms : 1);
+  if (cudaFuncSetAttribute(ens_hllc_wide_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsWideSmem) !=
+          cudaSuccess ||
+      cudaFuncSetAttribute(ens_hllc_wide_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kEnsWideSmem) !=
+          cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, ens_hllc_wide_kernel<2>, kEnsWideNT, kEnsWideSmem) !=
+          cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();  // the refusal is reported by the caller, not left to a later launch
+    return 0;
+  }
+  return per_sm * (sms > 0 ? sms : 1);
 }
 
 // Ensemble HLLC variants: 0 = 32 x 16 tiles, 1 = 32 x 8 (256 threads), 2 = 32 x 32.
