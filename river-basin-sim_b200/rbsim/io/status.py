@@ -1,63 +1,82 @@
-"""Run-status writer (the status.json channel of solver/io/status.py:36-117).
+"""Progress channel of a run: ``status.json`` (the contract of solver/io/status.py:36-117).
 
-``{"state", "progress", "sim_time", "eta_s", "message"}`` rewritten atomically
-(temp file + os.replace); ``state`` walks starting -> running -> writing -> done
-(or error); ``eta_s`` is wall-clock extrapolation and never feeds the solver. A
-lost rename race (a reader holding the file on some platforms) is retried with
-backoff and, if it keeps losing, that one update is dropped.
+A viewer that launched the solver as a subprocess polls one small JSON document::
+
+    {"state": "running", "progress": 0.42, "sim_time": 1512.0, "eta_s": 8.3, "message": "..."}
+
+``state`` is one of starting, running, writing, done, error; ``progress`` is
+``sim_time / end_time`` clipped to [0, 1] (1 once done); ``eta_s`` extrapolates the
+wall time spent so far to the rest of the run, or is null before any simulated time
+has passed. The document observes the run and never feeds it.
+
+Every update lands whole: it is written to a temporary file beside the target and
+renamed over it, so a poller never sees half a document. Where a reader that holds
+the file open blocks the rename (Windows), the rename is retried with growing pauses
+until a short deadline; an update that still cannot land is dropped, because the
+next one supersedes it and a run must not fail over its progress file.
 """
 
 from __future__ import annotations
 
 import json
 import os
+import tempfile
 import time
 from pathlib import Path
 
-VALID_STATES = {"starting", "running", "writing", "done", "error"}
-_RETRIES = 12
-_BACKOFF_S = 0.005
+VALID_STATES = frozenset({"starting", "running", "writing", "done", "error"})
+RENAME_DEADLINE_S = 0.5  # how long one update may keep retrying a blocked rename
+_FIRST_PAUSE_S = 0.002
+
+
+def _clip01(x: float) -> float:
+    return 0.0 if x < 0.0 else (1.0 if x > 1.0 else x)
 
 
 class StatusWriter:
     def __init__(self, path, end_time: float):
         self.path = Path(path)
         self.end_time = float(end_time)
-        self._t0 = time.monotonic()
+        self._started = time.monotonic()  # wall clock, for eta_s only
         self.path.parent.mkdir(parents=True, exist_ok=True)
+        self.dropped = 0  # updates that lost every rename attempt
 
-    def _eta(self, sim_time: float):
-        if sim_time <= 0.0 or self.end_time <= 0.0:
-            return None
-        elapsed = time.monotonic() - self._t0
-        frac = min(sim_time / self.end_time, 1.0)
-        if frac <= 0.0:
-            return None
-        return max(elapsed / frac - elapsed, 0.0)
-
-    def write(self, state: str, *, sim_time: float = 0.0, message: str = "") -> None:
+    def document(self, state: str, sim_time: float = 0.0, message: str = "") -> dict:
         if state not in VALID_STATES:
-            raise ValueError(f"invalid status state {state!r}; expected one of {VALID_STATES}")
-        progress = 0.0
-        if self.end_time > 0.0:
-            progress = min(max(sim_time / self.end_time, 0.0), 1.0)
-        if state == "done":
-            progress = 1.0
-        record = {"state": state, "progress": progress, "sim_time": float(sim_time),
-                  "eta_s": self._eta(sim_time), "message": message}  # fmt: skip
-        tmp = self.path.with_name(self.path.name + ".tmp")
-        tmp.write_text(json.dumps(record), encoding="utf-8")
-        delay = _BACKOFF_S
-        for attempt in range(_RETRIES):
+            raise ValueError(f"invalid status state {state!r}; expected one of {sorted(VALID_STATES)}")
+        frac = _clip01(sim_time / self.end_time) if self.end_time > 0.0 else 0.0
+        eta = None
+        if sim_time > 0.0 and frac > 0.0:
+            spent = time.monotonic() - self._started
+            eta = max(spent * (1.0 - frac) / frac, 0.0)
+        return {"state": state, "progress": 1.0 if state == "done" else frac, "sim_time": float(sim_time),
+                "eta_s": eta, "message": message}  # fmt: skip
+
+    def write(self, state: str, *, sim_time: float = 0.0, message: str = "") -> bool:
+        """Publish one update; returns False if it was dropped (see the module docstring)."""
+        payload = json.dumps(self.document(state, sim_time, message)).encode("utf-8")
+        fd, tmp = tempfile.mkstemp(prefix=self.path.name + ".", suffix=".tmp", dir=self.path.parent)
+        try:
+            with os.fdopen(fd, "wb") as f:
+                f.write(payload)
+            if self._rename(tmp):
+                return True
+        except BaseException:
+            Path(tmp).unlink(missing_ok=True)
+            raise
+        Path(tmp).unlink(missing_ok=True)
+        self.dropped += 1
+        return False
+
+    def _rename(self, tmp: str) -> bool:
+        deadline = time.monotonic() + RENAME_DEADLINE_S
+        pause = _FIRST_PAUSE_S
+        while True:
             try:
                 os.replace(tmp, self.path)
-                return
+                return True
             except PermissionError:
-                if attempt == _RETRIES - 1:
-                    break
-                time.sleep(delay)
-                delay = min(delay * 2.0, 0.1)
-        try:
-            tmp.unlink()
-        except OSError:
-            pass
+                if time.monotonic() + pause > deadline:
+                    return False
+                time.sleep(pause)
+                pause *= 2.0

@@ -157,6 +157,30 @@ def read_array(store, name: str) -> np.ndarray:
     return out
 
 
+def _meta(store, name: str) -> dict:
+    return json.loads((Path(store) / name / "zarr.json").read_text())
+
+
+def has_array(store, name: str) -> bool:
+    return (Path(store) / name / "zarr.json").is_file()
+
+
+def array_shape(store, name: str) -> tuple:
+    return tuple(_meta(store, name)["shape"])
+
+
+def read_frame(store, name: str, index: int) -> np.ndarray:
+    """Frame ``index`` of a (time, y, x) array written one frame per chunk; zeros
+    (the fill value) where the frame was never written."""
+    meta = _meta(store, name)
+    _, ny, nx = meta["shape"]
+    dtype = np.dtype({"float32": "<f4", "float64": "<f8"}[meta["data_type"]])
+    key = Path(store) / name / "c" / str(int(index)) / "0" / "0"
+    if not key.exists():
+        return np.zeros((ny, nx), dtype)
+    return np.frombuffer(key.read_bytes(), dtype).reshape(ny, nx)
+
+
 def read_attrs(store) -> dict:
     return json.loads((Path(store) / "zarr.json").read_text())["attributes"]
 
