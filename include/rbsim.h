@@ -300,16 +300,25 @@ int rb_reservoir_deliver(float *h, int32_t ny, int32_t nx, int32_t r0, int32_t c
  * device memory (an embedding engine, a plugin host that forbids allocation after
  * start-up), a framework whose allocator is frozen while it records a CUDA graph,
  * or a loop that cannot take cudaMalloc's implicit device synchronisation.
- * Limit: 1,048,576 cells (e.g. 1024 x 1024); larger grids return RB_ERR_ARG. The
- * array (~14 MiB) is reserved on every GPU that loads the library until exit.
- * Every call shares it: the loss ledger and error word are cleared at the start
- * of each call, and calls that overlap on the GPU race. The first call on a
- * device looks up the array's address (cudaGetSymbolAddress), so make it before
- * any stream capture. If loss_out (device, one double) is given, it receives the
- * depth this step banked through open / fixed_stage edges and infiltration
- * (metres summed over cells). Calls no allocation routine. */
+ * Limit: 1,048,576 cells (e.g. 1024 x 1024); larger grids return RB_ERR_ARG.
+ * The array (~14 MiB) is held until exit by every GPU that loads the library's
+ * device code; under CUDA's lazy module loading (the default since CUDA 12.2) a
+ * GPU loads it, and so reserves the array, at the first call on that GPU. Make
+ * that first call at start-up: before any stream capture on the device (it looks
+ * up the array's address with cudaGetSymbolAddress) and before the host's own
+ * allocator takes the rest of the memory. Every call shares the array: the loss
+ * ledger is cleared at the start of each call, and calls that overlap on the GPU
+ * race. If loss_out (device, one double) is given, it receives the depth this step
+ * banked through open / fixed_stage edges and infiltration (metres summed over
+ * cells). A step that produces a non-finite state sets RB_DEVERR_NONFINITE in the
+ * array's error word, which stays set until rb_hllc_noalloc_read_error reads it.
+ * Calls no allocation routine. */
 int rb_hllc_step_noalloc(const rb_hllc_fields *f, int32_t cur, const rb_step_args *a, double *loss_out,
                          void *stream);
+/* The error bits rb_hllc_step_noalloc calls on the current device have set since
+ * the last read (RB_DEVERR_*), then cleared. Synchronises `stream`. No counterpart
+ * in the reference (its kernels raise no device-side errors). */
+int rb_hllc_noalloc_read_error(uint32_t *err_out, void *stream);
 
 /* --- diagnostics ------------------------------------------------------------ */
 /* Message of this thread's last failed call (empty if none). Returns its length. */

@@ -37,6 +37,20 @@ int cuda_fail(cudaError_t e, const char* where) {
 
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+rb::WsHeader* header(void* ws) { return static_cast<rb::WsHeader*>(ws); }
+
+bool any_bc(const int32_t* bc, int kind) {
+  return bc[0] == kind || bc[1] == kind || bc[2] == kind || bc[3] == kind;
+}
+
+}  // namespace
+
+namespace rb {
+
+void set_last_error(const char* msg) { snprintf(g_err, sizeof g_err, "%s", msg); }
+
+// Argument checks shared by every entry point that takes a grid, edge kinds or a
+// timestep, so that all of them refuse the same inputs with the same messages.
 int check_grid(int ny, int nx, double dx, const char* who) {
   if (ny < 1 || nx < 1) return fail(RB_ERR_ARG, "%s: grid %d x %d must be at least 1 x 1", who, ny, nx);
   if ((long long)ny * (long long)(nx + 1) > (1LL << 40)) return fail(RB_ERR_ARG, "%s: grid too large", who);
@@ -57,17 +71,6 @@ int check_dt(double dt, const char* who) {
   return RB_OK;
 }
 
-rb::WsHeader* header(void* ws) { return static_cast<rb::WsHeader*>(ws); }
-
-bool any_bc(const int32_t* bc, int kind) {
-  return bc[0] == kind || bc[1] == kind || bc[2] == kind || bc[3] == kind;
-}
-
-}  // namespace
-
-namespace rb {
-
-void set_last_error(const char* msg) { snprintf(g_err, sizeof g_err, "%s", msg); }
 
 size_t ws_ledger_bytes(int ny, int nx) {
   // one slot per tile of the smallest tile any kernel variant uses (32 x 8)
@@ -81,6 +84,10 @@ size_t ws_hllc_bytes(int ny, int nx) {
 }
 
 }  // namespace rb
+
+using rb::check_bc;
+using rb::check_dt;
+using rb::check_grid;
 
 extern "C" {
 

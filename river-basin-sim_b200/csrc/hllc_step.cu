@@ -762,8 +762,14 @@ bool hllc_set_kernel_variant(int v) {
   return true;
 }
 
+int hllc_current_variant() { return g_hllc_variant.load(); }
+
 cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s) {
-  switch (g_hllc_variant.load()) {
+  return hllc_stage_launch_variant(p, stage, g_hllc_variant.load(), s);
+}
+
+cudaError_t hllc_stage_launch_variant(const HllcParams& p, int stage, int variant, cudaStream_t s) {
+  switch (variant) {
     case 1: return launch_hllc<32, 16, 256, 1, 1>(p, stage, s);
     case 2: return launch_hllc<32, 16, 256, 3, 1>(p, stage, s);
     case 3: return launch_hllc<32, 16, 256, 2, 1>(p, stage, s);
@@ -776,8 +782,10 @@ cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s) {
 
 // Tiles of the current variant (one ledger slot each); never more than the 32 x 8
 // tiling the workspace ledger is sized for.
-int hllc_tiles(int ny, int nx) {
-  const HllcKernelVariant& v = kHllcVariants[g_hllc_variant.load()];
+int hllc_tiles(int ny, int nx) { return hllc_tiles_of(g_hllc_variant.load(), ny, nx); }
+
+int hllc_tiles_of(int variant, int ny, int nx) {
+  const HllcKernelVariant& v = kHllcVariants[variant >= 0 && variant < kNumHllcVariants ? variant : kDefaultHllcVariant];
   return ((nx + v.tx - 1) / v.tx) * ((ny + v.ty - 1) / v.ty);
 }
 

@@ -7,19 +7,25 @@
 // new allocations after start-up), a framework whose allocator is frozen while it
 // records a CUDA graph, or a stepping loop that cannot afford the implicit device
 // synchronisation of cudaMalloc/cudaFree. rb_hllc_step_noalloc serves them: its
-// scratch is the file-scope array below, reserved when the library is loaded and
-// held by every GPU that loads it until the process exits.
+// scratch is the file-scope array below, which a GPU reserves when the library's
+// device code is loaded on it (with lazy module loading, at the first call) and
+// holds until the process exits.
 //
 // Limits and sharing:
 //  * at most kMaxCells cells (1,048,576, e.g. 1024 x 1024) per call; larger grids
 //    are rejected with RB_ERR_ARG;
-//  * every call uses the same array and leaves its contents behind; the parts
-//    that must start at zero (the loss ledger, the error word) are cleared at the
-//    start of each call, so calls that overlap on the GPU (different streams, or
-//    threads racing on one device) corrupt each other's scratch;
+//  * every call uses the same array and leaves its contents behind; the loss
+//    ledger, which must start at zero, is cleared at the start of each call, so
+//    calls that overlap on the GPU (different streams, or threads racing on one
+//    device) corrupt each other's scratch;
+//  * the error word in the array is sticky: a step that produces a non-finite
+//    state sets RB_DEVERR_NONFINITE there, and it stays set until
+//    rb_hllc_noalloc_read_error reads and clears it;
 //  * the first call on each device looks up the array's device address with
-//    cudaGetSymbolAddress (with that device current); make that first call
-//    before any stream capture on the device.
+//    cudaGetSymbolAddress (with that device current); under CUDA's lazy module
+//    loading (the default since CUDA 12.2) that lookup is also when the device
+//    reserves the array. Make that first call at start-up, before any stream
+//    capture on the device and before the host's allocator is frozen.
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -68,29 +74,32 @@ int scratch_address(unsigned char** out) {
 
 extern "C" int rb_hllc_step_noalloc(const rb_hllc_fields* f, int32_t cur, const rb_step_args* a, double* loss_out,
                                     void* stream) {
+  static const char* who = "rb_hllc_step_noalloc";
   if (f == nullptr || a == nullptr) return fail(RB_ERR_ARG, "rb_hllc_step_noalloc: null argument");
-  if (f->ny < 1 || f->nx < 1 || !(f->dx > 0.0)) return fail(RB_ERR_ARG, "rb_hllc_step_noalloc: bad grid");
+  int rc = rb::check_grid(f->ny, f->nx, f->dx, who);
+  if (rc) return rc;
   if ((int64_t)f->ny * (int64_t)f->nx > kMaxCells)
     return fail(RB_ERR_ARG,
                 "rb_hllc_step_noalloc: grid exceeds the 1048576-cell static scratch (use rb_hllc_step with a "
                 "workspace)");
-  if ((int64_t)rb::hllc_tiles(f->ny, f->nx) > kMaxTiles)
+  // one read of the kernel variant serves the tile count, the launches and the ledger sum
+  const int variant = rb::hllc_current_variant();
+  const int64_t tiles = (int64_t)rb::hllc_tiles_of(variant, f->ny, f->nx);
+  if (tiles > kMaxTiles)
     return fail(RB_ERR_ARG, "rb_hllc_step_noalloc: grid shape needs more ledger slots than the static scratch has");
   if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_hllc_step_noalloc: cur must be 0 or 1");
-  if (!(a->dt > 0.0)) return fail(RB_ERR_STEP, "rb_hllc_step_noalloc: non-positive timestep");
-  for (int e = 0; e < 4; e++)
-    if (f->bc[e] < RB_BC_CLOSED || f->bc[e] > RB_BC_STAGE) return fail(RB_ERR_ARG, "rb_hllc_step_noalloc: bad edge kind");
+  if ((rc = rb::check_dt(a->dt, who))) return rc;
+  if ((rc = rb::check_bc(f->bc, true, who))) return rc;
   if (!f->h[0] || !f->h[1] || !f->hu[0] || !f->hu[1] || !f->hv[0] || !f->hv[1] || !f->z || !f->n)
     return fail(RB_ERR_ARG, "rb_hllc_step_noalloc: missing state buffer");
 
   unsigned char* base = nullptr;
-  int rc = scratch_address(&base);
-  if (rc) return rc;
+  if ((rc = scratch_address(&base))) return rc;
   cudaStream_t s = (cudaStream_t)stream;
-  const size_t nslots = (size_t)rb::hllc_tiles(f->ny, f->nx);
-  // The ledger and the error word must start at zero; the rest is overwritten.
-  if (cudaMemsetAsync(base, 0, rb::WS_HEADER, s) != cudaSuccess ||
-      cudaMemsetAsync(base + kLedgerOff, 0, nslots * 2 * sizeof(double), s) != cudaSuccess)
+  const size_t nslots = (size_t)tiles;
+  // The ledger must start at zero; U1 and the sum partials are overwritten before
+  // they are read, and the error word accumulates until it is read.
+  if (cudaMemsetAsync(base + kLedgerOff, 0, nslots * 2 * sizeof(double), s) != cudaSuccess)
     return fail(RB_ERR_CUDA, "rb_hllc_step_noalloc: clearing the static scratch failed");
 
   const bool banks = f->infil != nullptr || f->bc[0] == RB_BC_OPEN || f->bc[1] == RB_BC_OPEN ||
@@ -127,11 +136,27 @@ extern "C" int rb_hllc_step_noalloc(const rb_hllc_fields* f, int32_t cur, const 
   p.err = &reinterpret_cast<rb::WsHeader*>(base)->err;
   p.clk = nullptr;
   p.smax_key = nullptr;
-  if (rb::hllc_stage_launch(p, 1, s) != cudaSuccess || rb::hllc_stage_launch(p, 2, s) != cudaSuccess)
+  if (rb::hllc_stage_launch_variant(p, 1, variant, s) != cudaSuccess ||
+      rb::hllc_stage_launch_variant(p, 2, variant, s) != cudaSuccess)
     return fail(RB_ERR_CUDA, "rb_hllc_step_noalloc: kernel launch failed");
   if (loss_out != nullptr &&
       rb::sum_ledger((const double*)(base + kLedgerOff), nslots, (double*)(base + rb::WS_PARTIALS), loss_out, s) !=
           cudaSuccess)
     return fail(RB_ERR_CUDA, "rb_hllc_step_noalloc: ledger sum launch failed");
+  return RB_OK;
+}
+
+extern "C" int rb_hllc_noalloc_read_error(uint32_t* err_out, void* stream) {
+  if (err_out == nullptr) return fail(RB_ERR_ARG, "rb_hllc_noalloc_read_error: null argument");
+  unsigned char* base = nullptr;
+  int rc = scratch_address(&base);
+  if (rc) return rc;
+  cudaStream_t s = (cudaStream_t)stream;
+  unsigned int* word = &reinterpret_cast<rb::WsHeader*>(base)->err;
+  unsigned int host = 0;
+  if (cudaMemcpyAsync(&host, word, sizeof host, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+      cudaMemsetAsync(word, 0, sizeof(unsigned int), s) != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess)
+    return fail(RB_ERR_CUDA, "rb_hllc_noalloc_read_error: reading the static scratch's error word failed");
+  *err_out = host;
   return RB_OK;
 }

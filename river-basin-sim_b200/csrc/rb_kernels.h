@@ -112,7 +112,16 @@ cudaError_t ens_li_launch(int variant, int grid, const LiParams* P, const int2* 
 cudaError_t ens_hllc_launch(int variant, int grid, int stage, const HllcParams* P, const int2* map, long long total,
                             cudaStream_t s);
 void set_last_error(const char* msg);  // the message rb_last_error returns on this thread
+// Argument checks of the C ABI: RB_OK, or an error code with the message set.
+int check_grid(int ny, int nx, double dx, const char* who);
+int check_bc(const int32_t* bc, bool allow_stage, const char* who);
+int check_dt(double dt, const char* who);
 int hllc_tiles(int ny, int nx);
+// The HLLC stage-kernel variant in force now; the launch and tile count of one call
+// can take it once, so a concurrent rb_hllc_set_kernel_variant cannot split them.
+int hllc_current_variant();
+int hllc_tiles_of(int variant, int ny, int nx);
+cudaError_t hllc_stage_launch_variant(const HllcParams& p, int stage, int variant, cudaStream_t s);
 int li_kernel_variant_count();
 bool li_set_kernel_variant(int v);
 int hllc_kernel_variant_count();

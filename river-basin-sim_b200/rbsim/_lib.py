@@ -134,6 +134,7 @@ SIGNATURES = {
                                             ctypes.c_int32, ctypes.c_int32, ctypes.c_double, _P, _P]),
     "rb_hllc_step_noalloc": (ctypes.c_int, [ctypes.POINTER(HllcFields), ctypes.c_int32, ctypes.POINTER(StepArgs),
                                             _P, _P]),
+    "rb_hllc_noalloc_read_error": (ctypes.c_int, [ctypes.POINTER(ctypes.c_uint32), _P]),
     "rb_last_error": (ctypes.c_int, [ctypes.c_char_p, ctypes.c_size_t]),
     "rb_version": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)] * 3),
 }  # fmt: skip

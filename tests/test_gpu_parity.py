@@ -155,29 +155,25 @@ def test_hllc_dambreak_2048_matches_oracle_bitwise():
 
 
 def test_hllc_lake_at_rest_with_islands_matches_oracle_bitwise():
-    """The lake-at-rest configuration's generator on a 256 x 256 crop: dx 1 m, four
-    Gaussian bumps (amplitude U(0.5, 3.5) m, sigma U(10, 80) m, seed 2), h = max(2 - z, 0),
-    n 0.03, 100 steps. Shoreline films on bump summits keep a few mm/s of spurious
-    speed in both implementations (the scheme's own residual on slopes this steep);
-    the deep water stays at the float32 floor."""
+    """The lake-at-rest configuration's generator on a 256 x 256 crop (dx 1 m, four
+    Gaussian bumps of amplitude U(0.5, 3.5) m and sigma U(10, 80) m, seed 2,
+    h = max(2 - z, 0), n 0.03) run to the configuration's 600 s horizon: 5881 steps,
+    bit for bit against the float32 oracle. The deep-water speed at the horizon
+    (~5e-4 m/s) and the shoreline films' (~6.5e-3 m/s) are the scheme's own residual
+    at wet/dry fronts on slopes this steep: the float64 oracle shows the same speeds
+    (test_lake_at_rest_f64.py)."""
     from gpu_api import GpuAPI
+    from test_lake_at_rest_f64 import lake_crop
 
-    n = 256
-    rng = np.random.default_rng(2)
-    yy, xx = np.mgrid[0:n, 0:n].astype(np.float32)
-    z = np.zeros((n, n), np.float32)
-    for _ in range(4):
-        a, s = rng.uniform(0.5, 3.5), rng.uniform(10.0, 80.0)
-        cy, cx = rng.uniform(0, n), rng.uniform(0, n)
-        z += a * np.exp(-((yy - cy) ** 2 + (xx - cx) ** 2) / (2 * s * s))
-    z = z.astype(np.float32)
+    z = lake_crop()
     case = dict(scheme="hllc_fv", bed=z, dx=1.0, depth=np.maximum(2.0 - z, 0.0).astype(np.float32), manning=0.03,
-                steps=100, alpha=0.45, dt_max=30.0)  # fmt: skip
+                steps=5881, alpha=0.45, dt_max=30.0)  # fmt: skip
     got = run_case(case, GpuAPI())
-    _compare(got, _oracle_outputs(case), "hllc_lake256")
+    assert got["dts"].sum() >= 600.0 - 1e-6 > got["dts"][:-1].sum()
+    _compare(got, _oracle_outputs(case), "hllc_lake256_600s")
     deep = got["h"] > 0.1
     speed = np.maximum(np.abs(got["hu"]), np.abs(got["hv"]))[deep] / got["h"][deep]
-    assert speed.max() < 1e-4, speed.max()
+    assert speed.max() < 1e-3, speed.max()
 
 
 @pytest.mark.parametrize("name", ["hllc_bumpy_moving", "li_rain_open_infil", "li_sediment"])

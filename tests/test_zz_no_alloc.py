@@ -7,8 +7,12 @@ scratch in a fixed array inside the library instead of a caller workspace. This
 test drives it through the C ABI with ctypes and checks two consecutive steps
 against rb_hllc_step (the workspace entry point) on the same inputs: the states
 must match bit for bit (the tolerance of every parity test in this suite) and the
-banked loss to 1e-12. It also checks that a grid above the 1,048,576-cell limit is
-refused. The file is named to run last; it passes alone or after the others.
+banked loss to 1e-12 -- on a ragged grid with mixed edges, on a grid of exactly the
+1,048,576-cell limit and on one-row and one-column strips of that length (the
+largest ledger and stage-1 offsets the scratch holds). It also checks that a grid
+above the limit is refused and that a non-finite state is reported through
+rb_hllc_noalloc_read_error. The file is named to run last; it passes alone or after
+the others.
 """
 
 from __future__ import annotations
@@ -53,12 +57,25 @@ def _pair(t):
     return [t.clone(), torch.zeros_like(t)]
 
 
-def test_noalloc_step_matches_the_workspace_step_on_two_calls_in_a_row():
+def _read_noalloc_error():
+    from rbsim import _lib
+
+    err = ctypes.c_uint32(0)
+    _lib.check(_lib.lib().rb_hllc_noalloc_read_error(ctypes.byref(err), torch.cuda.current_stream().cuda_stream))
+    return err.value
+
+
+@pytest.mark.parametrize("ny, nx, bc", [
+    (300, 417, [0, 1, 2, 1]),     # ragged; north closed, south open, east fixed_stage, west open
+    (1024, 1024, [1, 1, 1, 1]),   # exactly the cell limit, every edge open
+    (1, 1 << 20, [1, 0, 2, 1]),   # one row of the limit's length
+    (1 << 20, 1, [2, 1, 0, 0]),   # one column of it
+])  # fmt: skip
+def test_noalloc_step_matches_the_workspace_step_on_two_calls_in_a_row(ny, nx, bc):
     from rbsim import _lib
 
     L = _lib.lib()
-    ny, nx, dx = 300, 417, 2.0
-    bc = [0, 1, 2, 1]  # north closed, south open, east fixed_stage, west open
+    dx = 2.0
     z, h0, hu0, hv0, n, infil = _inputs(ny, nx, seed=21)
     stream = torch.cuda.current_stream().cuda_stream
 
@@ -76,7 +93,7 @@ def test_noalloc_step_matches_the_workspace_step_on_two_calls_in_a_row():
 
     cur, banked_a = 0, []
     for k, dt in enumerate((0.05, 0.043)):
-        args = _lib.StepArgs(dt, 0.0, 1.0, 0, 0, (ctypes.c_double * 4)(0.0, 0.0, 1.1, 0.0))
+        args = _lib.StepArgs(dt, 0.0, 1.0, 0, 0, (ctypes.c_double * 4)(1.1, 1.2, 1.1, 1.3))
         _lib.check(L.rb_hllc_step(ctypes.byref(fa), cur, ctypes.byref(args), ws.data_ptr(), stream))
         out = ctypes.c_double()
         _lib.check(L.rb_ledger_loss(ws.data_ptr(), ny, nx, stream, ctypes.byref(out)))
@@ -91,6 +108,23 @@ def test_noalloc_step_matches_the_workspace_step_on_two_calls_in_a_row():
     per_step_a = [banked_a[0], banked_a[1] - banked_a[0]]
     np.testing.assert_allclose(loss_b.cpu().numpy(), per_step_a, rtol=1e-12)
     assert abs(per_step_a[0]) > 0.0  # the edges really banked something
+    assert _read_noalloc_error() == 0
+
+
+def test_noalloc_step_reports_a_non_finite_state():
+    from rbsim import _lib
+
+    L = _lib.lib()
+    ny, nx, dx = 64, 96, 1.0
+    z, h0, hu0, hv0, n, infil = _inputs(ny, nx, seed=5)
+    h0[10, 20] = float("nan")
+    g, gu, gv = _pair(h0), _pair(hu0), _pair(hv0)
+    f = _fields(ny, nx, dx, g, gu, gv, z, n, infil, [0, 0, 0, 0])
+    args = _lib.StepArgs(0.01, 0.0, 1.0, 0, 0)
+    stream = torch.cuda.current_stream().cuda_stream
+    _lib.check(L.rb_hllc_step_noalloc(ctypes.byref(f), 0, ctypes.byref(args), None, stream))
+    assert _read_noalloc_error() & _lib.RB_DEVERR_NONFINITE
+    assert _read_noalloc_error() == 0  # read and cleared
 
 
 def test_noalloc_step_refuses_grids_above_its_limit():
