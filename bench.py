@@ -60,7 +60,7 @@ NCU_DRAM_BYTES_PER_STEP = 253.0e6
 # (stage 1 84.7 %, stage 2 83.9 %).
 NCU_ISSUE_ACTIVE = (0.847, 0.839)
 WORKLOAD = "hllc_dambreak_2048x2048"
-CPU_BAND_ROWS = 256  # the CPU sample: a full-width band of the same dam break
+BUILD = "exact: one IEEE rounding per operation, bit-identical to the oracle"
 
 
 def dambreak_inputs(n: int = N):
@@ -135,62 +135,113 @@ class ClockSampler:
         }
 
 
-def cpu_baseline(steps_cap: int = 1000, budget_s: float = 10.0) -> dict:
-    """The CPU oracle on a full-width band of the dam break, OpenMP over all cores."""
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+# --------------------------------------------------------------------------- #
+# CPU-baseline leg and the oracle helpers the float64-error leg shares. The    #
+# oracle (oracle/: the reference's kernels restated in C) is the checker and   #
+# the CPU baseline: it is timed beside the device path and compared with it,   #
+# never part of what is measured on the device.                                #
+# --------------------------------------------------------------------------- #
+def oracle_module():
+    here = os.path.join(ROOT, "oracle")
+    if here not in sys.path:
+        sys.path.insert(0, here)
     import oracle
 
-    oracle.set_pow_mode(1)
-    z, depth = dambreak_inputs()
-    band = slice(N // 2 - CPU_BAND_ROWS // 2, N // 2 + CPU_BAND_ROWS // 2)
-    st = oracle.State.from_bed(z[band], DX, depth=depth[band], manning=0.0)
-    dt = oracle.hllc_compute_dt(st, ALPHA, DT_MAX)
-    oracle.hllc_step(st, dt)  # first touch of the scratch pages, untimed
-    steps, t0 = 0, time.perf_counter()
+    return oracle
+
+
+def oracle_state(spec, dtype):
+    o = oracle_module()
+    st = o.State.from_bed(spec["bed"], spec["dx"], depth=spec["depth"], manning=spec["manning"], dtype=dtype)
+    if spec["scheme"] == "hllc_fv":
+        st.arm_hllc()
+    if spec.get("infil") is not None:
+        st.set_infiltration(spec["infil"])
+    if spec.get("compensated"):
+        st.arm_source_compensation()
+    if spec.get("boundaries"):
+        st.set_open_boundaries(spec["boundaries"])
+    if spec.get("sediment"):
+        st.arm_sediment(spec["sediment"]["d50"], spec["sediment"]["porosity"])
+    inj = None
+    if spec.get("inflows"):
+        inj = o.InflowInjector([o.Inflow(tuple(c), list(h)) for c, h in spec["inflows"]], st.ny, st.nx, st.dx)
+    return st, inj
+
+
+def cpu_leg(spec, *, budget_s=10.0, steps_cap=1000, warmup=1, pow_mode=0) -> dict:
+    """The CPU oracle stepping ``spec`` (compute_dt + sources + step) for at most
+    ``budget_s`` seconds after ``warmup`` untimed steps; OpenMP over the host's cores."""
+    o = oracle_module()
+    o.set_pow_mode(pow_mode)
+    st, inj = oracle_state(spec, np.float32)
+    cdt, step = o.SCHEMES[spec["scheme"]]
+    t, steps = 0.0, 0
+
+    def one():
+        nonlocal t
+        dt = cdt(st, spec["alpha"], spec["dt_max"])
+        if inj is not None:
+            inj.apply(st, t, dt)
+        step(st, dt, rain=spec.get("rain", 0.0))
+        t += dt
+
+    for _ in range(warmup):
+        one()
+    t0 = time.perf_counter()
     while steps < steps_cap and time.perf_counter() - t0 < budget_s:
-        dt = oracle.hllc_compute_dt(st, ALPHA, DT_MAX)
-        oracle.hllc_step(st, dt)
+        one()
         steps += 1
     el = time.perf_counter() - t0
-    cells = CPU_BAND_ROWS * N
-    cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
-    return {
-        "value": cells * steps / el / 1e9, "unit": "Gcell-updates/s", "cores": cores, "kind": "port",
-        "sample": f"{steps} HLLC steps (compute_dt + step) of a {CPU_BAND_ROWS}x{N} full-width band of the "
-                  f"2048x2048 dam break, C oracle (oracle/rbo.c) with OpenMP, {el:.1f} s",
-    }  # fmt: skip
+    o.set_pow_mode(0)
+    return {"value": st.ny * st.nx * steps / el / 1e9, "unit": "Gcell-updates/s",
+            "cores": int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1)), "kind": "port",
+            "steps": steps, "seconds": el}  # fmt: skip
+
+
+def dambreak_spec() -> dict:
+    z, depth = dambreak_inputs()
+    return dict(scheme="hllc_fv", bed=z, dx=DX, depth=depth, manning=0.0, alpha=ALPHA, dt_max=DT_MAX)
+
+
+def cpu_baseline(budget_s: float = 10.0) -> dict:
+    """The CPU oracle (the reference's kernels restated in C, OpenMP over all host
+    cores, libm powf as the reference's CPU build) on the full headline grid."""
+    out = cpu_leg(dambreak_spec(), budget_s=budget_s, warmup=2)
+    out["sample"] = (f"{out['steps']} HLLC steps (compute_dt + step) of the full {N}x{N} dam break after 2 untimed "
+                     f"steps, C oracle (oracle/rbo.c) with OpenMP, {out['seconds']:.1f} s")
+    return out
 
 
 def run_reference(args) -> None:
+    """The reference path's CPU implementation (the oracle port: its Warp CPU device
+    cannot be installed here) on the headline configuration itself: W untimed warm-up
+    steps, then K timed steps of the full 2048 x 2048 grid on all host cores."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle
-
-    oracle.set_pow_mode(0)
-    z, depth = dambreak_inputs()
-    band = slice(N // 2 - CPU_BAND_ROWS // 2, N // 2 + CPU_BAND_ROWS // 2)
-    st = oracle.State.from_bed(z[band], DX, depth=depth[band], manning=0.0)
-    for _ in range(max(args.warmup, 1)):
-        oracle.hllc_step(st, oracle.hllc_compute_dt(st, ALPHA, DT_MAX))
+    o = oracle_module()
+    o.set_pow_mode(0)
+    st, _ = oracle_state(dambreak_spec(), np.float32)
+    for _ in range(args.warmup):
+        o.hllc_step(st, o.hllc_compute_dt(st, ALPHA, DT_MAX))
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        oracle.hllc_step(st, oracle.hllc_compute_dt(st, ALPHA, DT_MAX))
+        o.hllc_step(st, o.hllc_compute_dt(st, ALPHA, DT_MAX))
     el = time.perf_counter() - t0
-    cells = CPU_BAND_ROWS * N
+    cells = N * N
     value = cells * args.steps / el / 1e9
     cores = int(os.environ.get("OMP_NUM_THREADS", os.cpu_count() or 1))
     line = {
         "impl": "reference", "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": el / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_rows": CPU_BAND_ROWS, "grid": [N, N], "dx_m": DX,
-                   "alpha": ALPHA},
+        "config": {"workload": WORKLOAD, "grid": [N, N], "dx_m": DX, "alpha": ALPHA, "scheme": "hllc_fv",
+                   "boundaries": "closed"},
         "cpu_baseline": {"value": value, "unit": "Gcell-updates/s", "cores": cores, "kind": "port",
-                         "sample": f"each step one HLLC step of a {CPU_BAND_ROWS}x{N} band of the dam break "
-                                   "(the reference's Warp CPU device is not installable; C restatement of its "
-                                   "kernels, OpenMP)"},
+                         "sample": f"each step one HLLC step (compute_dt + step) of the full {N}x{N} dam break, "
+                                   f"after {args.warmup} untimed steps (the reference's Warp CPU device is not "
+                                   "installable; C restatement of its kernels, OpenMP, libm powf)"},
         "e2e": {"value": value, "unit": "Gcell-updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }  # fmt: skip
     print(json.dumps(line))
@@ -276,8 +327,8 @@ def main(argv=None) -> int:
     if cs.steps != args.warmup + K:
         raise RuntimeError(f"device clock took {cs.steps} steps, expected {args.warmup + K}")
     del graph
-    # Per-launch kernel durations for the roofline: the same clocked steps launched one
-    # by one on the stream, with CUDA events around each stage kernel.
+    # Per-launch kernel durations, a cross-check of the roofline's timing: the same
+    # clocked steps launched one by one on the stream, CUDA events around each stage.
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(min(K, 50))]
     clk.set_target(T_END, len(ev))
     for e in ev:
@@ -289,14 +340,84 @@ def main(argv=None) -> int:
         e[2].record(stream)
     torch.cuda.synchronize(dev)
     clk.read()
+    clk.close()
     stage1_ms = [e[0].elapsed_time(e[1]) for e in ev]
     stage2_ms = [e[1].elapsed_time(e[2]) for e in ev]
     st.check_device_errors()
+    del st, clk
     # Whole job: the cells every replica stepped over the slowest replica's time.
     value, sec = replicas.whole_job_rate(cells * K / 1e9, ms / 1e3)
     ms = sec * 1e3
 
-    # --- e2e: host arrays in, the public device-clock API, depth out -- all timed ---
+    e2e = _e2e(args, dev, barrier, z, depth)
+
+    # --- the other configurations' records: the LI roofline point and the largest
+    # single-GPU configuration, each with its own roofline, CPU baseline and error ---
+    import bench_workloads
+
+    legs = world == 1
+    sub = {"li_rain_2048": bench_workloads.li_rain_2048(args, legs=legs),
+           "li_reach_8192": bench_workloads.li_reach_8192(args, legs=legs)}  # fmt: skip
+    err64 = bench_workloads.f64_leg(dambreak_spec(), steps=12) if legs else None
+
+    if rank == 0:
+        pk = peaks()
+        # roofline from the timed region itself: the step's algorithmic bytes over the
+        # replayed step's event time (which also holds the one-thread plan kernel, so
+        # this is a lower bound for the two stage kernels)
+        achieved = BYTES_PER_CELL_STEP * cells / (ms / K / 1e3) / 1e9
+        mean_kernel_ms = statistics.mean(a + b for a, b in zip(stage1_ms, stage2_ms, strict=True))
+        line = {
+            "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "grid": [N, N], "dx_m": DX, "alpha": ALPHA, "scheme": "hllc_fv",
+                       "boundaries": "closed", "parallelism": f"replicas{world}", "build": BUILD,
+                       "l2": "inputs larger than L2: 11 float32 fields of 16.8 MB (h, hu, hv double-buffered, "
+                             "stage-1 state, z, n) = 185 MB touched per step vs 126 MB L2",
+                       "step_loop": "device-resident clock (dt, fill_span, rain gating on the GPU), K steps "
+                                     "replayed as one CUDA graph"},
+            "gpu_launches": 3 * K,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                         "frac": achieved / pk["hbm_gbs"], "traffic": NCU_DRAM_BYTES_PER_STEP,
+                         "traffic_note": "DRAM bytes read + written by stage 1 + stage 2 of one step, from one "
+                                         "ncu capture of this workload; the algorithmic bytes per step are 134 MB",
+                         "peak_source": pk["source"],
+                         "timing": "CUDA events around the timed replay of K steps (stage 1 + stage 2 + the "
+                                   "one-thread plan kernel per step): a lower bound for the stage pair",
+                         "issue_bound": {"issue_slots_busy_stage1": NCU_ISSUE_ACTIVE[0],
+                                         "issue_slots_busy_stage2": NCU_ISSUE_ACTIVE[1],
+                                         "source": "the same ncu capture"},
+                         "kernel": "hllc_stage_kernel stage 1 + stage 2 (one SSP-RK2 step)",
+                         "bytes_per_cell_step": BYTES_PER_CELL_STEP,
+                         "launched_one_by_one": {"stage_pair_ms_mean": mean_kernel_ms,
+                                                 "stage1_ms_mean": statistics.mean(stage1_ms),
+                                                 "stage2_ms_mean": statistics.mean(stage2_ms),
+                                                 "note": f"{len(stage1_ms)} clocked steps launched one by one with "
+                                                         "events around each stage (launch gaps included)"}},
+            "clocks": clocks.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu_baseline() if legs else None,
+            "err_vs_f64": err64,
+            "workloads": sub,
+        }  # fmt: skip
+        print(json.dumps(line))
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def _e2e(args, dev, barrier, z, depth) -> dict:
+    """The headline metric end to end through the public API, from and to pinned host memory."""
+    import torch
+
+    import rbsim
+    from rbsim import replicas
+    from rbsim.device_clock import DeviceClock
+    from rbsim.schemes import hllc
+
+    K = args.steps
+    cells = N * N
     # The job's inputs and result live in pinned host memory (staged before timing);
     # each timed run copies the bed and the initial depth in and the final depth out.
     z_host = torch.from_numpy(z).pin_memory()
@@ -320,7 +441,7 @@ def main(argv=None) -> int:
         h_host.copy_(st3.h)
         return h_host.numpy()
 
-    e2e_device_clock()  # warms the allocator and the kernels outside the timing; each timed call builds its own clock and graph
+    e2e_device_clock()  # warms the allocator and the kernels outside the timing
     timings = {}
     for name, fn in (("device_clock", e2e_device_clock), ("per_step_api", e2e_per_step_api)):
         barrier()
@@ -329,49 +450,12 @@ def main(argv=None) -> int:
         barrier()
         timings[name], _ = replicas.whole_job_rate(cells * K / 1e9, time.perf_counter() - t0)
         assert np.isfinite(h_out).all()
-    e2e_value = timings["device_clock"]
-    e2e_step_api = timings["per_step_api"]
-
-    if rank == 0:
-        pk = peaks()
-        mean_kernel_ms = statistics.mean(a + b for a, b in zip(stage1_ms, stage2_ms, strict=True))
-        achieved = BYTES_PER_CELL_STEP * cells / (mean_kernel_ms / 1e3) / 1e9
-        line = {
-            "metric": "Gcell-updates/s", "value": value, "unit": "Gcell-updates/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "grid": [N, N], "dx_m": DX, "alpha": ALPHA, "scheme": "hllc_fv",
-                       "boundaries": "closed", "parallelism": f"replicas{world}",
-                       "l2": "inputs larger than L2: 11 float32 fields of 16.8 MB (h, hu, hv double-buffered, "
-                             "stage-1 state, z, n) = 185 MB touched per step vs 126 MB L2",
-                       "step_loop": "device-resident clock (dt, fill_span, rain gating on the GPU), K steps "
-                                     "replayed as one CUDA graph"},
-            "gpu_launches": 3 * K,
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
-                         "frac": achieved / pk["hbm_gbs"], "traffic": NCU_DRAM_BYTES_PER_STEP,
-                         "traffic_note": "DRAM bytes read + written by stage 1 + stage 2 of one step, from one "
-                                         "ncu capture of this workload; the algorithmic bytes per step are 134 MB",
-                         "peak_source": pk["source"],
-                         "issue_bound": {"issue_slots_busy_stage1": NCU_ISSUE_ACTIVE[0],
-                                         "issue_slots_busy_stage2": NCU_ISSUE_ACTIVE[1],
-                                         "source": "the same ncu capture"},
-                         "kernel": "hllc_stage_kernel stage 1 + stage 2 (one SSP-RK2 step)",
-                         "kernel_ms_mean": mean_kernel_ms,
-                         "kernel_timing": f"CUDA events around each stage launch, {len(stage1_ms)} clocked steps "
-                                          "launched one by one after the timed replay", "stage1_ms_mean": statistics.mean(stage1_ms),
-                         "stage2_ms_mean": statistics.mean(stage2_ms), "bytes_per_cell_step": BYTES_PER_CELL_STEP},
-            "clocks": clocks.summary(),
-            "e2e": {"value": e2e_value, "unit": "Gcell-updates/s", "api": "State.from_bed + DeviceClock.run_until "
-                    "+ a read of the final depth, from and to pinned host memory", "h2d_bytes_per_step": 2 * 4 * cells / K,
-                    "d2h_bytes_per_step": 4 * cells / K,
-                    "per_step_api": {"value": e2e_step_api, "api": "compute_dt + step per step (dt read back "
-                                     "every step, as the reference's scheme API does)"}},
-            "cpu_baseline": cpu_baseline() if world == 1 else None,
-        }  # fmt: skip
-        print(json.dumps(line))
-    if world > 1:
-        dist.destroy_process_group()
-    return 0
+    return {"value": timings["device_clock"], "unit": "Gcell-updates/s",
+            "api": "State.from_bed + DeviceClock.run_until + a read of the final depth, from and to pinned host "
+                   "memory", "h2d_bytes_per_step": 2 * 4 * cells / K, "d2h_bytes_per_step": 4 * cells / K,
+            "per_step_api": {"value": timings["per_step_api"],
+                             "api": "compute_dt + step per step (dt read back every step, as the reference's "
+                                    "scheme API does)"}}  # fmt: skip
 
 
 if __name__ == "__main__":

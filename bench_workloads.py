@@ -50,6 +50,86 @@ def _peak():
     return bench.peaks()
 
 
+# The float64-error leg (the CPU-baseline leg and the oracle helpers are in bench.py).
+def _oracle():
+    import bench
+
+    return bench.oracle_module()
+
+
+def _oracle_state(spec, dtype):
+    import bench
+
+    return bench.oracle_state(spec, dtype)
+
+
+def cpu_leg(spec, **kw) -> dict:
+    import bench
+
+    return bench.cpu_leg(spec, **kw)
+
+
+def _gpu_state(spec):
+    from rbsim.schemes import hllc
+
+    st = rbsim.State.from_bed(spec["bed"], spec["dx"], depth=spec["depth"], manning=spec["manning"])
+    if spec["scheme"] == "hllc_fv":
+        hllc.arm_hllc(st)
+    if spec.get("infil") is not None:
+        st.set_infiltration(spec["infil"])
+    if spec.get("compensated"):
+        st.arm_source_compensation()
+    if spec.get("boundaries"):
+        st.set_open_boundaries(spec["boundaries"])
+    if spec.get("sediment"):
+        arm_sediment(st, spec["sediment"]["d50"], spec["sediment"]["porosity"])
+    inj = None
+    if spec.get("inflows"):
+        inj = InflowInjector([Inflow(tuple(c), list(h)) for c, h in spec["inflows"]], st.grid, st.device)
+    return st, inj
+
+
+def f64_leg(spec, steps: int) -> dict:
+    """Error of the device's float32 result against the float64 oracle after ``steps``
+    steps of ``spec``: the device steps through the public scheme API and records its
+    timesteps; the float64 oracle replays them, so the runs differ only in precision."""
+    o = _oracle()
+    scheme = rbsim.get_scheme(spec["scheme"])
+    st, inj = _gpu_state(spec)
+    t, dts = 0.0, []
+    for _ in range(steps):
+        dt = scheme.compute_dt(st, alpha=spec["alpha"], dt_max=spec["dt_max"])
+        if inj is not None:
+            inj.apply(st, t, dt)
+        scheme.step(st, dt=dt, rain=spec.get("rain", 0.0), t=t)
+        dts.append(dt)
+        t += dt
+    qn = ("hu", "hv") if spec["scheme"] == "hllc_fv" else ("qx", "qy")
+    got = {"h": st.h.cpu().numpy(), qn[0]: getattr(st, qn[0]).cpu().numpy(), qn[1]: getattr(st, qn[1]).cpu().numpy()}
+    del st
+    o.set_pow_mode(1)
+    ref, rinj = _oracle_state(spec, np.float64)
+    step = o.SCHEMES[spec["scheme"]][1]
+    t = 0.0
+    for dt in dts:
+        if rinj is not None:
+            rinj.apply(ref, t, dt)
+        step(ref, dt, rain=spec.get("rain", 0.0))
+        t += dt
+    o.set_pow_mode(0)
+    h64 = ref.h
+    h_max = float(np.abs(h64).max())
+    q_scale = max([float(np.abs(getattr(ref, k)).max()) for k in qn] + [h_max * math.sqrt(9.81 * h_max)])
+    dq = max(float(np.abs(got[k].astype(np.float64) - getattr(ref, k)).max()) for k in qn)
+    dh = float(np.abs(got["h"].astype(np.float64) - h64).max())
+    v64 = float(h64.sum())
+    return {"steps": steps, "max_abs_depth_m": dh, "max_rel_depth": dh / h_max if h_max > 0 else 0.0,
+            "max_abs_discharge_m2_s": dq, "max_rel_discharge": dq / q_scale if q_scale > 0 else 0.0,
+            "rel_volume": abs(float(got["h"].astype(np.float64).sum()) - v64) / v64 if v64 > 0 else 0.0,
+            "reference": "float64 build of the same kernels (oracle/librbo_f64.so), replaying the device's "
+                         "timesteps; discharge relative to max(|q|_max, h_max sqrt(g h_max))"}  # fmt: skip
+
+
 def _bumps(ny, nx, dx, rng, n, amp, sigma, slope=1e-3):
     yy, xx = np.mgrid[0:ny, 0:nx].astype(np.float32)
     z = slope * xx * dx
@@ -60,13 +140,13 @@ def _bumps(ny, nx, dx, rng, n, amp, sigma, slope=1e-3):
     return z.astype(np.float32)
 
 
-def _kernel_roofline(state, scheme, steps, bytes_per_cell, injector=None):
+def _kernel_roofline(state, scheme, steps, bytes_per_cell, injector=None, rain_rate=0.0):
     """Per-launch CUDA-event time of the step kernel(s) over a timed span of device-clock steps."""
     import ctypes
 
     L = _lib.lib()
     clk = DeviceClock(state, scheme, alpha=0.7, dt_max=30.0, sync_times=[1e9], graph_steps=steps,
-                      injector=injector)  # fmt: skip
+                      injector=injector, rain_rate=rain_rate, rain_until=1e9)  # fmt: skip
     f = state.li_fields()
     ws = state.workspace.data_ptr()
     stream = torch.cuda.current_stream()
@@ -124,17 +204,39 @@ def li_rain_512(args):
             "mass_max_rel_error": ledger.max_rel_error, "roofline": roof}  # fmt: skip
 
 
-def li_rain_2048(args):
-    """The rain-on-grid step at 2048^2 (inputs larger than L2): the LI kernel's roofline."""
+RAIN_50_MM_H = 50.0 / 1000.0 / 3600.0
+
+
+def li_rain_2048_spec() -> dict:
+    """Rain-on-grid at 2048^2, dx 10 m: a sloping bed with 40 Gaussian bumps, 0.5-0.6 m of
+    water, n 0.03, compensated uniform rain 50 mm/h, every edge open."""
     n, dx = 2048, 10.0
     rng = np.random.default_rng(1)
     bed = _bumps(n, n, dx, rng, 40, (0.5, 5.0), (50.0, 1200.0))
-    st = rbsim.State.from_bed(bed, dx, depth=(0.5 + 0.1 * rng.random((n, n))).astype(np.float32), manning=0.03)
-    st.arm_source_compensation()
-    st.set_open_boundaries({e: "open" for e in ("north", "south", "east", "west")})
-    roof = _kernel_roofline(st, "local_inertial", args.steps, 40)
-    return {"workload": "li_rain_2048", "metric": "Gcell-updates/s", "value": roof["gcell_per_s_step"],
-            "steps": args.steps, "roofline": roof}  # fmt: skip
+    return dict(scheme="local_inertial", bed=bed, dx=dx, depth=(0.5 + 0.1 * rng.random((n, n))).astype(np.float32),
+                manning=0.03, compensated=True, rain=RAIN_50_MM_H,
+                boundaries={e: "open" for e in ("north", "south", "east", "west")}, alpha=0.7, dt_max=30.0)  # fmt: skip
+
+
+def li_rain_2048(args, legs: bool = True):
+    """The rain-on-grid step at 2048^2 (inputs larger than L2): the LI kernel's roofline
+    point, 40 algorithmic bytes per cell-step (read h, z, n, qx, qy, h_comp; write h, qx,
+    qy, h_comp); with ``legs``, the CPU oracle on the same grid and the float64 error."""
+    spec = li_rain_2048_spec()
+    st, _ = _gpu_state(spec)
+    _kernel_roofline(st, "local_inertial", max(args.warmup, 1), 40, rain_rate=RAIN_50_MM_H)  # warm-up steps
+    roof = _kernel_roofline(st, "local_inertial", args.steps, 40, rain_rate=RAIN_50_MM_H)
+    del st
+    out = {"workload": "li_rain_2048", "metric": "Gcell-updates/s", "value": roof["gcell_per_s_step"],
+           "steps": args.steps, "warmup": args.warmup, "roofline": roof,
+           "config": {"grid": [2048, 2048], "dx_m": 10.0, "rain_mm_h": 50.0, "edges": "open", "manning": 0.03,
+                      "l2": "9 float32 fields of 16.8 MB touched per step (151 MB) vs 126 MB L2"}}  # fmt: skip
+    if legs:
+        cpu = cpu_leg(spec, budget_s=8.0)
+        cpu["sample"] = f"{cpu['steps']} steps of the full 2048 x 2048 grid, C oracle with OpenMP"
+        out["cpu_baseline"] = cpu
+        out["err_vs_f64"] = f64_leg(spec, steps=20)
+    return out
 
 
 def hllc_lake_2048(args):
@@ -196,7 +298,23 @@ def reach_inputs(n=8192, dx=5.0, seed=3):
     return z, manning, infil, inflows, depth
 
 
-def li_reach_8192(args):
+def reach_band_spec(z, manning, infil, inflows, depth, rows: int) -> dict:
+    """Rows n/2 - rows/2 .. n/2 + rows/2 - 1 of the reach: the meandering channel and all
+    eight inflow cells lie inside; bedload armed (no Exner activation in so few steps)."""
+    n = z.shape[1]
+    r0 = z.shape[0] // 2 - rows // 2
+    band = slice(r0, r0 + rows)
+    return dict(scheme="local_inertial", bed=z[band].copy(), dx=5.0, depth=depth[band].copy(),
+                manning=manning[band].copy(), infil=infil[band].copy(),
+                inflows=[((inf.cell[0] - r0, inf.cell[1]), inf.hydrograph) for inf in inflows],
+                boundaries={"east": "open"}, sediment=dict(d50=np.full((rows, n), 0.002, np.float32), porosity=0.4),
+                alpha=0.7, dt_max=30.0)  # fmt: skip
+
+
+def li_reach_8192(args, legs: bool = True):
+    """The largest single-GPU configuration: the 8192^2 valley reach (infiltration, eight
+    inflow cells, bedload), 72 algorithmic bytes per cell-step; with ``legs``, the CPU
+    oracle and the float64 error on a 512 x 8192 band of it."""
     n, dx = 8192, 5.0
     z, manning, infil, inflows, depth = reach_inputs(n, dx)
     st = rbsim.State.from_bed(z, dx, depth=depth, manning=manning)
@@ -205,12 +323,33 @@ def li_reach_8192(args):
     arm_sediment(st, 0.002, 0.4)
     inj = InflowInjector(inflows, st.grid, st.device)
     # warm up on the first steps of the flood so transport is active, then time
-    clk = DeviceClock(st, "local_inertial", alpha=0.7, dt_max=30.0, sync_times=[43200.0], graph_steps=20,
-                      injector=inj)  # fmt: skip
-    clk.run_until(43200.0, max_steps=20)
+    clk = DeviceClock(st, "local_inertial", alpha=0.7, dt_max=30.0, sync_times=[43200.0],
+                      graph_steps=max(args.warmup, 1), injector=inj)  # fmt: skip
+    clk.run_until(43200.0, max_steps=max(args.warmup, 1))
+    clk.close()
     roof = _kernel_roofline(st, "local_inertial", args.steps, 72, injector=inj)
-    return {"workload": "li_reach_8192", "metric": "Gcell-updates/s", "value": roof["gcell_per_s_step"],
-            "steps": args.steps, "roofline": roof}  # fmt: skip
+    del st, clk, inj
+    torch.cuda.empty_cache()
+    out = {"workload": "li_reach_8192", "metric": "Gcell-updates/s", "value": roof["gcell_per_s_step"],
+           "steps": args.steps, "warmup": args.warmup, "roofline": roof,
+           "config": {"grid": [n, n], "dx_m": dx, "inflow_cells": len(inflows), "edges": "east open",
+                      "physics": "infiltration U(0, 20) mm/h, lognormal Manning (median 0.035, sigma 0.3), "
+                                 "MPM bedload d50 2 mm"}}  # fmt: skip
+    if legs:
+        spec = reach_band_spec(z, manning, infil, inflows, depth, rows=512)
+        cpu = cpu_leg(spec, budget_s=8.0)
+        cpu["sample"] = f"{cpu['steps']} steps of a 512 x 8192 band of the reach (the channel and the inflows), " \
+                        "C oracle with OpenMP"
+        out["cpu_baseline"] = cpu
+        out["err_vs_f64"] = f64_leg(spec, steps=10)
+        out["err_vs_f64"]["sample"] = "the same 512 x 8192 band"
+    return out
+
+
+def _digest(t: torch.Tensor) -> str:
+    import hashlib
+
+    return hashlib.blake2b(t.cpu().numpy().tobytes(), digest_size=16).hexdigest()
 
 
 def _ensemble_members(n=256, seed=5):
@@ -259,7 +398,7 @@ def ensemble_256(args):
             plain_steps += 1
     torch.cuda.synchronize()
     plain_wall = time.perf_counter() - t0
-    plain_h = [st.h.cpu().numpy() for st in sts[:8]]
+    plain_h = [_digest(st.h) for st in sts]  # every member's final depth, as a digest
     del sts
     torch.cuda.empty_cache()
 
@@ -282,7 +421,7 @@ def ensemble_256(args):
     torch.cuda.synchronize()
     batched_wall = time.perf_counter() - t0
     steps = sum(c.steps for c in ens.clock)
-    same = all(np.array_equal(sts[k].h.cpu().numpy(), plain_h[k]) for k in range(len(plain_h)))
+    same = sum(_digest(st.h) == d for st, d in zip(sts, plain_h, strict=True))
     cell_updates = sum(c.steps * b.size for c, (b, _, _) in zip(ens.clock, spec, strict=True))
     # whole job: every rank's domains over the slowest rank's time
     job_rate, job_wall = replicas.whole_job_rate(float(len(spec)), batched_wall)
@@ -294,20 +433,28 @@ def ensemble_256(args):
                     "tiles": {"li_variant": best[0]}, "autotune_ms_per_replay": {str(k): v for k, v in timings.items()},
                     "gcell_per_s_this_rank": cell_updates / batched_wall / 1e9, "steps": steps},
         "plain_loop": {"wall_s": plain_job_wall, "solves_per_s": plain_rate, "steps": plain_steps},
-        "speedup": plain_job_wall / job_wall, "first_8_domains_bitwise_equal_to_plain": same,
+        "speedup": plain_job_wall / job_wall, "domains_bitwise_equal_to_plain": f"{same} of {len(spec)}",
+        "all_domains_bitwise_equal_to_plain": same == len(spec),
     }  # fmt: skip
 
 
 def serve(args):
+    import tempfile
+
     from rbsim.serve import Server, poisson_stream, serial_baseline
 
-    out = {"workload": "serve", "metric": "solves/s, p50/p99 latency", "rates": {}}
+    out = {"workload": "serve", "metric": "solves/s, p50/p99 latency", "rates": {},
+           "frames": "every request streams a frame every 600 simulated s and at its horizon to its own result "
+                     "store, in both the batched server and the serial loop"}  # fmt: skip
     for rate in [float(r) for r in args.rates.split(",")]:
         reqs = poisson_stream(rate, args.requests, seed=int(rate * 100))
-        srv = Server(hbm_budget=150e9, graph_steps=16)
-        srv.run(reqs)
-        torch.cuda.empty_cache()
-        serial = serial_baseline(reqs)
+        for r in reqs:
+            r.output_every = 600.0
+        with tempfile.TemporaryDirectory() as tmp:
+            srv = Server(hbm_budget=150e9, graph_steps=16, out_dir=f"{tmp}/batched")
+            srv.run(reqs)
+            torch.cuda.empty_cache()
+            serial = serial_baseline(reqs, out_dir=f"{tmp}/serial")
         out["rates"][str(rate)] = {"batched": srv.stats, "serial": serial,
                                    "throughput_ratio": srv.stats["solves_per_s"] / serial["solves_per_s"]}  # fmt: skip
         torch.cuda.empty_cache()

@@ -279,6 +279,27 @@ int rb_hllc_kernel_variants(int32_t *count);
 int rb_li_set_kernel_variant(int32_t variant);
 int rb_li_kernel_variants(int32_t *count);
 
+/* --- arithmetic of the step kernels ---------------------------------------------
+ * No counterpart in the reference. A process-wide choice of the arithmetic the
+ * single-domain local-inertial step and HLLC stage kernels run with:
+ *  RB_ARITH_EXACT (the default): one IEEE rounding per operation in the
+ *    reference's expression order, no fused multiply-add, IEEE division and square
+ *    root, deterministic powers -- bit-identical to the CPU oracle;
+ *  RB_ARITH_FAST: the same kernels built with contracted multiply-adds and the
+ *    hardware's approximate division, square root and powers, the arithmetic of a
+ *    GPU build of the reference; it agrees with the exact build to the solver
+ *    tolerance, not bit for bit. Compensated (Kahan) additions stay exact.
+ * Read at each launch (a captured graph keeps the mode it was captured with).
+ * Ensembles always run the exact arithmetic. */
+#define RB_ARITH_EXACT 0
+#define RB_ARITH_FAST 1
+int rb_set_arith_mode(int32_t mode);
+int rb_arith_mode(int32_t *mode);
+/* The launch configuration in force now: LI kernel variant, HLLC kernel variant and
+ * arithmetic mode. A host that caches captured graphs keys them on it, since a graph
+ * keeps the kernels it was captured with. */
+int rb_launch_config(int32_t *li_variant, int32_t *hllc_variant, int32_t *arith_mode);
+
 /* --- reservoir release (solver/processes/reservoir.py) -------------------------
  * Boxes are inclusive (r0, c0, r1, c1), as Structure.pool / .outlet. h is the
  * current depth buffer, modified in place between steps. */

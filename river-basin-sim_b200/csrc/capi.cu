@@ -4,6 +4,7 @@
 // the reference computes in float64 (compute_dt, the open-edge drain factor, the
 // Heun banking weight), and every float32 kernel argument is rounded from the
 // float64 value exactly as Warp rounds a Python float at launch.
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -16,6 +17,7 @@
 namespace {
 
 thread_local char g_err[512] = {0};
+std::atomic<int> g_arith_mode{RB_ARITH_EXACT};
 
 int fail(int code, const char* fmt, ...) {
   va_list ap;
@@ -48,6 +50,8 @@ bool any_bc(const int32_t* bc, int kind) {
 namespace rb {
 
 void set_last_error(const char* msg) { snprintf(g_err, sizeof g_err, "%s", msg); }
+
+int arith_mode() { return g_arith_mode.load(); }
 
 // Argument checks shared by every entry point that takes a grid, edge kinds or a
 // timestep, so that all of them refuse the same inputs with the same messages.
@@ -413,6 +417,28 @@ int rb_li_set_kernel_variant(int32_t variant) {
 int rb_li_kernel_variants(int32_t* count) {
   if (count == nullptr) return fail(RB_ERR_ARG, "rb_li_kernel_variants: null argument");
   *count = rb::li_kernel_variant_count();
+  return RB_OK;
+}
+
+int rb_set_arith_mode(int32_t mode) {
+  if (mode != RB_ARITH_EXACT && mode != RB_ARITH_FAST)
+    return fail(RB_ERR_ARG, "rb_set_arith_mode: mode %d is neither RB_ARITH_EXACT nor RB_ARITH_FAST", mode);
+  g_arith_mode.store(mode);
+  return RB_OK;
+}
+
+int rb_arith_mode(int32_t* mode) {
+  if (mode == nullptr) return fail(RB_ERR_ARG, "rb_arith_mode: null argument");
+  *mode = g_arith_mode.load();
+  return RB_OK;
+}
+
+int rb_launch_config(int32_t* li_variant, int32_t* hllc_variant, int32_t* arith_mode) {
+  if (li_variant == nullptr || hllc_variant == nullptr || arith_mode == nullptr)
+    return fail(RB_ERR_ARG, "rb_launch_config: null argument");
+  *li_variant = rb::li_current_variant();
+  *hllc_variant = rb::hllc_current_variant();
+  *arith_mode = g_arith_mode.load();
   return RB_OK;
 }
 

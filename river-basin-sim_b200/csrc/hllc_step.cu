@@ -28,6 +28,7 @@
 #include "rb_kernels.h"
 
 namespace rb {
+RB_ARITH_BEGIN
 
 // hllc.py:158-165 _minmod
 __device__ __forceinline__ float minmod(float a, float b) {
@@ -63,7 +64,7 @@ __device__ __forceinline__ void hllc_flux(float hl, float ul, float vtl, float h
     sr = ul + 2.0f * cl;
   } else {
     const float hs = 0.5f * (cl + cr) + 0.25f * (ul - ur);
-    const float h_star = rmax(rb_div_g(hs * hs), 0.0f);  // = hs * hs / g, bit for bit
+    const float h_star = rmax(div_g(hs * hs), 0.0f);  // hs * hs / g
     const float c_star = sqrtf(g * h_star);
     const float u_star = 0.5f * (ul + ur) + cl - cr;
     sl = rmin(ul - cl, u_star - c_star);
@@ -86,10 +87,10 @@ __device__ __forceinline__ void hllc_flux(float hl, float ul, float vtl, float h
     fmn = (sr * fmn_l - sl * fmn_r + sl * sr * (hr * ur - hl * ul)) * inv;
   }
   // The contact speed s_star is read only through s_star >= 0 (hllc.py:231-238), so
-  // its sign is decided exactly without the division (rb_quotient_nonneg).
+  // its sign is decided without the division (quotient_nonneg).
   const float den_s = hr * (ur - sr) - hl * (ul - sl);
   const bool star_nonneg = fabsf(den_s) > 1.0e-12f
-                               ? rb_quotient_nonneg(sl * hr * (ur - sr) - sr * hl * (ul - sl), den_s) != 0
+                               ? quotient_nonneg(sl * hr * (ur - sr) - sr * hl * (ul - sl), den_s)
                                : 0.5f * (ul + ur) >= 0.0f;
   const float vt = star_nonneg ? vtl : vtr;
   f0 = fh;
@@ -632,7 +633,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
         if (!((k == 0.0f && m2 <= FLT_MAX) || (m2 == 0.0f && k <= FLT_MAX))) {
           const float f = k * sqrtf(m2);
           if (!(f == 0.0f)) {
-            const float denom = 1.0f + f / rb_pow73f(hh);
+            const float denom = 1.0f + f / pow73(hh);
             hu = div_pos(hu, denom);
             hv = div_pos(hv, denom);
           }
@@ -741,9 +742,11 @@ static const HllcKernelVariant kHllcVariants[] = {
 };
 constexpr int kNumHllcVariants = (int)(sizeof(kHllcVariants) / sizeof(kHllcVariants[0]));
 constexpr int kDefaultHllcVariant = 6;
+#if !defined(RB_FAST_MATH)
 static std::atomic<int> g_hllc_variant{kDefaultHllcVariant};
 
 int hllc_kernel_variant_count() { return kNumHllcVariants; }
+#endif
 
 // Set every variant's shared-memory opt-in on the current device, outside any
 // stream capture (called by the non-capturable set-up entry points).
@@ -755,7 +758,11 @@ void hllc_prepare_device() {
   prepare_hllc<32, 32, 512, 1, 1>();
   prepare_hllc<64, 16, 512, 1, 1>();
   prepare_hllc<32, 32, 640, 1, 1>();
+#if !defined(RB_FAST_MATH)
+  fast::hllc_prepare_device();
+#endif
 }
+#if !defined(RB_FAST_MATH)
 bool hllc_set_kernel_variant(int v) {
   if (v < 0 || v >= kNumHllcVariants) return false;
   g_hllc_variant.store(v);
@@ -768,7 +775,12 @@ cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s) {
   return hllc_stage_launch_variant(p, stage, g_hllc_variant.load(), s);
 }
 
+#endif  // !RB_FAST_MATH
+
 cudaError_t hllc_stage_launch_variant(const HllcParams& p, int stage, int variant, cudaStream_t s) {
+#if !defined(RB_FAST_MATH)
+  if (arith_mode() == RB_ARITH_FAST) return fast::hllc_stage_launch_variant(p, stage, variant, s);
+#endif
   switch (variant) {
     case 1: return launch_hllc<32, 16, 256, 1, 1>(p, stage, s);
     case 2: return launch_hllc<32, 16, 256, 3, 1>(p, stage, s);
@@ -780,6 +792,7 @@ cudaError_t hllc_stage_launch_variant(const HllcParams& p, int stage, int varian
   }
 }
 
+#if !defined(RB_FAST_MATH)
 // Tiles of the current variant (one ledger slot each); never more than the 32 x 8
 // tiling the workspace ledger is sized for.
 int hllc_tiles(int ny, int nx) { return hllc_tiles_of(g_hllc_variant.load(), ny, nx); }
@@ -903,5 +916,7 @@ cudaError_t ens_hllc_launch(int variant, int grid, int stage, const HllcParams* 
   }
   return cudaGetLastError();
 }
+#endif  // !RB_FAST_MATH: the ensembles run the exact arithmetic only
 
+RB_ARITH_END
 }  // namespace rb

@@ -39,18 +39,19 @@
 #include "rb_kernels.h"
 
 namespace rb {
+RB_ARITH_BEGIN
 
 // sediment.py:161-207 kinematic_shear / shields_number / mpm_capacity / face_capacity.
 __device__ __forceinline__ float face_capacity(float q, float h, float radius, float n, float d50) {
   if (h < kHDry || d50 <= 0.0f || q == 0.0f) return 0.0f;
-  const float tau = div_pos(kG * n * n * q * q, h * h * rb_pow13f(radius));
+  const float tau = div_pos(kG * n * n * q * q, h * h * pow13(radius));
   const float theta = div_pos(tau, 1.65f * kG * d50);
   float qs;
   if (theta <= 0.047f) {
     qs = 0.0f;
   } else {
     const float excess = theta - 0.047f;
-    qs = 8.0f * rb_pow15f(excess) * sqrtf(1.65f * kG * d50 * d50 * d50);
+    qs = 8.0f * pow15(excess) * sqrtf(1.65f * kG * d50 * d50 * d50);
   }
   return q < 0.0f ? -qs : qs;
 }
@@ -76,7 +77,7 @@ __device__ __forceinline__ float channel_flux(float q_prev, float eta_max, float
   // zero dividends as in manning_divide: a zero friction numerator makes den exactly 1
   const float f = kG * dt * n_ch * n_ch * fabsf(q_prev);
   if (f == 0.0f) return num;
-  const float den = 1.0f + f / (h_ch * rb_pow43f(radius));
+  const float den = 1.0f + f / (h_ch * pow43(radius));
   return div_pos(num, den);
 }
 
@@ -602,6 +603,7 @@ struct LiKernelVariant {
 static const LiKernelVariant kLiVariants[] = {{32, 16, 256}, {32, 32, 512}, {64, 16, 512}, {32, 8, 256}, {32, 16, 256}};
 constexpr int kNumLiVariants = (int)(sizeof(kLiVariants) / sizeof(kLiVariants[0]));
 constexpr int kDefaultLiVariant = 1;
+#if !defined(RB_FAST_MATH)
 static std::atomic<int> g_li_variant{kDefaultLiVariant};
 
 int li_kernel_variant_count() { return kNumLiVariants; }
@@ -611,9 +613,17 @@ bool li_set_kernel_variant(int v) {
   return true;
 }
 
+int li_current_variant() { return g_li_variant.load(); }
+
 cudaError_t li_step_launch(const LiParams& p, cudaStream_t s) {
+  if (arith_mode() == RB_ARITH_FAST) return fast::li_step_launch_variant(p, g_li_variant.load(), s);
+  return li_step_launch_variant(p, g_li_variant.load(), s);
+}
+#endif  // !RB_FAST_MATH
+
+cudaError_t li_step_launch_variant(const LiParams& p, int variant, cudaStream_t s) {
   if (p.cw != nullptr) return launch_li<32, 16, 256, true, 1>(p, s);
-  switch (g_li_variant.load()) {
+  switch (variant) {
     case 0: return launch_li<32, 16, 256, false, 1>(p, s);
     case 2: return launch_li<64, 16, 512, false, 3>(p, s);
     case 3: return launch_li<32, 8, 256, false, 1>(p, s);
@@ -622,6 +632,7 @@ cudaError_t li_step_launch(const LiParams& p, cudaStream_t s) {
   }
 }
 
+#if !defined(RB_FAST_MATH)
 // Ensemble: a persistent grid walks the (domain, local tile) work-list of every
 // local-inertial domain; a tile of a domain whose clock is not active returns at
 // its first instruction. Each domain's tiles, ledger slots and clock are its own,
@@ -688,5 +699,7 @@ cudaError_t ens_li_launch(int variant, int grid, const LiParams* P, const int2* 
   }
   return cudaGetLastError();
 }
+#endif  // !RB_FAST_MATH: the ensembles run the exact arithmetic only
 
+RB_ARITH_END
 }  // namespace rb

@@ -1,11 +1,18 @@
 // rb_common.cuh -- shared device helpers for the river-basin solver kernels.
 //
-// Arithmetic contract (identical to the CPU oracle): every kernel is compiled with
-// --fmad=false and IEEE division/square root, so each operation rounds once in
-// the reference's expression order; the fractional powers come from
-// include/rb_detmath.h. `rmax/rmin/rclamp` are the scalar builtins of the
-// reference's kernel language (a > b ? a : b, a < b ? a : b, min(max(lo,x),hi)),
-// which differ from fmaxf/fminf on signed zeros.
+// Two arithmetic contracts, one source:
+//  * exact (every translation unit in csrc/): compiled with --fmad=false and IEEE
+//    division / square root, so each operation rounds once in the reference's
+//    expression order (identical to the CPU oracle); the fractional powers come
+//    from include/rb_detmath.h;
+//  * fast (csrc/fast/, RB_FAST_MATH defined, everything in namespace rb::fast):
+//    contracted multiply-adds, the hardware's approximate division and square root
+//    and __powf for the fractional powers -- the arithmetic of a GPU build of the
+//    reference, held to the solver tolerance instead of bit equality. Compensated
+//    (Kahan) additions stay explicit IEEE adds in both.
+// `rmax/rmin/rclamp` are the scalar builtins of the reference's kernel language
+// (a > b ? a : b, a < b ? a : b, min(max(lo,x),hi)), which differ from
+// fmaxf/fminf on signed zeros.
 #pragma once
 
 #include <cstdint>
@@ -14,23 +21,52 @@
 #include "rb_detmath.h"
 #include "rbsim.h"
 
+// The kernels of a translation unit live in rb (exact) or rb::fast (fast).
+#if defined(RB_FAST_MATH)
+#define RB_ARITH_BEGIN namespace fast {
+#define RB_ARITH_END }
+#else
+#define RB_ARITH_BEGIN
+#define RB_ARITH_END
+#endif
+
 namespace rb {
 
 constexpr float kG = 9.81f;     // solver/core/grid.py:43 GRAVITY
 constexpr float kHDry = 1.0e-3f;  // solver/core/grid.py:48 H_DRY
 
+RB_ARITH_BEGIN
+
 __device__ __forceinline__ float rmax(float a, float b) { return a > b ? a : b; }
 __device__ __forceinline__ float rmin(float a, float b) { return a < b ? a : b; }
 __device__ __forceinline__ float rclamp(float x, float lo, float hi) { return rmin(rmax(lo, x), hi); }
 
-// sources.py:66-82 kahan_add: (total, comp) <- compensated total + inc.
+// sources.py:66-82 kahan_add: (total, comp) <- compensated total + inc. Explicit
+// IEEE adds, which no build contracts or reassociates.
 __device__ __forceinline__ void kahan_add(float& total, float& comp, float inc) {
-  const float y = inc - comp;
-  const float t = total + y;
-  comp = (t - total) - y;
+  const float y = __fsub_rn(inc, comp);
+  const float t = __fadd_rn(total, y);
+  comp = __fsub_rn(__fsub_rn(t, total), y);
   total = t;
 }
 
+#if defined(RB_FAST_MATH)
+// Fast arithmetic: the approximate division has no slow path to steer around, so
+// the quotient helpers are plain divisions (an unused lane divides by 1).
+__device__ __forceinline__ float opaque(float v) { return v; }
+__device__ __forceinline__ float div_pos(float x, float y) { return x / y; }
+__device__ __forceinline__ float div_if(bool use, float x, float y) { return use ? x / (use ? y : 1.0f) : 0.0f; }
+__device__ __forceinline__ float div_in_branch(float x, float y) { return x / y; }
+// x / g
+__device__ __forceinline__ float div_g(float x) { return x * (1.0f / kG); }
+// n / d >= 0 for |d| > 0, from the signs
+__device__ __forceinline__ bool quotient_nonneg(float n, float d) { return n == 0.0f || ((n > 0.0f) == (d > 0.0f)); }
+// x ^ float32(p) for x > 0 with the float32 exponents of the reference (7/3, 1/3, 4/3, 1.5)
+__device__ __forceinline__ float pow73(float x) { return __powf(x, 2.33333325f); }
+__device__ __forceinline__ float pow13(float x) { return __powf(x, 0.333333343f); }
+__device__ __forceinline__ float pow43(float x) { return __powf(x, 1.33333337f); }
+__device__ __forceinline__ float pow15(float x) { return x * sqrtf(x); }
+#else
 // Zero operands. The IEEE single-precision division takes its slow path when the
 // dividend is zero (about 3x the cost of the fast path on B200) or the divisor is.
 // Still water, dry neighbours and frictionless beds make such operands common, and
@@ -71,6 +107,14 @@ __device__ __forceinline__ float div_in_branch(float x, float y) {
   return q;
 }
 
+__device__ __forceinline__ float div_g(float x) { return rb_div_g(x); }  // x / g, bit for bit
+__device__ __forceinline__ bool quotient_nonneg(float n, float d) { return rb_quotient_nonneg(n, d) != 0; }
+__device__ __forceinline__ float pow73(float x) { return rb_pow73f(x); }
+__device__ __forceinline__ float pow13(float x) { return rb_pow13f(x); }
+__device__ __forceinline__ float pow43(float x) { return rb_pow43f(x); }
+__device__ __forceinline__ float pow15(float x) { return rb_pow15f(x); }
+#endif  // RB_FAST_MATH
+
 // channels.py:58-70 eta_subgrid: the storage curve h -> eta.
 __device__ __forceinline__ float eta_subgrid(float h, float z, float w, float d, float dx) {
   float eta = h + z;
@@ -99,7 +143,7 @@ __device__ __forceinline__ float column_depth(float h, float w, float d, float d
 
 // friction.py:18-31 manning_denominator
 __device__ __forceinline__ float manning_denominator(float q_prev, float h_flow, float n, float g, float dt) {
-  return 1.0f + g * dt * n * n * fabsf(q_prev) / rb_pow73f(h_flow);
+  return 1.0f + g * dt * n * n * fabsf(q_prev) / pow73(h_flow);
 }
 
 // num / manning_denominator(q_prev, h_flow, n, g, dt) for h_flow >= H_DRY, with the
@@ -108,7 +152,7 @@ __device__ __forceinline__ float manning_denominator(float q_prev, float h_flow,
 __device__ __forceinline__ float manning_divide(float num, float q_prev, float h_flow, float n, float g, float dt) {
   const float f = g * dt * n * n * fabsf(q_prev);
   if (f == 0.0f) return num;
-  const float den = 1.0f + f / rb_pow73f(h_flow);
+  const float den = 1.0f + f / pow73(h_flow);
   return div_pos(num, den);
 }
 
@@ -172,4 +216,5 @@ __device__ __forceinline__ void flag_error(unsigned int* err, unsigned int bit) 
   if (err) atomicOr(err, bit);
 }
 
+RB_ARITH_END
 }  // namespace rb

@@ -95,6 +95,11 @@ struct HllcParams {
 };
 
 cudaError_t li_step_launch(const LiParams& p, cudaStream_t s);
+cudaError_t li_step_launch_variant(const LiParams& p, int variant, cudaStream_t s);
+int li_current_variant();
+// Arithmetic of the single-domain step kernels (RB_ARITH_EXACT / RB_ARITH_FAST),
+// set with rb_set_arith_mode; the launchers above dispatch on it.
+int arith_mode();
 cudaError_t clock_plan_launch(DevClock* clk, cudaStream_t s);
 cudaError_t clock_commit_launch(DevClock* clk, cudaStream_t s);
 cudaError_t clock_target_launch(DevClock* clk, double t_target, int max_steps, cudaStream_t s);
@@ -165,5 +170,12 @@ cudaError_t inject_points(float* h, int nx, int nsrc, const int32_t* rows, const
 cudaError_t exner_apply(int ny, int nx, float dx32, float inv1mp, float* qs_int_x, float* qs_int_y,
                         const float* dz_lo, const float* dz_hi, double* dz_cum, double* dz_unapplied,
                         const float* z0, float* z, cudaStream_t s);
+
+// The same step kernels built with fast arithmetic (csrc/fast/, RB_FAST_MATH).
+namespace fast {
+cudaError_t li_step_launch_variant(const LiParams& p, int variant, cudaStream_t s);
+cudaError_t hllc_stage_launch_variant(const HllcParams& p, int stage, int variant, cudaStream_t s);
+void hllc_prepare_device();
+}  // namespace fast
 
 }  // namespace rb

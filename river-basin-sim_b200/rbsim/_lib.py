@@ -22,6 +22,8 @@ RB_ERR_STEP = -5
 RB_DEVERR_NONFINITE = 1
 RB_DEVERR_CLOCK = 2
 RB_DEVERR_STEPS = 4
+RB_ARITH_EXACT = 0
+RB_ARITH_FAST = 1
 
 EDGES = ("north", "south", "east", "west")  # the ABI's per-edge order
 BC_CODE = {"closed": 0, "open": 1, "fixed_stage": 2}
@@ -124,6 +126,9 @@ SIGNATURES = {
     "rb_ensemble_read": (ctypes.c_int, [ctypes.POINTER(EnsembleLayout), _P, _P, _P]),
     "rb_li_set_kernel_variant": (ctypes.c_int, [ctypes.c_int32]),
     "rb_li_kernel_variants": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
+    "rb_launch_config": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)] * 3),
+    "rb_set_arith_mode": (ctypes.c_int, [ctypes.c_int32]),
+    "rb_arith_mode": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
     "rb_hllc_set_kernel_variant": (ctypes.c_int, [ctypes.c_int32]),
     "rb_hllc_kernel_variants": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int32)]),
     "rb_li_clock_reseed": (ctypes.c_int, [ctypes.POINTER(LiFields), ctypes.c_int32, _P, _P]),
@@ -162,6 +167,13 @@ def lib() -> ctypes.CDLL:
 
 class DeviceError(RuntimeError):
     """A kernel raised a device-side error bit (e.g. a non-finite depth)."""
+
+
+def launch_config() -> tuple[int, int, int]:
+    """(LI kernel variant, HLLC kernel variant, arithmetic mode) the library launches with now."""
+    li, hl, mode = ctypes.c_int32(0), ctypes.c_int32(0), ctypes.c_int32(0)
+    check(lib().rb_launch_config(ctypes.byref(li), ctypes.byref(hl), ctypes.byref(mode)))
+    return li.value, hl.value, mode.value
 
 
 def last_error() -> str:

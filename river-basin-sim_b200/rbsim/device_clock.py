@@ -15,6 +15,14 @@ device at the step midpoint, as the host loop samples them.
 Sync times must include every time a step may not cross (outputs, forcing
 breakpoints, slow-process activations, the end time), exactly as they are given
 to ``MultiRateScheduler``; ``run_until`` is then called with a sync time as target.
+
+Set-up cost. A span shorter than ``graph_steps`` is enqueued launch by launch, with
+no capture at all (the device clock still plans every step; the host only issues
+the launches, which overlap the device's work). A captured span graph is kept in a
+small process-wide cache keyed by everything its launches bake in -- the field and
+workspace pointers, the step count, the inflow flag, the kernel variant and the
+arithmetic mode -- so a clock built again over the same buffers (a re-run, the
+next request on recycled memory) replays it without capturing or instantiating.
 """
 
 from __future__ import annotations
@@ -25,9 +33,31 @@ import math
 import numpy as np
 import torch
 
+from collections import OrderedDict
+
 from . import _lib, graphs
 from .scheduler import EPS_T
 from .state import State
+
+_GRAPH_CACHE_SIZE = 8
+_graph_cache: OrderedDict = OrderedDict()
+
+
+def _cached_graph(key, build):
+    """The instantiated graph for ``key``, capturing it with ``build()`` on a miss."""
+    g = _graph_cache.get(key)
+    if g is None:
+        g = build()
+        _graph_cache[key] = g
+        while len(_graph_cache) > _GRAPH_CACHE_SIZE:
+            _graph_cache.popitem(last=False)
+    else:
+        _graph_cache.move_to_end(key)
+    return g
+
+
+def clear_graph_cache() -> None:
+    _graph_cache.clear()
 
 
 class DeviceClock:
@@ -106,12 +136,20 @@ class DeviceClock:
         else:
             _lib.check(self._L.rb_li_enqueue_steps(ctypes.byref(self._fields), n, src, ws, stream))
 
-    def _replay(self) -> None:
-        if not self.use_graph:
-            self._enqueue(self.graph_steps, self.state.stream)
+    def _graph_key(self):
+        return (self.state.device.index, self.scheme, bytes(self._fields), self.state.workspace.data_ptr(),
+                self.graph_steps, self._cfg.nsrc > 0, _lib.launch_config())  # fmt: skip
+
+    def _replay(self, steps: int | None = None) -> None:
+        """Enqueue one span: ``graph_steps`` steps from the (cached) graph, or, for a
+        shorter span, ``steps`` steps launched directly."""
+        if steps is not None and steps < self.graph_steps or not self.use_graph:
+            self._enqueue(self.graph_steps if steps is None else steps, self.state.stream)
             return
         if self._graph is None:
-            self._graph = graphs.capture(self.state.device, lambda s: self._enqueue(self.graph_steps, s))
+            dev = self.state.device
+            self._graph = _cached_graph(self._graph_key(),
+                                        lambda: graphs.capture(dev, lambda s: self._enqueue(self.graph_steps, s)))
         self._graph.replay()
 
     def set_target(self, t_target: float, max_steps: int = 2**31 - 1) -> None:
@@ -136,7 +174,7 @@ class DeviceClock:
         self.set_target(t_target, max_steps)
         while True:
             before = self.steps
-            self._replay()
+            self._replay(max(max_steps - (self.steps - start), 1))
             st = self.read()
             taken = st.steps - start
             if st.t >= t_target - EPS_T or taken >= max_steps:
@@ -154,8 +192,11 @@ class DeviceClock:
     def enqueue_span(self, max_steps: int) -> None:
         """Enqueue (without waiting) replays covering at most ``max_steps`` more steps."""
         self.set_target(math.inf, max_steps)
-        for _ in range(-(-max_steps // self.graph_steps)):
+        full, rest = divmod(max_steps, self.graph_steps)
+        for _ in range(full):
             self._replay()
+        if rest:
+            self._replay(rest)
 
     def close(self) -> None:
         self._graph = None

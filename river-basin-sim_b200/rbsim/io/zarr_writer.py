@@ -216,10 +216,12 @@ class AsyncFrameWriter:
             raise self._error
         torch = self._torch
         bufs = self._free.get()
+        # snapshot on the compute stream: the steps after this call write the state's
+        # buffers again while the side stream may still be copying them
+        srcs = [t.clone() for t in (depth, u, v)] + ([bed_change.float()] if bed_change is not None else [])
         ready = torch.cuda.Event()
         ready.record(torch.cuda.current_stream(self.device))
         self._side.wait_event(ready)
-        srcs = [depth, u, v] + ([bed_change.float()] if bed_change is not None else [])
         with torch.cuda.stream(self._side):
             for b, s in zip(bufs, srcs, strict=True):
                 b.copy_(s, non_blocking=True)

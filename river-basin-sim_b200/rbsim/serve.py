@@ -6,10 +6,19 @@ while the HBM they need fits the budget, keeps every admitted solve resident, an
 steps all of them together as one ``Ensemble`` (one persistent kernel per scheme
 over every member's tiles, each member on its own device clock). Between graph
 replays it retires finished solves (freeing their memory), runs due slow processes
-(Exner activations) for the members that reached them, writes output frames
-asynchronously, and admits whatever arrived meanwhile -- so new work joins the
-batch while older work is still on the GPU. Each result is bit-identical to
-solving that request alone (``solve_alone``).
+(Exner activations) for the members that reached them, streams output frames, and
+admits whatever arrived meanwhile -- so new work joins the batch while older work
+is still on the GPU. Each result is bit-identical to solving that request alone
+(``solve_alone``), frames included.
+
+Frames. With ``out_dir`` set, every request with ``output_every > 0`` gets its own
+result store (``req_<rid>.zarr``, the layout of ``rbsim.io.zarr_writer``, as the
+reference's run loop writes one per run, solver/run.py:329-429): frame 0 at
+admission, then one frame at every multiple of ``output_every`` and at the horizon
+(each member's clock lands on those times exactly). A frame's fields are copied
+device-to-host on a side stream into pinned buffers and written by one writer
+thread (``FrameStream``), so the batch keeps stepping while frames travel; a
+bounded queue holds at most ``max_pending_frames`` frames in flight.
 
 ``serial_baseline`` solves the same requests one after another, each alone, in
 arrival order: the plain loop the batched server is measured against.
@@ -18,13 +27,18 @@ arrival order: the plain loop the batched server is measured against.
 from __future__ import annotations
 
 import math
+import queue
+import threading
 import time
 from dataclasses import dataclass, field
+from pathlib import Path
 
 import numpy as np
 import torch
 
 from .ensemble import Ensemble
+from .grid import H_DRY
+from .io.zarr_writer import ZarrWriter
 from .processes.morphology import MorphologyProcess
 from .scheduler import EPS_T
 from .sediment import arm_sediment
@@ -45,6 +59,7 @@ class Request:
     dx: float = 10.0
     rain_mm_hr: float = 30.0
     morph_interval: float = 300.0
+    output_every: float = 0.0  # simulated seconds between frames; 0: no frames
 
 
 @dataclass
@@ -72,6 +87,93 @@ def request_bytes(req: Request) -> int:
         if req.exner:
             per += 4 + 4 + 8 + 8 + 16  # d50, z0, dz_cum, dz_unapplied, four transport accumulators
     return per * n + (1 << 20)
+
+
+def output_times(req: Request) -> list[float]:
+    """Frame times after t = 0: multiples of ``output_every`` up to the horizon, and the horizon."""
+    if req.output_every <= 0.0:
+        return []
+    out, k = [], 1
+    while k * req.output_every < req.horizon - EPS_T:
+        out.append(k * req.output_every)
+        k += 1
+    return out + [req.horizon]
+
+
+def _cell_velocities(st: State):
+    """Cell-centred (u, v) on the device, 0 where h < H_DRY (state.py:232-256)."""
+    h = st.h
+    if st.hu is not None:
+        qx, qy = st.hu, st.hv
+    else:
+        qx = 0.5 * (st.qx[:, :-1] + st.qx[:, 1:])
+        qy = 0.5 * (st.qy[:-1, :] + st.qy[1:, :])
+    wet = h >= H_DRY
+    zero = torch.zeros_like(h)
+    return torch.where(wet, qx / h, zero), torch.where(wet, qy / h, zero)
+
+
+class FrameStream:
+    """Frames of every served request to that request's store, off the compute path.
+
+    ``submit`` orders a frame's device-to-host copies on a side stream after the
+    compute stream's work so far, into pinned buffers, and queues the write; one
+    thread waits for each copy to land and appends it to its store. ``finish``
+    queues a store's finalisation behind its frames. The queue is bounded, so at
+    most ``max_pending`` frames' buffers are in flight.
+    """
+
+    def __init__(self, device, max_pending: int = 8):
+        self.device = device
+        self._side = torch.cuda.Stream(device)
+        self._jobs: queue.Queue = queue.Queue(maxsize=max(1, int(max_pending)))
+        self._error: BaseException | None = None
+        self._thread = threading.Thread(target=self._run, daemon=True)
+        self._thread.start()
+        self.frames = 0
+
+    def submit(self, writer: ZarrWriter, t: float, fields: list) -> None:
+        if self._error is not None:
+            raise self._error
+        ready = torch.cuda.Event()
+        ready.record(torch.cuda.current_stream(self.device))
+        self._side.wait_event(ready)
+        with torch.cuda.stream(self._side):
+            bufs = []
+            for f in fields:
+                b = torch.empty(f.shape, dtype=torch.float32, pin_memory=True)
+                b.copy_(f, non_blocking=True)
+                f.record_stream(self._side)
+                bufs.append(b)
+            done = torch.cuda.Event()
+            done.record(self._side)
+        self._jobs.put(("frame", writer, float(t), done, bufs))
+        self.frames += 1
+
+    def finish(self, writer: ZarrWriter, attrs: dict) -> None:
+        self._jobs.put(("finish", writer, attrs))
+
+    def _run(self) -> None:
+        while True:
+            job = self._jobs.get()
+            if job is None:
+                return
+            try:
+                if job[0] == "frame":
+                    _, writer, t, done, bufs = job
+                    done.synchronize()
+                    arrs = [b.numpy() for b in bufs]
+                    writer.append(t, arrs[0], arrs[1], arrs[2], arrs[3] if len(arrs) > 3 else None)
+                else:
+                    job[1].finalize(job[2])
+            except BaseException as e:  # surfaced on the next submit / close
+                self._error = e
+
+    def close(self) -> None:
+        self._jobs.put(None)
+        self._thread.join()
+        if self._error is not None:
+            raise self._error
 
 
 def build_state(req: Request, device) -> tuple[State, MorphologyProcess | None]:
@@ -111,10 +213,12 @@ class _Member:
     t: float = 0.0  # simulated time reached
     steps: int = 0  # steps taken
     base_steps: int = 0  # steps taken before the current ensemble was built
+    writer: ZarrWriter | None = None  # the request's result store, when frames are streamed
+    outputs: list[float] = field(default_factory=list)  # frame times still to come
 
     @property
     def target(self) -> float:
-        return min(self.next_act, self.req.horizon)
+        return min(self.next_act, self.outputs[0] if self.outputs else math.inf, self.req.horizon)
 
     def sync_times(self) -> list[float]:
         acts = []
@@ -123,7 +227,15 @@ class _Member:
             while k * self.req.morph_interval <= self.req.horizon + EPS_T:
                 acts.append(k * self.req.morph_interval)
                 k += 1
-        return sorted({*acts, self.req.horizon})
+        return sorted({*acts, *output_times(self.req), self.req.horizon})
+
+    def frame_fields(self) -> list:
+        """The frame's fields as fresh device tensors: the depth is snapshotted on the
+        compute stream, because the steps that follow write its buffer again while the
+        side stream may still be copying."""
+        u, v = _cell_velocities(self.st)
+        extra = [self.st.sediment.dz_cum.float()] if self.morph is not None else []
+        return [self.st.h.clone(), u, v, *extra]
 
 
 def _build_ensemble(members: list[_Member], graph_steps: int) -> Ensemble:
@@ -141,16 +253,42 @@ def _build_ensemble(members: list[_Member], graph_steps: int) -> Ensemble:
     return ens
 
 
+def _open_store(req: Request, st: State, out_dir: Path, morph) -> ZarrWriter:
+    attrs = {"scheme": req.scheme, "dx": req.dx, "coarsen": 1,
+             "units": {"depth": "m", "u": "m/s", "v": "m/s", "time": "s", "bed": "m"},
+             "scenario": f"request {req.rid}", "request": {"rid": req.rid, "seed": req.seed, "side": req.side},
+             "rain_type": "uniform", "rain_mm_hr": req.rain_mm_hr, "rain_duration_s": req.horizon,
+             "end_time_s": req.horizon, "output_every_s": req.output_every, "solver": "rbsim serve (B200 CUDA)"}  # fmt: skip
+    w = ZarrWriter(out_dir / f"req_{req.rid}.zarr", st.grid, 1 + len(output_times(req)), attrs,
+                   bed_change=morph is not None)  # fmt: skip
+    w.write_bed(st.z.cpu().numpy())
+    return w
+
+
 @dataclass
 class Server:
     hbm_budget: float = 150e9
     graph_steps: int = 16
     device: str = "cuda"
     keep_depth: bool = False
+    out_dir: str | None = None  # where requests with output_every > 0 get their result stores
+    max_pending_frames: int = 8
     stats: dict = field(default_factory=dict)
 
     def run(self, requests: list[Request]) -> list[Result]:
         dev = torch.device(self.device)
+        frames = FrameStream(dev, self.max_pending_frames) if self.out_dir is not None else None
+        try:
+            return self._serve(requests, dev, frames)
+        finally:
+            if frames is not None:
+                frames.close()
+                self.stats["frames"] = frames.frames
+
+    def _serve(self, requests: list[Request], dev, frames: FrameStream | None) -> list[Result]:
+        out_dir = Path(self.out_dir) if self.out_dir is not None else None
+        if out_dir is not None:
+            out_dir.mkdir(parents=True, exist_ok=True)
         queue = sorted(requests, key=lambda r: r.arrival)
         active: list[_Member] = []
         results: list[Result] = []
@@ -165,6 +303,10 @@ class Server:
                 st, morph = build_state(req, dev)
                 m = _Member(req, st, morph, admitted=time.perf_counter() - t0, nbytes=request_bytes(req),
                             next_act=req.morph_interval if morph is not None else math.inf)  # fmt: skip
+                if frames is not None and req.output_every > 0.0:
+                    m.writer = _open_store(req, st, out_dir, morph)
+                    m.outputs = output_times(req)
+                    frames.submit(m.writer, 0.0, m.frame_fields())
                 active.append(m)
                 used += m.nbytes
                 ens = None
@@ -189,9 +331,15 @@ class Server:
                     m.last_act = c.t
                     m.next_act += m.req.morph_interval
                     retarget = True
+                if m.outputs and c.t >= m.outputs[0] - EPS_T:  # after the slow processes, as run.py
+                    m.outputs.pop(0)
+                    frames.submit(m.writer, c.t, m.frame_fields())
+                    retarget = True
                 if c.t >= m.req.horizon - EPS_T:
                     finished.append(m)
             for m in finished:
+                if m.writer is not None:
+                    frames.finish(m.writer, {"steps": m.steps})
                 depth = m.st.h.cpu().numpy() if self.keep_depth else None
                 results.append(Result(m.req.rid, m.req.arrival, m.admitted, time.perf_counter() - t0, m.steps,
                                       m.t, depth))  # fmt: skip
@@ -212,14 +360,14 @@ class Server:
         return sorted(results, key=lambda r: r.rid)
 
 
-def solve_alone(req: Request, device="cuda", graph_steps: int = 16) -> Result:
+def solve_alone(req: Request, device="cuda", graph_steps: int = 16, out_dir: str | None = None) -> Result:
     """One request on its own (the reference for "same alone and in the mix")."""
-    srv = Server(graph_steps=graph_steps, device=device, keep_depth=True)
+    srv = Server(graph_steps=graph_steps, device=device, keep_depth=True, out_dir=out_dir)
     r = Request(**{**req.__dict__, "arrival": 0.0})
     return srv.run([r])[0]
 
 
-def serial_baseline(requests: list[Request], device="cuda", graph_steps: int = 16) -> dict:
+def serial_baseline(requests: list[Request], device="cuda", graph_steps: int = 16, out_dir: str | None = None) -> dict:
     """The plain loop: each request solved alone, in arrival order, one after another."""
     t0 = time.perf_counter()
     lat = []
@@ -227,7 +375,7 @@ def serial_baseline(requests: list[Request], device="cuda", graph_steps: int = 1
         now = time.perf_counter() - t0
         if req.arrival > now:
             time.sleep(req.arrival - now)
-        solve_alone(req, device, graph_steps)
+        solve_alone(req, device, graph_steps, out_dir)
         lat.append(time.perf_counter() - t0 - req.arrival)
     wall = time.perf_counter() - t0
     lat = np.array(lat)

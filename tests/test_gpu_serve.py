@@ -44,3 +44,34 @@ def test_results_are_the_same_alone_and_in_the_mix(room):
         alone = solve_alone(req, graph_steps=4)
         assert alone.steps == res.steps, req.rid
         np.testing.assert_array_equal(res.depth, alone.depth, err_msg=f"request {req.rid}")
+
+
+def test_frames_stream_and_are_the_same_alone_and_in_the_mix(tmp_path):
+    """Each request with output_every > 0 gets its own result store: frame 0, one frame at
+    every multiple of output_every and at the horizon, written while the batch steps on.
+    Every frame (time, depth, u, v, bed change) is bit-identical to the request served alone."""
+    from rbsim.io.zarr_writer import read_array, read_attrs
+    from rbsim.serve import Server, output_times, solve_alone
+
+    reqs = _stream()
+    for k, r in enumerate(reqs):
+        r.output_every = 0.0 if k == 2 else 50.0  # one request streams nothing
+    srv = Server(hbm_budget=150e9, graph_steps=4, out_dir=str(tmp_path / "mix"))
+    srv.run(reqs)
+    want_frames = sum(1 + len(output_times(r)) for r in reqs if r.output_every > 0)
+    assert srv.stats["frames"] == want_frames
+    assert not (tmp_path / "mix" / "req_2.zarr").exists()
+    for req in reqs:
+        if req.output_every <= 0:
+            continue
+        solve_alone(req, graph_steps=4, out_dir=str(tmp_path / "alone"))
+        mix, alone = tmp_path / "mix" / f"req_{req.rid}.zarr", tmp_path / "alone" / f"req_{req.rid}.zarr"
+        n = 1 + len(output_times(req))
+        assert read_attrs(mix)["n_frames"] == read_attrs(alone)["n_frames"] == n
+        times = read_array(mix, "time")
+        np.testing.assert_allclose(times, [0.0, *output_times(req)], rtol=0, atol=1e-6)
+        names = ["time", "depth", "u", "v", "bed"] + (["bed_change"] if req.exner else [])
+        for name in names:
+            np.testing.assert_array_equal(read_array(mix, name), read_array(alone, name),
+                                          err_msg=f"request {req.rid}: {name}")  # fmt: skip
+        assert np.isfinite(read_array(mix, "depth")).all()

@@ -112,15 +112,17 @@ def test_noalloc_step_matches_the_workspace_step_on_two_calls_in_a_row(ny, nx, b
 
 
 def test_noalloc_step_reports_a_non_finite_state():
+    """The HLLC stages clamp depth with max(h, 0), which turns a planted NaN into 0, so
+    the non-finite state is made the way it can reach the stored depth: a uniform rain
+    whose depth over the step overflows float32 (plain float arithmetic, no fault)."""
     from rbsim import _lib
 
     L = _lib.lib()
     ny, nx, dx = 64, 96, 1.0
     z, h0, hu0, hv0, n, infil = _inputs(ny, nx, seed=5)
-    h0[10, 20] = float("nan")
     g, gu, gv = _pair(h0), _pair(hu0), _pair(hv0)
     f = _fields(ny, nx, dx, g, gu, gv, z, n, infil, [0, 0, 0, 0])
-    args = _lib.StepArgs(0.01, 0.0, 1.0, 0, 0)
+    args = _lib.StepArgs(10.0, 3.0e38, 1.0, 0, 0)
     stream = torch.cuda.current_stream().cuda_stream
     _lib.check(L.rb_hllc_step_noalloc(ctypes.byref(f), 0, ctypes.byref(args), None, stream))
     assert _read_noalloc_error() & _lib.RB_DEVERR_NONFINITE
