@@ -362,18 +362,11 @@ def _ensemble_members(n=256, seed=5):
     return out
 
 
-def ensemble_256(args):
-    """Config 4. Under torchrun each rank takes its share of the 256 domains (whole
-    domains, longest first onto the least-loaded rank); solves/s is all domains over
-    the slowest rank's time."""
-    from rbsim import replicas
-
-    horizon = 1800.0
-    rank, world = replicas.rank_world()
-    all_spec = _ensemble_members()
-    mine = replicas.shard_units([float(b.size) for b, _, _ in all_spec], world)[rank]
-    spec = [all_spec[i] for i in mine]
-    cells = sum(b.size for b, _, _ in spec)
+def _ensemble_vs_plain(spec, horizon: float) -> dict:
+    """``spec`` (bed, rain, Manning per domain) to ``horizon``: the plain per-domain loop,
+    then the batched ensemble from fresh states; wall times, steps and the digests."""
+    from rbsim.scheduler import MultiRateScheduler
+    from rbsim.schemes import local_inertial as li
 
     def fresh():
         sts = []
@@ -384,18 +377,17 @@ def ensemble_256(args):
         return sts
 
     # plain loop: each domain to the horizon through compute_dt + step, one after another
-    from rbsim.scheduler import MultiRateScheduler
-    from rbsim.schemes import local_inertial as li
-
     sts = fresh()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    plain_steps = 0
+    plain_steps = []
     for st, (_, rain, _) in zip(sts, spec, strict=True):
         sched = MultiRateScheduler(end_time=horizon, output_every=horizon)
+        k = 0
         for tick in sched.ticks(lambda st=st: li.compute_dt(st, 0.7, 30.0)):
             li.step(st, tick.dt, rain=rain)
-            plain_steps += 1
+            k += 1
+        plain_steps.append(k)
     torch.cuda.synchronize()
     plain_wall = time.perf_counter() - t0
     plain_h = [_digest(st.h) for st in sts]  # every member's final depth, as a digest
@@ -420,22 +412,80 @@ def ensemble_256(args):
     replays = ens.run_until(horizon)
     torch.cuda.synchronize()
     batched_wall = time.perf_counter() - t0
-    steps = sum(c.steps for c in ens.clock)
     same = sum(_digest(st.h) == d for st, d in zip(sts, plain_h, strict=True))
-    cell_updates = sum(c.steps * b.size for c, (b, _, _) in zip(ens.clock, spec, strict=True))
-    # whole job: every rank's domains over the slowest rank's time
-    job_rate, job_wall = replicas.whole_job_rate(float(len(spec)), batched_wall)
-    plain_rate, plain_job_wall = replicas.whole_job_rate(float(len(spec)), plain_wall)
-    return {
-        "workload": "ensemble_256", "metric": "ensemble solves/s", "n_gpus": world, "domains": len(all_spec),
-        "domains_this_rank": len(spec), "cells_this_rank": cells,
-        "batched": {"wall_s": job_wall, "solves_per_s": job_rate, "replays": replays,
-                    "tiles": {"li_variant": best[0]}, "autotune_ms_per_replay": {str(k): v for k, v in timings.items()},
-                    "gcell_per_s_this_rank": cell_updates / batched_wall / 1e9, "steps": steps},
-        "plain_loop": {"wall_s": plain_job_wall, "solves_per_s": plain_rate, "steps": plain_steps},
-        "speedup": plain_job_wall / job_wall, "domains_bitwise_equal_to_plain": f"{same} of {len(spec)}",
-        "all_domains_bitwise_equal_to_plain": same == len(spec),
-    }  # fmt: skip
+    steps = [c.steps for c in ens.clock]
+    cell_updates = sum(k * b.size for k, (b, _, _) in zip(steps, spec, strict=True))
+    del ens, sts
+    torch.cuda.empty_cache()
+    return {"batched_wall": batched_wall, "plain_wall": plain_wall, "replays": replays, "best": best,
+            "timings": timings, "steps": steps, "plain_steps": plain_steps, "same": same,
+            "cell_updates": cell_updates}  # fmt: skip
+
+
+def _host_step_overhead(samples: int = 300) -> float:
+    """Seconds the plain loop spends per step outside the kernel: compute_dt (a reduction
+    and a read-back) + step on a domain small enough that the kernels cost nothing."""
+    from rbsim.schemes import local_inertial as li
+
+    st = rbsim.State.from_bed(np.zeros((32, 32), np.float32), 10.0, depth=0.1, manning=0.03)
+    st.arm_source_compensation()
+    for _ in range(20):
+        li.step(st, li.compute_dt(st, 0.7, 30.0), rain=1e-5)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(samples):
+        li.step(st, li.compute_dt(st, 0.7, 30.0), rain=1e-5)
+    torch.cuda.synchronize()
+    return (time.perf_counter() - t0) / samples
+
+
+def ensemble_256(args):
+    """Config 4. Under torchrun each rank takes its share of the 256 domains (whole
+    domains, longest first onto the least-loaded rank); solves/s is all domains over
+    the slowest rank's time.
+
+    Also measured: the small-domain share (sides <= 512) on its own, and the bound on
+    batched / plain that the kernel rate allows. The batched run cannot step faster
+    than its kernel rate R (cell-updates/s), and the plain loop pays, per step, the
+    kernel time plus a host overhead t_host (the dt read-back and the launch), so
+    plain / batched <= sum_d steps_d (cells_d / R + t_host) / sum_d steps_d cells_d / R."""
+    from rbsim import replicas
+
+    horizon = 1800.0
+    rank, world = replicas.rank_world()
+    all_spec = _ensemble_members()
+    mine = replicas.shard_units([float(b.size) for b, _, _ in all_spec], world)[rank]
+    spec = [all_spec[i] for i in mine]
+    cells = sum(b.size for b, _, _ in spec)
+    t_host = _host_step_overhead()
+
+    def record(r, sub):
+        job_rate, job_wall = replicas.whole_job_rate(float(len(sub)), r["batched_wall"])
+        plain_rate, plain_job_wall = replicas.whole_job_rate(float(len(sub)), r["plain_wall"])
+        rate = r["cell_updates"] / r["batched_wall"]
+        work = sum(k * b.size for k, (b, _, _) in zip(r["plain_steps"], sub, strict=True))
+        bound = (work / rate + t_host * sum(r["plain_steps"])) / (work / rate)
+        return {
+            "domains": len(sub), "cells": sum(b.size for b, _, _ in sub),
+            "batched": {"wall_s": job_wall, "solves_per_s": job_rate, "replays": r["replays"],
+                        "tiles": {"li_variant": r["best"][0]},
+                        "autotune_ms_per_replay": {str(k): v for k, v in r["timings"].items()},
+                        "gcell_per_s_this_rank": rate / 1e9, "steps": sum(r["steps"])},
+            "plain_loop": {"wall_s": plain_job_wall, "solves_per_s": plain_rate, "steps": sum(r["plain_steps"])},
+            "speedup": plain_job_wall / job_wall,
+            "speedup_bound_at_this_kernel_rate": bound,
+            "domains_bitwise_equal_to_plain": f"{r['same']} of {len(sub)}",
+            "all_domains_bitwise_equal_to_plain": r["same"] == len(sub),
+        }  # fmt: skip
+
+    full = record(_ensemble_vs_plain(spec, horizon), spec)
+    small = [m for m in spec if m[0].shape[0] <= 512]
+    out = {"workload": "ensemble_256", "metric": "ensemble solves/s", "n_gpus": world, "domains": len(all_spec),
+           "domains_this_rank": len(spec), "cells_this_rank": cells, "host_overhead_per_plain_step_s": t_host,
+           **full}  # fmt: skip
+    if small:
+        out["small_domains_up_to_512"] = record(_ensemble_vs_plain(small, horizon), small)
+    return out
 
 
 def serve(args):
