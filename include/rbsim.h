@@ -46,6 +46,7 @@ extern "C" {
 #define RB_DEVERR_NONFINITE 1u /* a step produced a NaN/inf depth */
 #define RB_DEVERR_CLOCK 2u     /* the device clock produced a non-positive timestep */
 #define RB_DEVERR_STEPS 4u     /* the device clock hit its step budget before its target */
+#define RB_DEVERR_TIMEOUT 8u   /* a bounded device wait (a tensor-memory copy) gave up */
 
 /* Edge order of every per-edge array: north, south, east, west (state.py:35). */
 enum { RB_EDGE_NORTH = 0, RB_EDGE_SOUTH = 1, RB_EDGE_EAST = 2, RB_EDGE_WEST = 3 };

@@ -20,9 +20,14 @@
 // own faces. Stage 1 writes U1 = (h1, hu1, hv1) to workspace buffers; stage 2
 // reads U1 with the halo and U^n on the tile and writes U^{n+1} to the other
 // buffer of the caller's double-buffered (h, hu, hv).
+#include <cuda.h>  // CUtensorMap and its encoder's signature (reached through the runtime)
+
 #include <atomic>
 #include <cfloat>
+#include <cstring>
+#include <mutex>
 #include <type_traits>
+#include <unordered_map>
 
 #include "rb_common.cuh"
 #include "rb_kernels.h"
@@ -252,14 +257,62 @@ struct HllcSmemRecon : HllcSmem<TX, TY> {
   float4 ex[RXH * RXW], wx[RXH * RXW], ey[RYH * RYW], wy[RYH * RYW];
 };
 
-template <int TX, int TY, int FU>
+// LP = 2 stages interior tiles with tensor-memory-accelerator copies: one 2-D box per
+// field (h, hu, hv, z) of TY + 6 rows by TX + 8 columns starting at column x0 - 4 (a
+// multiple of 4, so the copy starts on a 16-byte boundary) and row y0 - 3, each into
+// its own 128-byte aligned landing area, completed on one shared-memory barrier.
+template <int TX, int TY>
+struct HllcSmemTma : HllcSmem<TX, TY> {
+  static constexpr int LW = TX + 8, LH = TY + 6;
+  static constexpr int LAND = (LW * LH + 31) / 32 * 32;  // floats per field, a multiple of 128 bytes
+  alignas(128) float land[4][LAND];
+  unsigned long long bar;
+};
+
+template <int TX, int TY, int FU, int LP>
 struct HllcSmemOf {
   using type = HllcSmem<TX, TY>;
 };
-template <int TX, int TY>
-struct HllcSmemOf<TX, TY, 0> {
+template <int TX, int TY, int LP>
+struct HllcSmemOf<TX, TY, 0, LP> {
   using type = HllcSmemRecon<TX, TY>;
 };
+template <int TX, int TY>
+struct HllcSmemOf<TX, TY, 1, 2> {
+  using type = HllcSmemTma<TX, TY>;
+};
+
+__device__ __forceinline__ unsigned smem_addr(const void* ptr) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(ptr));
+}
+
+// One 2-D tile copy global -> this CTA's shared memory, completing on `bar`. No
+// multicast: every copy reads this GPU's own memory into its own CTA.
+__device__ __forceinline__ void tma_load_tile(void* dst, const TileMap* map, int x, int y, unsigned long long* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
+          smem_addr(dst)),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(smem_addr(bar))
+      : "memory");
+}
+
+// Wait for phase `parity` of `bar` for at most `max_cycles` SM clocks; false if it gave up.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity, long long max_cycles) {
+  const long long t0 = clock64();
+  for (;;) {
+    unsigned done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if (clock64() - t0 > max_cycles) return false;
+  }
+}
+
+// A copy that has not landed after ~1 s at the B200's clock is treated as lost.
+constexpr long long kTmaWaitCycles = 2000000000LL;
 
 // One Heun stage of tile (bx, by) of domain p; ledger slot `slot`. Called by every
 // thread of the block; returns uniformly. FU selects the face phase: 1, each face
@@ -267,9 +320,11 @@ struct HllcSmemOf<TX, TY, 0> {
 // window that reconstructs each cell once; 0, every cell is reconstructed once per
 // direction into shared memory first, then each face reads its two sides. LP 1
 // issues a thread's halo loads before its divisions. Every choice computes the
-// same bits.
+// same bits. LP 2 stages tiles whose halo lies inside the domain with tensor-memory
+// copies from the tensor maps in `maps` (edge tiles take the LP 1 path).
 template <int TX, int TY, int NT, int STAGE, int FU = 1, int LP = 1, class SMEM = HllcSmem<TX, TY>>
-__device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, size_t slot, SMEM& S) {
+__device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, size_t slot, SMEM& S,
+                                          const HllcMaps* maps = nullptr) {
   static_assert(NT / 32 <= 32, "reduction scratch sized for <= 32 warps");
   using SM = HllcSmem<TX, TY>;
   constexpr int H = SM::H, RW = SM::RW, RH = SM::RH, XW = SM::XW, XH = SM::XH, YW = SM::YW, YH = SM::YH;
@@ -318,7 +373,53 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
   const float dx = p.dx32;
 
   // 1. stage the clamped halo and the primitives (hllc.py:262-282).
-  if constexpr (LP == 0) {
+  bool staged = false;
+  if constexpr (LP == 2) {
+    using ST = HllcSmemTma<TX, TY>;
+    constexpr int LW = ST::LW, LAND = ST::LAND;
+    constexpr unsigned kBytes = 4u * LW * ST::LH * sizeof(float);
+    const bool interior = x0 >= 4 && x0 + TX + 4 <= nx && y0 >= 3 && y0 + TY + 3 <= ny &&
+                          (smem_addr(&S.land[0][0]) & 127u) == 0;
+    if (interior) {
+      if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(&S.bar)), "r"(kBytes)
+                     : "memory");
+        const TileMap* mh = STAGE == 1 ? &maps->h[cur] : &maps->h1;
+        const TileMap* mu = STAGE == 1 ? &maps->hu[cur] : &maps->hu1;
+        const TileMap* mv = STAGE == 1 ? &maps->hv[cur] : &maps->hv1;
+        tma_load_tile(&S.land[0][0], mh, x0 - 4, y0 - H, &S.bar);
+        tma_load_tile(&S.land[1][0], mu, x0 - 4, y0 - H, &S.bar);
+        tma_load_tile(&S.land[2][0], mv, x0 - 4, y0 - H, &S.bar);
+        tma_load_tile(&S.land[3][0], &maps->z, x0 - 4, y0 - H, &S.bar);
+      }
+      // every thread waits for the copies, each for a bounded time; the block agrees
+      // on the outcome, so a copy that never lands flags an error and the whole block
+      // returns (after waiting, bounded again, for the copies it started)
+      const bool ok = mbar_wait_bounded(&S.bar, 0, kTmaWaitCycles);
+      if (__syncthreads_or(!ok)) {
+        if (threadIdx.x == 0) flag_error(p.err, RB_DEVERR_TIMEOUT);
+        mbar_wait_bounded(&S.bar, 0, kTmaWaitCycles);
+        return;
+      }
+      for (int k = threadIdx.x; k < RH * RW; k += NT) {
+        const int r = k / RW, c = k - r * RW;
+        const int l = r * LW + c + 1;  // the box starts one column left of the staged region
+        const float hh = S.land[0][l];
+        float u, v;
+        primitives(hh, S.land[1][l], S.land[2][l], u, v);
+        s_c[r][c] = make_float4(hh, u, v, S.land[3][l]);
+      }
+      static_assert(RH * LW <= LAND, "landing area too small");
+      staged = true;
+    }
+  }
+  if (staged) {
+  } else if constexpr (LP == 0) {
     for (int k = threadIdx.x; k < RH * RW; k += NT) {
       const int r = k / RW, c = k - r * RW;
       const int gi = min(max(y0 - H + r, 0), ny - 1), gj = min(max(x0 - H + c, 0), nx - 1);
@@ -813,7 +914,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
 template <int TX, int TY, int NT, int STAGE, int FU, int LP>
 __global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT) hllc_stage_kernel(const HllcParams p) {
   extern __shared__ __align__(16) unsigned char hllc_smem_raw[];
-  using SMEM = typename HllcSmemOf<TX, TY, FU>::type;
+  using SMEM = typename HllcSmemOf<TX, TY, FU, LP>::type;
   auto& S = *reinterpret_cast<SMEM*>(hllc_smem_raw);
   hllc_tile<TX, TY, NT, STAGE, FU, LP>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S);
 }
@@ -822,7 +923,7 @@ __global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT) hllc_stage_kerne
 // for an instantiation (setting it twice is harmless if threads race here).
 template <int TX, int TY, int NT, int FU, int LP>
 static void prepare_hllc() {
-  constexpr int smem = (int)sizeof(typename HllcSmemOf<TX, TY, FU>::type);
+  constexpr int smem = (int)sizeof(typename HllcSmemOf<TX, TY, FU, LP>::type);
   static std::atomic<unsigned long long> attr_set{0};
   int dev = 0;
   cudaGetDevice(&dev);
@@ -836,7 +937,7 @@ static void prepare_hllc() {
 
 template <int TX, int TY, int NT, int FU, int LP>
 static cudaError_t launch_hllc(const HllcParams& p, int stage, cudaStream_t s) {
-  constexpr size_t smem = sizeof(typename HllcSmemOf<TX, TY, FU>::type);
+  constexpr size_t smem = sizeof(typename HllcSmemOf<TX, TY, FU, LP>::type);
   static_assert(smem <= 227 * 1024, "tile does not fit in shared memory");
   prepare_hllc<TX, TY, NT, FU, LP>();
   const dim3 grid((p.nx + TX - 1) / TX, (p.ny + TY - 1) / TY);
@@ -844,6 +945,122 @@ static cudaError_t launch_hllc(const HllcParams& p, int stage, cudaStream_t s) {
     hllc_stage_kernel<TX, TY, NT, 1, FU, LP><<<grid, NT, smem, s>>>(p);
   else
     hllc_stage_kernel<TX, TY, NT, 2, FU, LP><<<grid, NT, smem, s>>>(p);
+  return cudaGetLastError();
+}
+
+// The TMA-staged stage kernel: interior tiles copy their halo with tensor-memory
+// copies from the tensor maps passed by value (grid constants).
+template <int TX, int TY, int NT, int STAGE>
+__global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT)
+    hllc_stage_tma_kernel(const HllcParams p, const __grid_constant__ HllcMaps maps) {
+  extern __shared__ __align__(1024) unsigned char hllc_tma_smem_raw[];
+  auto& S = *reinterpret_cast<HllcSmemTma<TX, TY>*>(hllc_tma_smem_raw);
+  hllc_tile<TX, TY, NT, STAGE, 1, 2>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S,
+                                     &maps);
+}
+
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// The driver's tensor-map encoder, reached through the runtime (the library links no
+// driver library); null if the driver does not offer it.
+static EncodeTiledFn tensor_map_encoder() {
+  static const EncodeTiledFn fn = []() -> EncodeTiledFn {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      return nullptr;
+    }
+    return reinterpret_cast<EncodeTiledFn>(f);
+  }();
+  return fn;
+}
+
+// The tensor map of one ny x nx float32 field for boxes of bw columns by bh rows.
+// Maps depend only on (address, shape, box), so they are kept in a small cache.
+static bool field_map(TileMap& out, const float* base, int ny, int nx, int bw, int bh) {
+  static_assert(sizeof(CUtensorMap) == sizeof(TileMap), "a tensor map is 128 bytes");
+  if (base == nullptr || (reinterpret_cast<uintptr_t>(base) & 15u) != 0 || nx % 4 != 0 || nx < bw || ny < bh)
+    return false;  // the copies need 16-byte aligned rows
+  struct Key {
+    const float* base;
+    int ny, nx, bw, bh;
+    bool operator==(const Key& o) const {
+      return base == o.base && ny == o.ny && nx == o.nx && bw == o.bw && bh == o.bh;
+    }
+  };
+  struct KeyHash {
+    size_t operator()(const Key& k) const {
+      return std::hash<const void*>()(k.base) ^ ((size_t)k.ny * 1000003u + (size_t)k.nx * 8191u + k.bw * 131u + k.bh);
+    }
+  };
+  static std::mutex mu;
+  static std::unordered_map<Key, TileMap, KeyHash> cache;
+  const Key key{base, ny, nx, bw, bh};
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+      out = it->second;
+      return true;
+    }
+  }
+  const EncodeTiledFn enc = tensor_map_encoder();
+  if (enc == nullptr) return false;
+  CUtensorMap m;
+  const cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)ny};
+  const cuuint64_t strides[1] = {(cuuint64_t)nx * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)bw, (cuuint32_t)bh};
+  const cuuint32_t elem[2] = {1, 1};
+  if (enc(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims, strides, box, elem,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  std::memcpy(&out, &m, sizeof m);
+  std::lock_guard<std::mutex> lock(mu);
+  if (cache.size() > 4096) cache.clear();
+  cache.emplace(key, out);
+  return true;
+}
+
+template <int TX, int TY, int NT>
+static void prepare_hllc_tma() {
+  constexpr int smem = (int)sizeof(HllcSmemTma<TX, TY>);
+  static std::atomic<unsigned long long> attr_set{0};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  const unsigned long long bit = 1ull << (dev & 63);
+  if (!(attr_set.load() & bit)) {
+    cudaFuncSetAttribute(hllc_stage_tma_kernel<TX, TY, NT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(hllc_stage_tma_kernel<TX, TY, NT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    attr_set.fetch_or(bit);
+  }
+}
+
+// Launch the TMA-staged kernel when every staged field can be mapped (16-byte aligned
+// rows, a grid at least one box large); otherwise the same tile with plain loads.
+template <int TX, int TY, int NT>
+static cudaError_t launch_hllc_tma(const HllcParams& p, int stage, cudaStream_t s) {
+  constexpr size_t smem = sizeof(HllcSmemTma<TX, TY>);
+  static_assert(smem <= 113 * 1024, "two blocks of the TMA-staged tile must fit an SM");
+  constexpr int BW = TX + 8, BH = TY + 6;
+  HllcMaps m;
+  bool ok = true;
+  for (int b = 0; b < 2 && ok; b++)
+    ok = field_map(m.h[b], p.hb[b], p.ny, p.nx, BW, BH) && field_map(m.hu[b], p.hub[b], p.ny, p.nx, BW, BH) &&
+         field_map(m.hv[b], p.hvb[b], p.ny, p.nx, BW, BH);
+  ok = ok && field_map(m.z, p.z, p.ny, p.nx, BW, BH) && field_map(m.h1, p.h1, p.ny, p.nx, BW, BH) &&
+       field_map(m.hu1, p.hu1, p.ny, p.nx, BW, BH) && field_map(m.hv1, p.hv1, p.ny, p.nx, BW, BH);
+  if (!ok) return launch_hllc<TX, TY, NT, 1, 1>(p, stage, s);
+  prepare_hllc_tma<TX, TY, NT>();
+  const dim3 grid((p.nx + TX - 1) / TX, (p.ny + TY - 1) / TY);
+  if (stage == 1)
+    hllc_stage_tma_kernel<TX, TY, NT, 1><<<grid, NT, smem, s>>>(p, m);
+  else
+    hllc_stage_tma_kernel<TX, TY, NT, 2><<<grid, NT, smem, s>>>(p, m);
   return cudaGetLastError();
 }
 
@@ -860,7 +1077,7 @@ struct HllcKernelVariant {
 static const HllcKernelVariant kHllcVariants[] = {
     {32, 16, 256, 1, 0}, {32, 16, 256, 1, 1}, {32, 16, 256, 3, 1},
     {32, 16, 256, 2, 1}, {32, 32, 512, 1, 1}, {64, 16, 512, 1, 1}, {32, 32, 640, 1, 1},
-    {32, 16, 512, 0, 1}, {32, 16, 384, 0, 1},
+    {32, 16, 512, 0, 1}, {32, 16, 384, 0, 1}, {32, 32, 640, 1, 2},
 };
 constexpr int kNumHllcVariants = (int)(sizeof(kHllcVariants) / sizeof(kHllcVariants[0]));
 constexpr int kDefaultHllcVariant = 6;
@@ -882,6 +1099,7 @@ void hllc_prepare_device() {
   prepare_hllc<32, 32, 640, 1, 1>();
   prepare_hllc<32, 16, 512, 0, 1>();
   prepare_hllc<32, 16, 384, 0, 1>();
+  prepare_hllc_tma<32, 32, 640>();
 #if !defined(RB_FAST_MATH)
   fast::hllc_prepare_device();
 #endif
@@ -914,6 +1132,7 @@ cudaError_t hllc_stage_launch_variant(const HllcParams& p, int stage, int varian
     case 4: return launch_hllc<32, 32, 512, 1, 1>(p, stage, s);
     case 7: return launch_hllc<32, 16, 512, 0, 1>(p, stage, s);
     case 8: return launch_hllc<32, 16, 384, 0, 1>(p, stage, s);
+    case 9: return launch_hllc_tma<32, 32, 640>(p, stage, s);
     default: return launch_hllc<32, 32, 640, 1, 1>(p, stage, s);
   }
 }

@@ -94,6 +94,16 @@ struct HllcParams {
   unsigned int *err;
 };
 
+// The tensor maps (CUtensorMap, 128 bytes each, held opaque here) of the fields the
+// TMA-staged HLLC stage kernel copies into shared memory: both buffers of h, hu, hv
+// (the clock picks one at run time), the bed and the stage-1 state.
+struct alignas(64) TileMap {
+  unsigned char bytes[128];
+};
+struct HllcMaps {
+  TileMap h[2], hu[2], hv[2], z, h1, hu1, hv1;
+};
+
 cudaError_t li_step_launch(const LiParams& p, cudaStream_t s);
 cudaError_t li_step_launch_variant(const LiParams& p, int variant, cudaStream_t s);
 int li_current_variant();

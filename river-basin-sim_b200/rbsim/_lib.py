@@ -22,6 +22,7 @@ RB_ERR_STEP = -5
 RB_DEVERR_NONFINITE = 1
 RB_DEVERR_CLOCK = 2
 RB_DEVERR_STEPS = 4
+RB_DEVERR_TIMEOUT = 8
 RB_ARITH_EXACT = 0
 RB_ARITH_FAST = 1
 
