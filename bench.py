@@ -15,20 +15,27 @@ here.
 * ``e2e``: the same metric through the public API from host memory: the bed and
   initial depth are copied in from pinned host buffers (State.from_bed), K steps
   run through DeviceClock, and the final depth is copied back to a pinned buffer,
-  all inside the timed region. ``e2e.per_step_api`` is
-  the same through the reference-shaped ``compute_dt`` / ``step`` loop, which reads
-  dt back to the host every step as the reference does.
+  all inside the timed region. ``e2e.per_step_api`` is the same through the
+  reference-shaped ``compute_dt`` / ``step`` loop, which reads dt back to the host
+  every step as the reference does.
 * ``roofline``: the step's kernels against the measured HBM copy bandwidth, from
-  algorithmic bytes (32 B per cell-step: read h, hu, hv, z, n; write h, hu, hv) and
-  per-launch durations: CUDA events on the launching stream around each stage
-  kernel of the same clocked steps, launched one by one right after the timed
-  replay (event nodes inside the timed graph would add their own cost to it).
-* ``cpu_baseline``: the CPU oracle (the reference's kernels restated in C,
-  OpenMP over the host cores) on a bounded band of the same workload.
+  algorithmic bytes (32 B per cell-step: read h, hu, hv, z, n; write h, hu, hv) over
+  the CUDA-event time of the timed replay itself (which also holds the one-thread
+  plan kernel of each step, so the figure is a lower bound for the stage pair);
+  ``launched_one_by_one`` times each stage kernel with events around single launches
+  as a cross-check.
+* ``cpu_baseline``: the CPU oracle (the reference's kernels restated in C, OpenMP
+  over the host cores, libm powf) on the full 2048 x 2048 grid for ~10 s.
+* ``err_vs_f64``: the device result after 12 steps against the float64 build of the
+  same kernels replaying the device's timesteps.
+* ``workloads``: the LI roofline point (2048^2 rain-on-grid, 40 B/cell-step) and the
+  largest single-GPU configuration (the 8192^2 valley reach, 72 B/cell-step), each
+  with its own roofline, CPU baseline and float64 error.
 
 Under torchrun each rank runs an independent replica of the workload on its own
 GPU (replicas only: the path has no exchange step), ``scaling`` = "weak".
-``--impl reference`` times the CPU oracle port of the reference path alone (rank 0).
+``--impl reference`` times the CPU oracle port of the reference path on the same
+2048 x 2048 grid, W warm-up steps then K timed steps (rank 0 alone).
 """
 
 from __future__ import annotations
@@ -358,6 +365,10 @@ def main(argv=None) -> int:
     legs = world == 1
     sub = {"li_rain_2048": bench_workloads.li_rain_2048(args, legs=legs),
            "li_reach_8192": bench_workloads.li_reach_8192(args, legs=legs)}  # fmt: skip
+    for rec in sub.values():  # whole job: every replica's cell-updates over the slowest replica's time
+        roof = rec["roofline"]
+        rec["value"], _ = replicas.whole_job_rate(roof["cell_updates"] / 1e9, roof["timed_s"])
+        rec["n_gpus"] = world
     err64 = bench_workloads.f64_leg(dambreak_spec(), steps=12) if legs else None
 
     if rank == 0:

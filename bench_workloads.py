@@ -175,6 +175,7 @@ def _kernel_roofline(state, scheme, steps, bytes_per_cell, injector=None, rain_r
         "kernel": "li_step_kernel", "kernel_ms_mean": kms, "bytes_per_cell_step": bytes_per_cell,
         "gcell_per_s_kernel": cells / (kms / 1e3) / 1e9,
         "gcell_per_s_step": cells * steps / (start.elapsed_time(stop) / 1e3) / 1e9,
+        "timed_s": start.elapsed_time(stop) / 1e3, "cell_updates": cells * steps,
     }  # fmt: skip
 
 
