@@ -67,7 +67,11 @@ NCU_DRAM_BYTES_PER_STEP = 253.0e6
 # (stage 1 84.7 %, stage 2 83.9 %).
 NCU_ISSUE_ACTIVE = (0.847, 0.839)
 WORKLOAD = "hllc_dambreak_2048x2048"
-BUILD = "exact: one IEEE rounding per operation, bit-identical to the oracle"
+BUILDS = {
+    "exact": "exact: one IEEE rounding per operation in the reference's order, bit-identical to the oracle",
+    "fast": "fast: contracted multiply-adds, approximate division / square root / powers; within 1e-5 relative "
+            "(L2) and 1e-4 m of the oracle on the same timesteps, every physics gate",
+}
 
 
 def dambreak_inputs(n: int = N):
@@ -97,6 +101,8 @@ class ClockSampler:
         self.lines: list[str] = []
 
     def __enter__(self):
+        if self.index < 0:  # sampling off
+            return self
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -264,6 +270,11 @@ def main(argv=None) -> int:
                     choices=["hllc_dambreak", "li_rain_512", "li_rain_2048", "hllc_lake_2048", "li_reach_8192",
                              "ensemble_256", "serve"],
                     help="hllc_dambreak is the headline; the others measure the remaining configurations")
+    ap.add_argument("--arith", default="fast", choices=["exact", "fast"],
+                    help="arithmetic of the step kernels for the headline (the other build is timed beside it)")
+    ap.add_argument("--headline-only", action="store_true",
+                    help="time the headline steps only (no e2e, other configurations, CPU or float64 legs)")
+    ap.add_argument("--no-legs", action="store_true", help="skip the CPU and float64 legs of a --workload record")
     ap.add_argument("--rates", default="2,10,50", help="serve: arrival rates, requests/s")
     ap.add_argument("--requests", type=int, default=16, help="serve: requests per rate")
     args = ap.parse_args(argv)
@@ -301,7 +312,7 @@ def main(argv=None) -> int:
     import ctypes
 
     import rbsim
-    from rbsim import _lib, graphs, replicas
+    from rbsim import _lib, arith, graphs, replicas
     from rbsim.device_clock import DeviceClock
     from rbsim.schemes import hllc
 
@@ -311,50 +322,64 @@ def main(argv=None) -> int:
     stream = torch.cuda.current_stream(dev)
     K = args.steps
 
-    # --- value: device-resident steps, one CUDA graph of K steps, inputs resident ---
-    st = rbsim.State.from_bed(z, DX, depth=depth, manning=0.0, device=dev)
-    hllc.arm_hllc(st)
-    clk = DeviceClock(st, "hllc_fv", alpha=ALPHA, dt_max=DT_MAX, sync_times=[T_END], graph_steps=K)
-    f = st.hllc_fields()
-    ws = st.workspace.data_ptr()
-    graph = graphs.capture(dev, lambda s: _lib.check(L.rb_hllc_enqueue_steps(ctypes.byref(f), K, 0, ws, s)))
-    for _ in range(args.warmup):  # W untimed warm-up steps
-        clk.set_target(T_END, 1)
-        _lib.check(L.rb_hllc_enqueue_steps(ctypes.byref(f), 1, 0, ws, stream.cuda_stream))
-    clk.set_target(T_END, K)
-    barrier()
-    start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local) as clocks:
-        start.record(stream)
-        graph.replay()
-        stop.record(stream)
+    def timed_replay(sample_clocks: bool):
+        """K device-resident steps, one CUDA graph, inputs resident, after W warm-up steps;
+        then the same clocked steps launched one by one with events around each stage."""
+        st = rbsim.State.from_bed(z, DX, depth=depth, manning=0.0, device=dev)
+        hllc.arm_hllc(st)
+        clk = DeviceClock(st, "hllc_fv", alpha=ALPHA, dt_max=DT_MAX, sync_times=[T_END], graph_steps=K)
+        f = st.hllc_fields()
+        ws = st.workspace.data_ptr()
+        graph = graphs.capture(dev, lambda s: _lib.check(L.rb_hllc_enqueue_steps(ctypes.byref(f), K, 0, ws, s)))
+        for _ in range(args.warmup):  # W untimed warm-up steps
+            clk.set_target(T_END, 1)
+            _lib.check(L.rb_hllc_enqueue_steps(ctypes.byref(f), 1, 0, ws, stream.cuda_stream))
+        clk.set_target(T_END, K)
         barrier()
-    ms = start.elapsed_time(stop)
-    cs = clk.read()
-    if cs.steps != args.warmup + K:
-        raise RuntimeError(f"device clock took {cs.steps} steps, expected {args.warmup + K}")
-    del graph
-    # Per-launch kernel durations, a cross-check of the roofline's timing: the same
-    # clocked steps launched one by one on the stream, CUDA events around each stage.
-    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(min(K, 50))]
-    clk.set_target(T_END, len(ev))
-    for e in ev:
-        _lib.check(L.rb_clock_plan(ws, stream.cuda_stream))
-        e[0].record(stream)
-        _lib.check(L.rb_hllc_stage_clocked(ctypes.byref(f), 1, ws, stream.cuda_stream))
-        e[1].record(stream)
-        _lib.check(L.rb_hllc_stage_clocked(ctypes.byref(f), 2, ws, stream.cuda_stream))
-        e[2].record(stream)
-    torch.cuda.synchronize(dev)
-    clk.read()
-    clk.close()
-    stage1_ms = [e[0].elapsed_time(e[1]) for e in ev]
-    stage2_ms = [e[1].elapsed_time(e[2]) for e in ev]
-    st.check_device_errors()
-    del st, clk
+        start, stop = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(local if sample_clocks else -1) as clocks:
+            start.record(stream)
+            graph.replay()
+            stop.record(stream)
+            barrier()
+        ms = start.elapsed_time(stop)
+        cs = clk.read()
+        if cs.steps != args.warmup + K:
+            raise RuntimeError(f"device clock took {cs.steps} steps, expected {args.warmup + K}")
+        del graph
+        ev = [[torch.cuda.Event(enable_timing=True) for _ in range(3)] for _ in range(min(K, 50))]
+        clk.set_target(T_END, len(ev))
+        for e in ev:
+            _lib.check(L.rb_clock_plan(ws, stream.cuda_stream))
+            e[0].record(stream)
+            _lib.check(L.rb_hllc_stage_clocked(ctypes.byref(f), 1, ws, stream.cuda_stream))
+            e[1].record(stream)
+            _lib.check(L.rb_hllc_stage_clocked(ctypes.byref(f), 2, ws, stream.cuda_stream))
+            e[2].record(stream)
+        torch.cuda.synchronize(dev)
+        clk.read()
+        clk.close()
+        st.check_device_errors()
+        return ms, clocks, [e[0].elapsed_time(e[1]) for e in ev], [e[1].elapsed_time(e[2]) for e in ev]
+
+    # --- value: the selected arithmetic; then the other build, for comparison ---
+    arith.set_arithmetic(args.arith)
+    ms, clocks, stage1_ms, stage2_ms = timed_replay(True)
     # Whole job: the cells every replica stepped over the slowest replica's time.
     value, sec = replicas.whole_job_rate(cells * K / 1e9, ms / 1e3)
     ms = sec * 1e3
+    other = "exact" if args.arith == "fast" else "fast"
+    arith.set_arithmetic(other)
+    ms_o, _, _, _ = timed_replay(False)
+    value_o, sec_o = replicas.whole_job_rate(cells * K / 1e9, ms_o / 1e3)
+    arith.set_arithmetic(args.arith)
+    if args.headline_only:
+        if rank == 0:
+            print(json.dumps({"metric": "Gcell-updates/s", "value": value, "ms_per_step": ms / K, "build": args.arith,
+                              "other_build": {"build": other, "value": value_o, "ms_per_step": sec_o * 1e3 / K}}))
+        if world > 1:
+            dist.destroy_process_group()
+        return 0
 
     e2e = _e2e(args, dev, barrier, z, depth)
 
@@ -383,7 +408,7 @@ def main(argv=None) -> int:
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "grid": [N, N], "dx_m": DX, "alpha": ALPHA, "scheme": "hllc_fv",
-                       "boundaries": "closed", "parallelism": f"replicas{world}", "build": BUILD,
+                       "boundaries": "closed", "parallelism": f"replicas{world}", "build": BUILDS[args.arith],
                        "l2": "inputs larger than L2: 11 float32 fields of 16.8 MB (h, hu, hv double-buffered, "
                              "stage-1 state, z, n) = 185 MB touched per step vs 126 MB L2",
                        "step_loop": "device-resident clock (dt, fill_span, rain gating on the GPU), K steps "
@@ -407,6 +432,7 @@ def main(argv=None) -> int:
                                                  "note": f"{len(stage1_ms)} clocked steps launched one by one with "
                                                          "events around each stage (launch gaps included)"}},
             "clocks": clocks.summary(),
+            "other_build": {"build": BUILDS[other], "value": value_o, "ms_per_step": sec_o * 1e3 / K},
             "e2e": e2e,
             "cpu_baseline": cpu_baseline() if legs else None,
             "err_vs_f64": err64,

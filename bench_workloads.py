@@ -528,8 +528,16 @@ def run(args):
         dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=torch.device("cuda", local))
     fn = {"li_rain_512": li_rain_512, "li_rain_2048": li_rain_2048, "hllc_lake_2048": hllc_lake_2048,
           "li_reach_8192": li_reach_8192, "ensemble_256": ensemble_256, "serve": serve}[args.workload]  # fmt: skip
+    from rbsim import arith
+
+    arith.set_arithmetic(args.arith)
     try:
-        return fn(args)
+        if args.workload in ("li_rain_2048", "li_reach_8192"):
+            out = fn(args, legs=not args.no_legs)
+        else:
+            out = fn(args)
+        out["build"] = args.arith
+        return out
     finally:
         if world > 1:
             import torch.distributed as dist

@@ -246,17 +246,6 @@ struct HllcSmem {
   float redf[32];
 };
 
-// The recon-once face phase (FU = 0) first reconstructs every cell its faces need,
-// once per direction, and keeps the values: along x the cells of rows y0-1..y0+TY,
-// cols x0-2..x0+TX+1, along y those of rows y0-2..y0+TY+1, cols x0-1..x0+TX; for
-// each, its east (+1/2) and west (-1/2) surface, bed, normal and transverse velocity.
-template <int TX, int TY>
-struct HllcSmemRecon : HllcSmem<TX, TY> {
-  static constexpr int RXW = TX + 4, RXH = TY + 2;
-  static constexpr int RYW = TX + 2, RYH = TY + 4;
-  float4 ex[RXH * RXW], wx[RXH * RXW], ey[RYH * RYW], wy[RYH * RYW];
-};
-
 // LP = 2 stages interior tiles with tensor-memory-accelerator copies: one 2-D box per
 // field (h, hu, hv, z) of TY + 6 rows by TX + 8 columns starting at column x0 - 4 (a
 // multiple of 4, so the copy starts on a 16-byte boundary) and row y0 - 3, each into
@@ -272,10 +261,6 @@ struct HllcSmemTma : HllcSmem<TX, TY> {
 template <int TX, int TY, int FU, int LP>
 struct HllcSmemOf {
   using type = HllcSmem<TX, TY>;
-};
-template <int TX, int TY, int LP>
-struct HllcSmemOf<TX, TY, 0, LP> {
-  using type = HllcSmemRecon<TX, TY>;
 };
 template <int TX, int TY>
 struct HllcSmemOf<TX, TY, 1, 2> {
@@ -317,10 +302,8 @@ constexpr long long kTmaWaitCycles = 2000000000LL;
 // One Heun stage of tile (bx, by) of domain p; ledger slot `slot`. Called by every
 // thread of the block; returns uniformly. FU selects the face phase: 1, each face
 // reconstructs its four-cell stencil; 2 or 3, FU faces per work item in a rolling
-// window that reconstructs each cell once; 0, every cell is reconstructed once per
-// direction into shared memory first, then each face reads its two sides. LP 1
-// issues a thread's halo loads before its divisions. Every choice computes the
-// same bits. LP 2 stages tiles whose halo lies inside the domain with tensor-memory
+// window that reconstructs each cell once. LP 1 issues a thread's halo loads before
+// its divisions. Every choice computes the same bits. LP 2 stages tiles whose halo lies inside the domain with tensor-memory
 // copies from the tensor maps in `maps` (edge tiles take the LP 1 path).
 template <int TX, int TY, int NT, int STAGE, int FU = 1, int LP = 1, class SMEM = HllcSmem<TX, TY>>
 __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, size_t slot, SMEM& S,
@@ -486,89 +469,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       if (a >= 1 && a <= TY) S.hmy[a - 1][b - 1] = h_r;
     }
   };
-  if constexpr (FU == 0) {
-    using SR = HllcSmemRecon<TX, TY>;
-    constexpr int RXW = SR::RXW, RYW = SR::RYW, NRX = SR::RXH * SR::RXW, NRY = SR::RYH * SR::RYW;
-    // (a) reconstruct: x-recon item (a, b) is the cell at row y0-1+a, col x0-2+b
-    // (staged at [a + 2][b + 1]); y-recon item (a, b) the cell at row y0-2+a, col
-    // x0-1+b (staged at [a + 1][b + 2]). A tile cell also keeps its face depths and
-    // bed slope for the update, as the face phase of FU = 1 does.
-    for (int k = threadIdx.x; k < NRX + NRY; k += NT) {
-      if (k < NRX) {
-        const int a = k / RXW, b = k - a * RXW;
-        const Rec r = recon(cell_x(s_c[a + 2][b]), cell_x(s_c[a + 2][b + 1]), cell_x(s_c[a + 2][b + 2]));
-        S.ex[k] = make_float4(r.eE, r.zE, r.nE, r.tE);
-        S.wx[k] = make_float4(r.eW, r.zW, r.nW, r.tW);
-        if (a >= 1 && a <= TY && b >= 2 && b <= TX + 1) {
-          S.hpx[a - 1][b - 2] = rmax(r.eE - r.zE, 0.0f);
-          S.hmx[a - 1][b - 2] = rmax(r.eW - r.zW, 0.0f);
-          S.szx[a - 1][b - 2] = r.sz;
-        }
-      } else {
-        const int ky = k - NRX;
-        const int a = ky / RYW, b = ky - a * RYW;
-        const Rec r = recon(cell_y(s_c[a][b + 2]), cell_y(s_c[a + 1][b + 2]), cell_y(s_c[a + 2][b + 2]));
-        S.ey[ky] = make_float4(r.eE, r.zE, r.nE, r.tE);
-        S.wy[ky] = make_float4(r.eW, r.zW, r.nW, r.tW);
-        if (a >= 2 && a <= TY + 1 && b >= 1 && b <= TX) {
-          S.hpy[a - 2][b - 1] = rmax(r.eE - r.zE, 0.0f);
-          S.hmy[a - 2][b - 1] = rmax(r.eW - r.zW, 0.0f);
-          S.szy[a - 2][b - 1] = r.sz;
-        }
-      }
-    }
-    __syncthreads();
-    // (b) faces: x-face (a, b) joins x-recon items (a, b) and (a, b + 1); y-face
-    // (a, b) joins y-recon items (a, b) and (a + 1, b)
-    constexpr int NXF = XH * XW, NF = XH * XW + YH * YW;
-    auto face_loop = [&](auto inner_tag) {
-      constexpr bool INNER = decltype(inner_tag)::value;
-      for (int k = threadIdx.x; k < NF; k += NT) {
-        float fh, fl, fr, ft, h_l, h_r;
-        if (k < NXF) {
-          const int a = k / XW, b = k - a * XW;
-          const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-          if (!INNER && (gi < 0 || gi >= ny || gj < 0 || gj > nx)) continue;
-          const int kind =
-              INNER ? RB_BC_OPEN : (gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN));
-          const float4 l = S.ex[a * RXW + b], r = S.wx[a * RXW + b + 1];
-          // the edge cell is column 0 (staged b + 2) or nx-1 (staged b + 1)
-          const Cell e = INNER ? Cell{} : cell_x(s_c[a + 2][gj == 0 ? b + 2 : b + 1]);
-          any_face_flux(FaceSides{l.x, l.y, l.z, l.w, r.x, r.y, r.z, r.w}, kind, gj == 0, e,
-                        gj == 0 ? stage_w : stage_e, fh, fl, fr, ft, h_l, h_r);
-          s_fxh[a][b] = fh;
-          if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
-            s_fxl[a - 1][b - 1] = fl;
-            s_fxr[a - 1][b - 1] = fr;
-            s_fxt[a - 1][b - 1] = ft;
-          }
-        } else {
-          const int ky = k - NXF;
-          const int a = ky / YW, b = ky - a * YW;
-          const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-          if (!INNER && (gj < 0 || gj >= nx || gi < 0 || gi > ny)) continue;
-          const int kind =
-              INNER ? RB_BC_OPEN : (gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN));
-          const float4 l = S.ey[a * RYW + b], r = S.wy[(a + 1) * RYW + b];
-          // the edge cell is row 0 (staged a + 2) or ny-1 (staged a + 1)
-          const Cell e = INNER ? Cell{} : cell_y(s_c[gi == 0 ? a + 2 : a + 1][b + 2]);
-          any_face_flux(FaceSides{l.x, l.y, l.z, l.w, r.x, r.y, r.z, r.w}, kind, gi == 0, e,
-                        gi == 0 ? stage_n : stage_s, fh, fl, fr, ft, h_l, h_r);
-          s_fyh[a][b] = fh;
-          if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
-            s_fyl[a - 1][b - 1] = fl;
-            s_fyr[a - 1][b - 1] = fr;
-            s_fyt[a - 1][b - 1] = ft;
-          }
-        }
-      }
-    };
-    const bool inner = x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= nx && y0 + TY + 2 <= ny;
-    if (inner)
-      face_loop(std::true_type{});
-    else
-      face_loop(std::false_type{});
-  } else if constexpr (FU == 1) {
+  if constexpr (FU == 1) {
     // One face per work item: four cells along the normal. x- and y-faces share
     // one loop, so the last pass over the block is partly filled once, not twice.
     // A tile whose faces (and the ring's) are all inner faces of the domain runs an
@@ -1077,7 +978,7 @@ struct HllcKernelVariant {
 static const HllcKernelVariant kHllcVariants[] = {
     {32, 16, 256, 1, 0}, {32, 16, 256, 1, 1}, {32, 16, 256, 3, 1},
     {32, 16, 256, 2, 1}, {32, 32, 512, 1, 1}, {64, 16, 512, 1, 1}, {32, 32, 640, 1, 1},
-    {32, 16, 512, 0, 1}, {32, 16, 384, 0, 1}, {32, 32, 640, 1, 2},
+    {32, 32, 640, 1, 2},
 };
 constexpr int kNumHllcVariants = (int)(sizeof(kHllcVariants) / sizeof(kHllcVariants[0]));
 constexpr int kDefaultHllcVariant = 6;
@@ -1097,8 +998,6 @@ void hllc_prepare_device() {
   prepare_hllc<32, 32, 512, 1, 1>();
   prepare_hllc<64, 16, 512, 1, 1>();
   prepare_hllc<32, 32, 640, 1, 1>();
-  prepare_hllc<32, 16, 512, 0, 1>();
-  prepare_hllc<32, 16, 384, 0, 1>();
   prepare_hllc_tma<32, 32, 640>();
 #if !defined(RB_FAST_MATH)
   fast::hllc_prepare_device();
@@ -1130,9 +1029,7 @@ cudaError_t hllc_stage_launch_variant(const HllcParams& p, int stage, int varian
     case 5: return launch_hllc<64, 16, 512, 1, 1>(p, stage, s);
     case 0: return launch_hllc<32, 16, 256, 1, 0>(p, stage, s);
     case 4: return launch_hllc<32, 32, 512, 1, 1>(p, stage, s);
-    case 7: return launch_hllc<32, 16, 512, 0, 1>(p, stage, s);
-    case 8: return launch_hllc<32, 16, 384, 0, 1>(p, stage, s);
-    case 9: return launch_hllc_tma<32, 32, 640>(p, stage, s);
+    case 7: return launch_hllc_tma<32, 32, 640>(p, stage, s);
     default: return launch_hllc<32, 32, 640, 1, 1>(p, stage, s);
   }
 }
