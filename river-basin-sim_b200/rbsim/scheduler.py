@@ -4,16 +4,22 @@ The fast scheme proposes a state-derived ``dt_raw``; the clock only ever shorten
 it, filling the span to the next sync point with ``ceil(span / dt_raw)`` equal
 steps (``fill_span``). Sync points are output times, forcing breakpoints,
 slow-process activations and the end time. A slow process is handed the exact
-elapsed simulated time since it last ran. All arithmetic is host float64, in the
-same order as the reference, so a device-side replay (``rbsim.device_clock``)
-reproduces the step sequence bit for bit.
+elapsed simulated time since it last ran.
+
+The sync points are kept sorted, so the next one is a bisection (the device clock,
+``rbsim.device_clock``, walks the same sorted list with a cursor); each slow
+process's pending activations are a queue that a step drains. Every comparison and
+every float64 operation is the reference's, in its order, so the host loop and the
+device replay take the same steps bit for bit.
 """
 
 from __future__ import annotations
 
 import math
+from bisect import bisect_right
+from collections import deque
 from collections.abc import Callable, Iterable, Iterator, Sequence
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 
 EPS_T = 1e-6  # simulated-seconds tolerance for "lands on"
 
@@ -26,7 +32,7 @@ def fill_span(span: float, dt_raw: float) -> float:
         return span
     n = math.ceil(span / dt_raw)
     dt = span / n
-    # an ulp over dt_raw can happen when span/dt_raw sits just above an integer
+    # span / n can land an ulp above dt_raw when span / dt_raw sits just above an integer
     return span / (n + 1) if dt > dt_raw else dt
 
 
@@ -57,24 +63,39 @@ class Tick:
     due: tuple[tuple[SlowProcess, float], ...] = ()
 
 
-@dataclass
-class MultiRateScheduler:
-    end_time: float
-    output_every: float
-    events: Sequence[float] = ()
-    processes: Sequence[SlowProcess] = ()
-    _sync: list[float] = field(init=False, repr=False)
+class _Due:
+    """One slow process's activations still ahead, and when it last ran."""
 
-    def __post_init__(self) -> None:
-        if self.end_time <= 0:
-            raise ValueError(f"end_time must be > 0, got {self.end_time}")
-        if self.output_every <= 0:
-            raise ValueError(f"output_every must be > 0, got {self.output_every}")
-        sync = [*self.output_times, *self.events]
-        for proc in self.processes:
-            sync += proc.activations(self.end_time)
-        sync.append(self.end_time)
-        self._sync = sync
+    def __init__(self, proc: SlowProcess, end_time: float):
+        self.proc = proc
+        self.queue = deque(proc.activations(end_time))
+        self.last = 0.0
+
+    def fire(self, t1: float) -> float | None:
+        """Drain the activations a step ending at ``t1`` reached; the elapsed time if any."""
+        if not self.queue or t1 < self.queue[0] - EPS_T:
+            return None
+        while self.queue and t1 >= self.queue[0] - EPS_T:
+            self.queue.popleft()
+        elapsed, self.last = t1 - self.last, t1
+        return elapsed
+
+
+class MultiRateScheduler:
+    def __init__(self, end_time: float, output_every: float, events: Sequence[float] = (),
+                 processes: Sequence[SlowProcess] = ()):  # fmt: skip
+        if end_time <= 0:
+            raise ValueError(f"end_time must be > 0, got {end_time}")
+        if output_every <= 0:
+            raise ValueError(f"output_every must be > 0, got {output_every}")
+        self.end_time = end_time
+        self.output_every = output_every
+        self.events = tuple(events)
+        self.processes = tuple(processes)
+        points = [*self.output_times, *self.events, *(t for p in self.processes for t in p.activations(end_time)),
+                  end_time]  # fmt: skip
+        self._points = points  # as given: the device clock sorts its own copy
+        self._sorted = sorted(points)
 
     @property
     def n_frames(self) -> int:
@@ -86,16 +107,16 @@ class MultiRateScheduler:
 
     @property
     def sync_times(self) -> list[float]:
-        return list(self._sync)
+        return list(self._points)
 
     def next_sync(self, t: float) -> float:
-        later = [s for s in self._sync if s > t + EPS_T]
-        return min(later) if later else math.inf
+        """The first sync point strictly after ``t + EPS_T`` (infinity past the last)."""
+        k = bisect_right(self._sorted, t + EPS_T)
+        return self._sorted[k] if k < len(self._sorted) else math.inf
 
     def ticks(self, dt_fn: Callable[[], float]) -> Iterator[Tick]:
         """One Tick per fast step until ``end_time``; ``dt_fn`` is the scheme's CFL dt."""
-        pending = {p.name: (p, p.activations(self.end_time)) for p in self.processes}
-        last_ran = {name: 0.0 for name in pending}
+        dues = [_Due(p, self.end_time) for p in self.processes]
         next_output = self.output_every
         t, index = 0.0, 0
         while t < self.end_time - EPS_T:
@@ -109,18 +130,9 @@ class MultiRateScheduler:
             is_output = t1 >= next_output - EPS_T and next_output <= self.end_time + EPS_T
             if is_output:
                 next_output += self.output_every
-            due = []
-            for name, (proc, times) in pending.items():
-                fired = False
-                while times and t1 >= times[0] - EPS_T:
-                    times.pop(0)
-                    fired = True
-                if fired:
-                    due.append((proc, t1 - last_ran[name]))
-                    last_ran[name] = t1
-            yield Tick(index=index, t0=t, dt=dt, t1=t1, is_output=is_output, due=tuple(due))
-            t = t1
-            index += 1
+            due = tuple((d.proc, e) for d in dues if (e := d.fire(t1)) is not None)
+            yield Tick(index=index, t0=t, dt=dt, t1=t1, is_output=is_output, due=due)
+            t, index = t1, index + 1
 
 
 def merge_events(*groups: Iterable[float]) -> list[float]:
