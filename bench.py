@@ -61,11 +61,12 @@ DT_MAX = 30.0
 T_END = 30.0  # simulated horizon of the dam-break configuration
 BYTES_PER_CELL_STEP = 32  # read h, hu, hv, z, n (20 B) + write h, hu, hv (12 B)
 # DRAM bytes (read + write) of one step's two stage launches in one ncu capture of this
-# workload (--set full, 2048^2 dam break, stage 1 + stage 2): 88.4 MB + 164.7 MB.
-NCU_DRAM_BYTES_PER_STEP = 253.0e6
+# workload (--set full, 2048^2 dam break, fast build, stage 1 + stage 2): 87.2 MB +
+# 165.5 MB (the exact build: 88.3 + 163.5 MB).
+NCU_DRAM_BYTES_PER_STEP = 252.7e6
 # The stage kernels are issue-bound: share of issue slots busy in the same capture
-# (stage 1 84.7 %, stage 2 83.9 %).
-NCU_ISSUE_ACTIVE = (0.847, 0.839)
+# (fast build: stage 1 83.4 %, stage 2 82.4 %; exact: 84.8 %, 84.3 %).
+NCU_ISSUE_ACTIVE = (0.834, 0.824)
 WORKLOAD = "hllc_dambreak_2048x2048"
 BUILDS = {
     "exact": "exact: one IEEE rounding per operation in the reference's order, bit-identical to the oracle",

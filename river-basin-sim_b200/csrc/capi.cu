@@ -77,11 +77,9 @@ int check_dt(double dt, const char* who) {
 
 
 size_t ws_ledger_bytes(int ny, int nx) {
-  // one slot per tile of whichever tiling has the most tiles: the smallest tile any
-  // variant uses (32 x 8), or the 28-wide one (28 x 28), which has more on thin grids
-  const size_t t8 = (size_t)((nx + 31) / 32) * (size_t)((ny + 7) / 8);
-  const size_t t28 = (size_t)((nx + 27) / 28) * (size_t)((ny + 27) / 28);
-  return align256((t8 > t28 ? t8 : t28) * 2 * sizeof(double));
+  // one slot per tile of the smallest tile any kernel variant uses (32 x 8)
+  const size_t t = (size_t)((nx + 31) / 32) * (size_t)((ny + 7) / 8);
+  return align256(t * 2 * sizeof(double));
 }
 size_t ws_li_bytes(int ny, int nx) { return WS_LEDGER + ws_ledger_bytes(ny, nx); }
 size_t ws_hllc_u1_offset(int ny, int nx) { return WS_LEDGER + ws_ledger_bytes(ny, nx); }

@@ -225,9 +225,7 @@ __device__ __forceinline__ void any_face_flux(const Rec& L, const Rec& R, int ki
   any_face_flux(sides(L, R), kind, low, e, stage, fh, fl, fr, ft, h_l_out, h_r_out);
 }
 
-// CW is the row pitch of the staged cells: RW, or RW + 1 where a warp walks a column
-// of them (an odd pitch in 16-byte words keeps its vector loads free of bank conflicts).
-template <int TX, int TY, int CW = TX + 6>
+template <int TX, int TY>
 struct HllcSmem {
   static constexpr int H = 3;                     // halo
   static constexpr int RW = TX + 2 * H, RH = TY + 2 * H;
@@ -236,7 +234,7 @@ struct HllcSmem {
   static constexpr int BW = TX + 2, BH = TY + 2;  // beta on the tile + ring
   // the staged cells (h, u, v, z) as one 16-byte word each: a face reads its four
   // stencil cells with four vector loads
-  float4 c[RH][CW];
+  float4 c[RH][RW];
   float fxh[XH][XW], fyh[YH][YW];
   float fxl[TY][TX + 1], fxr[TY][TX + 1], fxt[TY][TX + 1];  // tile x-faces
   float fyl[TY + 1][TX], fyr[TY + 1][TX], fyt[TY + 1][TX];  // tile y-faces
@@ -263,10 +261,6 @@ struct HllcSmemTma : HllcSmem<TX, TY> {
 template <int TX, int TY, int FU, int LP>
 struct HllcSmemOf {
   using type = HllcSmem<TX, TY>;
-};
-template <int TX, int TY, int LP>
-struct HllcSmemOf<TX, TY, 4, LP> {
-  using type = HllcSmem<TX, TY, TX + 7>;
 };
 template <int TX, int TY>
 struct HllcSmemOf<TX, TY, 1, 2> {
@@ -475,75 +469,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       if (a >= 1 && a <= TY) S.hmy[a - 1][b - 1] = h_r;
     }
   };
-  if constexpr (FU == 4) {
-    // A warp per row of x-faces or column of y-faces: lane j reconstructs cell j of the
-    // row (column) once, and face j joins lane j's east values with lane j + 1's west
-    // values, passed by a shuffle. A row of the 28-wide tile has 31 faces over 32 cells,
-    // so every lane but the last has a face. Tile cells keep their face depths and bed
-    // slope for the update, as in FU = 1.
-    static_assert(XW == 31 && YH == 31, "the warp-row face phase needs 28 x 28 tiles");
-    constexpr unsigned FULL = 0xffffffffu;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const bool inner = x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= nx && y0 + TY + 2 <= ny;
-    for (int task = warp; task < XH + YW; task += NT / 32) {
-      float fh, fl, fr, ft, h_l, h_r;
-      if (task < XH) {  // x-faces of row a: lane j is the cell at column x0-2+j (staged j+1)
-        const int a = task, r = a + 2;
-        const Rec me = recon(cell_x(s_c[r][lane]), cell_x(s_c[r][lane + 1]), cell_x(s_c[r][lane + 2]));
-        const FaceSides F{me.eE, me.zE, me.nE, me.tE, __shfl_down_sync(FULL, me.eW, 1),
-                          __shfl_down_sync(FULL, me.zW, 1), __shfl_down_sync(FULL, me.nW, 1),
-                          __shfl_down_sync(FULL, me.tW, 1)};
-        if (a >= 1 && a <= TY && lane >= 2 && lane <= TX + 1) {
-          S.hpx[a - 1][lane - 2] = rmax(me.eE - me.zE, 0.0f);
-          S.hmx[a - 1][lane - 2] = rmax(me.eW - me.zW, 0.0f);
-          S.szx[a - 1][lane - 2] = me.sz;
-        }
-        const int b = lane, gi = y0 - 1 + a, gj = x0 - 1 + b;
-        if (b >= XW || (!inner && (gi < 0 || gi >= ny || gj < 0 || gj > nx))) continue;
-        if (inner) {
-          any_face_flux(F, RB_BC_OPEN, false, Cell{}, 0.0f, fh, fl, fr, ft, h_l, h_r);
-        } else {
-          const int kind = gj == 0 ? p.bc[RB_EDGE_WEST] : (gj == nx ? p.bc[RB_EDGE_EAST] : RB_BC_OPEN);
-          // the edge cell: column 0 (the right cell, staged b + 2) or nx-1 (the left, b + 1)
-          any_face_flux(F, kind, gj == 0, cell_x(s_c[r][gj == 0 ? b + 2 : b + 1]), gj == 0 ? stage_w : stage_e,
-                        fh, fl, fr, ft, h_l, h_r);
-        }
-        s_fxh[a][b] = fh;
-        if (a >= 1 && a <= TY && b >= 1 && b <= TX + 1) {
-          s_fxl[a - 1][b - 1] = fl;
-          s_fxr[a - 1][b - 1] = fr;
-          s_fxt[a - 1][b - 1] = ft;
-        }
-      } else {  // y-faces of column b: lane j is the cell at row y0-2+j (staged j+1)
-        const int b = task - XH, c = b + 2;
-        const Rec me = recon(cell_y(s_c[lane][c]), cell_y(s_c[lane + 1][c]), cell_y(s_c[lane + 2][c]));
-        const FaceSides F{me.eE, me.zE, me.nE, me.tE, __shfl_down_sync(FULL, me.eW, 1),
-                          __shfl_down_sync(FULL, me.zW, 1), __shfl_down_sync(FULL, me.nW, 1),
-                          __shfl_down_sync(FULL, me.tW, 1)};
-        if (b >= 1 && b <= TX && lane >= 2 && lane <= TY + 1) {
-          S.hpy[lane - 2][b - 1] = rmax(me.eE - me.zE, 0.0f);
-          S.hmy[lane - 2][b - 1] = rmax(me.eW - me.zW, 0.0f);
-          S.szy[lane - 2][b - 1] = me.sz;
-        }
-        const int a = lane, gi = y0 - 1 + a, gj = x0 - 1 + b;
-        if (a >= YH || (!inner && (gj < 0 || gj >= nx || gi < 0 || gi > ny))) continue;
-        if (inner) {
-          any_face_flux(F, RB_BC_OPEN, false, Cell{}, 0.0f, fh, fl, fr, ft, h_l, h_r);
-        } else {
-          const int kind = gi == 0 ? p.bc[RB_EDGE_NORTH] : (gi == ny ? p.bc[RB_EDGE_SOUTH] : RB_BC_OPEN);
-          // the edge cell: row 0 (the lower cell, staged a + 2) or ny-1 (the upper, a + 1)
-          any_face_flux(F, kind, gi == 0, cell_y(s_c[gi == 0 ? a + 2 : a + 1][c]), gi == 0 ? stage_n : stage_s,
-                        fh, fl, fr, ft, h_l, h_r);
-        }
-        s_fyh[a][b] = fh;
-        if (a >= 1 && a <= TY + 1 && b >= 1 && b <= TX) {
-          s_fyl[a - 1][b - 1] = fl;
-          s_fyr[a - 1][b - 1] = fr;
-          s_fyt[a - 1][b - 1] = ft;
-        }
-      }
-    }
-  } else if constexpr (FU == 1) {
+  if constexpr (FU == 1) {
     // One face per work item: four cells along the normal. x- and y-faces share
     // one loop, so the last pass over the block is partly filled once, not twice.
     // A tile whose faces (and the ring's) are all inner faces of the domain runs an
@@ -1052,7 +978,7 @@ struct HllcKernelVariant {
 static const HllcKernelVariant kHllcVariants[] = {
     {32, 16, 256, 1, 0}, {32, 16, 256, 1, 1}, {32, 16, 256, 3, 1},
     {32, 16, 256, 2, 1}, {32, 32, 512, 1, 1}, {64, 16, 512, 1, 1}, {32, 32, 640, 1, 1},
-    {32, 32, 640, 1, 2}, {28, 28, 640, 4, 1},
+    {32, 32, 640, 1, 2},
 };
 constexpr int kNumHllcVariants = (int)(sizeof(kHllcVariants) / sizeof(kHllcVariants[0]));
 constexpr int kDefaultHllcVariant = 6;
@@ -1073,7 +999,6 @@ void hllc_prepare_device() {
   prepare_hllc<64, 16, 512, 1, 1>();
   prepare_hllc<32, 32, 640, 1, 1>();
   prepare_hllc_tma<32, 32, 640>();
-  prepare_hllc<28, 28, 640, 4, 1>();
 #if !defined(RB_FAST_MATH)
   fast::hllc_prepare_device();
 #endif
@@ -1105,14 +1030,13 @@ cudaError_t hllc_stage_launch_variant(const HllcParams& p, int stage, int varian
     case 0: return launch_hllc<32, 16, 256, 1, 0>(p, stage, s);
     case 4: return launch_hllc<32, 32, 512, 1, 1>(p, stage, s);
     case 7: return launch_hllc_tma<32, 32, 640>(p, stage, s);
-    case 8: return launch_hllc<28, 28, 640, 4, 1>(p, stage, s);
     default: return launch_hllc<32, 32, 640, 1, 1>(p, stage, s);
   }
 }
 
 #if !defined(RB_FAST_MATH)
-// Tiles of the current variant (one ledger slot each); never more than the workspace
-// ledger holds (one slot per tile of the 32 x 8 or the 28 x 28 tiling, the larger).
+// Tiles of the current variant (one ledger slot each); never more than the 32 x 8
+// tiling the workspace ledger is sized for.
 int hllc_tiles(int ny, int nx) { return hllc_tiles_of(g_hllc_variant.load(), ny, nx); }
 
 int hllc_tiles_of(int variant, int ny, int nx) {
