@@ -534,13 +534,15 @@ def run(args):
           "li_reach_8192": li_reach_8192, "ensemble_256": ensemble_256, "serve": serve}[args.workload]  # fmt: skip
     from rbsim import arith
 
-    arith.set_arithmetic(args.arith)
+    # ensembles run the exact arithmetic, so their plain-loop comparisons do too
+    mode = "exact" if args.workload in ("ensemble_256", "serve") else args.arith
+    arith.set_arithmetic(mode)
     try:
         if args.workload in ("li_rain_2048", "li_reach_8192"):
             out = fn(args, legs=not args.no_legs)
         else:
             out = fn(args)
-        out["build"] = args.arith
+        out["build"] = mode
         return out
     finally:
         if world > 1:
