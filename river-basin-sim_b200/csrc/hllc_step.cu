@@ -69,8 +69,12 @@ __device__ __forceinline__ void hllc_flux(float hl, float ul, float vtl, float h
     sr = ul + 2.0f * cl;
   } else {
     const float hs = 0.5f * (cl + cr) + 0.25f * (ul - ur);
+#if defined(RB_FAST_MATH)
+    const float c_star = fabsf(hs);  // sqrt(g * max(hs * hs / g, 0)) = |hs|
+#else
     const float h_star = rmax(div_g(hs * hs), 0.0f);  // hs * hs / g
     const float c_star = sqrtf(g * h_star);
+#endif
     const float u_star = 0.5f * (ul + ur) + cl - cr;
     sl = rmin(ul - cl, u_star - c_star);
     sr = rmax(ur + cr, u_star + c_star);
