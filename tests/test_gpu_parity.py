@@ -196,11 +196,13 @@ def _hllc_variants():
     return n.value
 
 
-@pytest.mark.parametrize("shape", [(301, 419), (5, 2), (1, 600)])
+@pytest.mark.parametrize("shape", [(301, 419), (300, 420), (5, 2), (1, 600)])
 def test_every_hllc_kernel_variant_matches_oracle_bitwise(shape):
-    """The stage kernel's variants (tile shape, block size, faces per thread, load batching)
-    are a speed choice only: each reproduces the oracle exactly, on a ragged grid with
-    open and fixed_stage edges and on degenerate shapes."""
+    """The stage kernel's variants (tile shape, block size, faces per thread, load batching,
+    tensor-memory staging) are a speed choice only: each reproduces the oracle exactly, on
+    ragged grids with open and fixed_stage edges and on degenerate shapes. 300 x 420 has
+    16-byte rows, so the TMA-staged variant copies its interior tiles with tensor copies
+    (the other shapes take its plain-load fallback)."""
     from gpu_api import GpuAPI
     from rbsim import _lib
 
