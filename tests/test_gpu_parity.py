@@ -257,3 +257,23 @@ def test_li_reach_8192_matches_oracle_bitwise():
                               dz_lo=np.full((n, n), -np.inf, np.float32), dz_hi=np.full((n, n), np.inf, np.float32)),
                 steps=2, alpha=0.7, dt_max=30.0)  # fmt: skip
     _compare(run_case(case, GpuAPI()), _oracle_outputs(case), "reach8192")
+
+
+def test_li_reach_band_long_run_matches_oracle_bitwise():
+    """A 512 x 8192 band of the 8192 x 8192 reach (the meandering channel and all eight
+    inflow cells, infiltration, lognormal roughness, bedload, the open downstream edge)
+    for 200 steps with an Exner activation every 50: the long-run complement of the
+    two full-size steps above, bit for bit against the oracle."""
+    from bench_workloads import reach_band_spec, reach_inputs
+    from gpu_api import GpuAPI
+
+    z, manning, infil, inflows, depth = reach_inputs(8192, 5.0)
+    spec = reach_band_spec(z, manning, infil, inflows, depth, rows=512)
+    rows, n = spec["bed"].shape
+    case = dict(scheme="local_inertial", bed=spec["bed"], dx=5.0, depth=spec["depth"], manning=spec["manning"],
+                infil=spec["infil"], inflows=spec["inflows"], boundaries={"east": "open"},
+                sediment=dict(d50=np.full((rows, n), 0.002, np.float32), porosity=0.4, every=50,
+                              dz_lo=np.full((rows, n), -np.inf, np.float32),
+                              dz_hi=np.full((rows, n), np.inf, np.float32)),
+                steps=200, alpha=0.7, dt_max=30.0)  # fmt: skip
+    _compare(run_case(case, GpuAPI()), _oracle_outputs(case), "reach_band_200")
