@@ -513,6 +513,18 @@ def serve(args):
         out["rates"][str(rate)] = {"batched": srv.stats, "serial": serial,
                                    "throughput_ratio": srv.stats["solves_per_s"] / serial["solves_per_s"]}  # fmt: skip
         torch.cuda.empty_cache()
+    # the small-request share on its own: sides 256-512, where the serial loop is launch-bound
+    reqs = poisson_stream(50.0, 2 * args.requests, seed=4242, side_lo=256, side_hi=512)
+    with tempfile.TemporaryDirectory() as tmp:
+        for r in reqs:
+            r.output_every = 600.0
+        srv = Server(hbm_budget=150e9, graph_steps=16, out_dir=f"{tmp}/batched")
+        srv.run(reqs)
+        torch.cuda.empty_cache()
+        serial = serial_baseline(reqs, out_dir=f"{tmp}/serial")
+    out["small_requests_256_512_at_50_per_s"] = {
+        "batched": srv.stats, "serial": serial,
+        "throughput_ratio": srv.stats["solves_per_s"] / serial["solves_per_s"]}  # fmt: skip
     return out
 
 
