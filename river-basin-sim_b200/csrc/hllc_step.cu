@@ -111,6 +111,15 @@ __device__ __forceinline__ void hllc_flux(float hl, float ul, float vtl, float h
 // one. Still water (hu = hv = 0) is common, and its quotients are the zero momenta
 // themselves, so such cells branch around both divisions (a zero dividend would take
 // the division's slow path); a cell with one zero momentum divides 1 in its place.
+#if defined(RB_FAST_MATH)
+// Fast arithmetic: one approximate reciprocal per wet cell.
+__device__ __forceinline__ void primitives(float h, float hu, float hv, float& u, float& v) {
+  const bool wet = h > kHDry;
+  const float r = 1.0f / (wet ? h : 1.0f);
+  u = wet ? hu * r : 0.0f;
+  v = wet ? hv * r : 0.0f;
+}
+#else
 __device__ __forceinline__ void primitives(float h, float hu, float hv, float& u, float& v) {
   const bool wet = h > kHDry;
   u = wet ? hu : 0.0f;
@@ -122,6 +131,7 @@ __device__ __forceinline__ void primitives(float h, float hu, float hv, float& u
     if (hv != 0.0f) v = qv;
   }
 }
+#endif
 
 // A cell of the stencil, in the face's frame: depth, normal and transverse
 // velocity, bed.
@@ -760,8 +770,14 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
           const float f = k * sqrtf(m2);
           if (!(f == 0.0f)) {
             const float denom = 1.0f + f / pow73(hh);
+#if defined(RB_FAST_MATH)
+            const float rd = 1.0f / denom;
+            hu = hu * rd;
+            hv = hv * rd;
+#else
             hu = div_pos(hu, denom);
             hv = div_pos(hv, denom);
+#endif
           }
         }
       }
@@ -795,7 +811,11 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       // hllc.py:948-966 _reduce_wavespeed on the new state
       const float cw = sqrtf(g * rmax(hh, 0.0f));
       const bool wet = hh > kHDry;
+#if defined(RB_FAST_MATH)
+      const float s = wet ? rmax(fabsf(hu), fabsf(hv)) * (1.0f / (wet ? hh : 1.0f)) + cw : cw;
+#else
       const float s = wet ? rmax(div_if(wet, fabsf(hu), hh), div_if(wet, fabsf(hv), hh)) + cw : cw;
+#endif
       smax = s > smax ? s : smax;
       bad |= !(fabsf(hh) <= FLT_MAX) || !(fabsf(hu) <= FLT_MAX) || !(fabsf(hv) <= FLT_MAX);
     }

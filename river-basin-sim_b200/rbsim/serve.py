@@ -5,7 +5,9 @@ morphology) arrive over wall-clock time. The server admits them in arrival order
 while the HBM they need fits the budget, keeps every admitted solve resident, and
 steps all of them together as one ``Ensemble`` (one persistent kernel per scheme
 over every member's tiles, each member on its own device clock). Between graph
-replays it retires finished solves (freeing their memory), runs due slow processes
+replays it retires finished solves (their results at once; a finished member stays
+in the batch, idle, until the next rebuild -- an admission, or finished members
+holding most of the batch's cells -- frees its memory), runs due slow processes
 (Exner activations) for the members that reached them, streams output frames, and
 admits whatever arrived meanwhile -- so new work joins the batch while older work
 is still on the GPU. Each result is bit-identical to solving that request alone
@@ -215,6 +217,7 @@ class _Member:
     base_steps: int = 0  # steps taken before the current ensemble was built
     writer: ZarrWriter | None = None  # the request's result store, when frames are streamed
     outputs: list[float] = field(default_factory=list)  # frame times still to come
+    done: bool = False  # reached its horizon; leaves the batch at the next rebuild
 
     @property
     def target(self) -> float:
@@ -290,13 +293,28 @@ class Server:
         if out_dir is not None:
             out_dir.mkdir(parents=True, exist_ok=True)
         queue = sorted(requests, key=lambda r: r.arrival)
+        # the members of the current batch; a finished member stays in it (its clock has
+        # stopped, its tiles return at once) until the batch is rebuilt, so a finish alone
+        # costs no rebuild
         active: list[_Member] = []
         results: list[Result] = []
         used, replays, rebuilds = 0, 0, 0
         ens = None
         t0 = time.perf_counter()
-        while queue or active:
+
+        def drop_finished() -> None:
+            nonlocal used, ens
+            done = [m for m in active if m.done]
+            if done:
+                for m in done:
+                    active.remove(m)
+                    used -= m.nbytes
+                ens = None
+
+        while queue or any(not m.done for m in active):
             now = time.perf_counter() - t0
+            if queue and queue[0].arrival <= now:
+                drop_finished()  # the batch is rebuilt for the arrival anyway: free the finished first
             # admit, in arrival order, whatever has arrived and fits the budget
             while queue and queue[0].arrival <= now and used + request_bytes(queue[0]) <= self.hbm_budget:
                 req = queue.pop(0)
@@ -310,10 +328,17 @@ class Server:
                 active.append(m)
                 used += m.nbytes
                 ens = None
-            if not active:
+            live = [m for m in active if not m.done]
+            if not live:
+                drop_finished()
+                if queue and queue[0].arrival <= now and request_bytes(queue[0]) > self.hbm_budget:
+                    raise ValueError(f"request {queue[0].rid} needs {request_bytes(queue[0])} bytes, more than the "
+                                     f"{self.hbm_budget:.0f}-byte budget")  # fmt: skip
                 if queue:
                     time.sleep(max(0.0, min(queue[0].arrival - (time.perf_counter() - t0), 0.01)))
                 continue
+            if sum(m.req.side ** 2 for m in active if m.done) > sum(m.req.side ** 2 for m in live):
+                drop_finished()  # finished members hold most of the batch's tiles: stop walking them
             if ens is None:
                 ens = _build_ensemble(active, self.graph_steps)
                 rebuilds += 1
@@ -321,10 +346,12 @@ class Server:
             ens.replay()
             replays += 1
             clk = ens.read()
-            if all(m.base_steps + c.steps == b for m, c, b in zip(active, clk, before, strict=True)):
+            if all(m.done or m.base_steps + c.steps == b for m, c, b in zip(active, clk, before, strict=True)):
                 raise RuntimeError("the batch made no progress in a replay (every member's clock is inactive)")
-            finished, retarget = [], False
+            retarget = False
             for m, c in zip(active, clk, strict=True):
+                if m.done:
+                    continue
                 m.t, m.steps = c.t, m.base_steps + c.steps
                 if m.morph is not None and c.t >= m.next_act - EPS_T:
                     m.morph.advance(c.t, c.t - m.last_act)  # operator split, scheduler order
@@ -336,18 +363,13 @@ class Server:
                     frames.submit(m.writer, c.t, m.frame_fields())
                     retarget = True
                 if c.t >= m.req.horizon - EPS_T:
-                    finished.append(m)
-            for m in finished:
-                if m.writer is not None:
-                    frames.finish(m.writer, {"steps": m.steps})
-                depth = m.st.h.cpu().numpy() if self.keep_depth else None
-                results.append(Result(m.req.rid, m.req.arrival, m.admitted, time.perf_counter() - t0, m.steps,
-                                      m.t, depth))  # fmt: skip
-                active.remove(m)
-                used -= m.nbytes
-            if finished:
-                ens = None  # rebuilt over the survivors (and any new arrivals) next round
-            elif retarget:
+                    m.done = True
+                    if m.writer is not None:
+                        frames.finish(m.writer, {"steps": m.steps})
+                    depth = m.st.h.cpu().numpy() if self.keep_depth else None
+                    results.append(Result(m.req.rid, m.req.arrival, m.admitted, time.perf_counter() - t0, m.steps,
+                                          m.t, depth))  # fmt: skip
+            if retarget and ens is not None:
                 ens.set_targets([m.target for m in active])
         wall = time.perf_counter() - t0
         lat = np.array([r.latency for r in results])
