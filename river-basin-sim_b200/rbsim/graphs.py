@@ -6,7 +6,9 @@ captured each time a clock or an ensemble is built, and that host work can cost
 more than the steps themselves (and then re-allocating what the cache gave back).
 ``capture`` records what ``enqueue`` launches on a side stream directly: the
 launches are the library's own kernels on raw stream handles, and no torch
-allocation happens during the capture.
+allocation happens during the capture. The capture is thread-local, so another
+host thread (the frame writers of ``rbsim.io`` and ``rbsim.serve``) may keep waiting
+on its own copy events while a graph is recorded.
 """
 
 from __future__ import annotations
@@ -23,7 +25,8 @@ def capture(device: torch.device, enqueue: Callable[[int], None]) -> torch.cuda.
     side = torch.cuda.Stream(device)
     side.wait_stream(cur)
     with torch.cuda.stream(side):
-        g.capture_begin()
+        # thread-local capture: a frame-writer thread may wait on its copy events meanwhile
+        g.capture_begin(capture_error_mode="thread_local")
         try:
             enqueue(side.cuda_stream)
         finally:
