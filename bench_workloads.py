@@ -513,8 +513,10 @@ def serve(args):
         out["rates"][str(rate)] = {"batched": srv.stats, "serial": serial,
                                    "throughput_ratio": srv.stats["solves_per_s"] / serial["solves_per_s"]}  # fmt: skip
         torch.cuda.empty_cache()
-    # the small-request share on its own: sides 256-512, where the serial loop is launch-bound
-    reqs = poisson_stream(50.0, 2 * args.requests, seed=4242, side_lo=256, side_hi=512)
+    # the small-request share on its own: sides 256-512, where the serial loop is launch-bound;
+    # a stream long enough (8 x --requests) that the batch reaches a steady state instead of
+    # waiting on its one longest request
+    reqs = poisson_stream(50.0, 8 * args.requests, seed=4242, side_lo=256, side_hi=512)
     with tempfile.TemporaryDirectory() as tmp:
         for r in reqs:
             r.output_every = 600.0
@@ -522,7 +524,7 @@ def serve(args):
         srv.run(reqs)
         torch.cuda.empty_cache()
         serial = serial_baseline(reqs, out_dir=f"{tmp}/serial")
-    out["small_requests_256_512_at_50_per_s"] = {
+    out["small_requests_256_512_at_50_per_s"] = {"requests": len(reqs),
         "batched": srv.stats, "serial": serial,
         "throughput_ratio": srv.stats["solves_per_s"] / serial["solves_per_s"]}  # fmt: skip
     return out
