@@ -501,7 +501,7 @@ def serve(args):
     out = {"workload": "serve", "metric": "solves/s, p50/p99 latency", "rates": {},
            "frames": "every request streams a frame every 600 simulated s and at its horizon to its own result "
                      "store, in both the batched server and the serial loop"}  # fmt: skip
-    for rate in [float(r) for r in args.rates.split(",")]:
+    for rate in [float(r) for r in args.rates.split(",") if r.strip() and r.strip() != "none"]:
         reqs = poisson_stream(rate, args.requests, seed=int(rate * 100))
         for r in reqs:
             r.output_every = 600.0
