@@ -496,7 +496,7 @@ def ensemble_256(args):
 def serve(args):
     import tempfile
 
-    from rbsim.serve import Server, poisson_stream, serial_baseline
+    from rbsim.serve import Server, poisson_stream, serial_baseline, serial_per_step_baseline
 
     out = {"workload": "serve", "metric": "solves/s, p50/p99 latency", "rates": {},
            "frames": "every request streams a frame every 600 simulated s and at its horizon to its own result "
@@ -524,9 +524,13 @@ def serve(args):
         srv.run(reqs)
         torch.cuda.empty_cache()
         serial = serial_baseline(reqs, out_dir=f"{tmp}/serial")
+        per_step = serial_per_step_baseline(reqs, out_dir=f"{tmp}/per_step")
     out["small_requests_256_512_at_50_per_s"] = {"requests": len(reqs),
-        "batched": srv.stats, "serial": serial,
-        "throughput_ratio": srv.stats["solves_per_s"] / serial["solves_per_s"]}  # fmt: skip
+        "batched": srv.stats, "serial": serial, "serial_per_step": per_step,
+        "throughput_ratio": srv.stats["solves_per_s"] / serial["solves_per_s"],
+        "throughput_ratio_vs_per_step_loop": srv.stats["solves_per_s"] / per_step["solves_per_s"],
+        "baselines": "serial: each request alone on the device clock (graph-replayed spans); serial_per_step: "
+                     "each request alone through compute_dt + step per step, the reference's loop"}  # fmt: skip
     return out
 
 

@@ -405,6 +405,70 @@ def serial_baseline(requests: list[Request], device="cuda", graph_steps: int = 1
             "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99))}  # fmt: skip
 
 
+def solve_per_step(req: Request, device="cuda", out_dir: str | None = None) -> int:
+    """One request through the reference-shaped loop: the scheduler's ticks with a
+    ``compute_dt`` (a device reduction read back every step) and a ``step`` launch per
+    tick, slow processes and frames at their ticks (solver/run.py:369-398). Same state,
+    forcing, sync times and step sequence as the server's device clock; returns the
+    steps taken."""
+    from .io.zarr_writer import AsyncFrameWriter
+    from .scheduler import MultiRateScheduler
+    from .schemes import get_scheme
+
+    st, morph = build_state(req, torch.device(device))
+    scheme = get_scheme(req.scheme)
+    outs = output_times(req)
+    frames = None
+    if out_dir is not None and outs:
+        Path(out_dir).mkdir(parents=True, exist_ok=True)
+        writer = _open_store(req, st, Path(out_dir), morph)
+        frames = AsyncFrameWriter(writer, st.device)
+    member = _Member(req, st, morph, admitted=0.0, nbytes=0)
+
+    def emit(t):
+        f = member.frame_fields()
+        frames.submit(t, f[0], f[1], f[2], f[3] if len(f) > 3 else None)
+
+    if frames is not None:
+        emit(0.0)
+    sched = MultiRateScheduler(end_time=req.horizon, output_every=req.horizon, events=outs,
+                               processes=[morph.as_slow_process()] if morph is not None else [])  # fmt: skip
+    rain = req.rain_mm_hr / 3.6e6
+    alpha = ALPHA[req.scheme]
+    steps, pending = 0, list(outs)
+    for tick in sched.ticks(lambda: scheme.compute_dt(st, alpha=alpha, dt_max=30.0)):
+        scheme.step(st, dt=tick.dt, rain=rain if tick.t0 < req.horizon - EPS_T else 0.0, t=tick.t0)
+        steps += 1
+        for proc, elapsed in tick.due:
+            proc.advance(tick.t1, elapsed)
+        if pending and tick.t1 >= pending[0] - EPS_T:
+            pending.pop(0)
+            if frames is not None:
+                emit(tick.t1)
+    st.check_device_errors()
+    if frames is not None:
+        frames.close()
+        frames.writer.finalize({"steps": steps})
+    return steps
+
+
+def serial_per_step_baseline(requests: list[Request], device="cuda", out_dir: str | None = None) -> dict:
+    """The plain loop in the reference's shape: each request solved alone, in arrival
+    order, one ``compute_dt`` + ``step`` per step (``solve_per_step``)."""
+    t0 = time.perf_counter()
+    lat = []
+    for req in sorted(requests, key=lambda r: r.arrival):
+        now = time.perf_counter() - t0
+        if req.arrival > now:
+            time.sleep(req.arrival - now)
+        solve_per_step(req, device, out_dir)
+        lat.append(time.perf_counter() - t0 - req.arrival)
+    wall = time.perf_counter() - t0
+    lat = np.array(lat)
+    return {"solves": len(lat), "wall_s": wall, "solves_per_s": len(lat) / wall,
+            "p50_s": float(np.percentile(lat, 50)), "p99_s": float(np.percentile(lat, 99))}  # fmt: skip
+
+
 def poisson_stream(rate: float, n: int, seed: int, side_lo: int = 256, side_hi: int = 4096,
                    horizon_lo: float = 600.0, horizon_hi: float = 7200.0) -> list[Request]:  # fmt: skip
     """Config-5 requests: Poisson arrivals, log-uniform sides, 70 % LI / 30 % HLLC, 10 % with Exner."""

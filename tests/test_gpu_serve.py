@@ -75,3 +75,23 @@ def test_frames_stream_and_are_the_same_alone_and_in_the_mix(tmp_path):
             np.testing.assert_array_equal(read_array(mix, name), read_array(alone, name),
                                           err_msg=f"request {req.rid}: {name}")  # fmt: skip
         assert np.isfinite(read_array(mix, "depth")).all()
+
+
+def test_the_reference_shaped_loop_gives_the_servers_frames(tmp_path):
+    """solve_per_step (compute_dt + step per tick through the scheme API, the shape of the
+    reference's run loop) and the server's device clock take the same steps: every frame
+    of an LI request with Exner and of an HLLC request is bit-identical."""
+    from rbsim.io.zarr_writer import read_array
+    from rbsim.serve import solve_alone, solve_per_step
+
+    reqs = _stream()
+    picks = [reqs[1]] + [r for r in reqs if r.scheme == "hllc_fv"][:1]
+    assert picks[0].exner and len(picks) == 2
+    for req in picks:
+        req.output_every = 60.0
+        res = solve_alone(req, graph_steps=4, out_dir=str(tmp_path / "server"))
+        steps = solve_per_step(req, out_dir=str(tmp_path / "loop"))
+        assert steps == res.steps
+        a, b = tmp_path / "server" / f"req_{req.rid}.zarr", tmp_path / "loop" / f"req_{req.rid}.zarr"
+        for name in ["time", "depth", "u", "v", "bed"] + (["bed_change"] if req.exner else []):
+            np.testing.assert_array_equal(read_array(b, name), read_array(a, name), err_msg=f"{req.rid}: {name}")
