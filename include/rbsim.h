@@ -267,11 +267,12 @@ int rb_ensemble_read(const rb_ensemble_layout *L, void *ens, rb_clock_state *out
 
 /* --- kernel tuning -------------------------------------------------------------
  * No counterpart in the reference. A process-wide choice among the HLLC stage
- * kernel's variants (tile shape, block size, faces per work item, load batching).
- * Every variant computes bit-identical results; this is a speed knob only, read at
- * each launch (a captured graph keeps the variant it was captured with). The
- * library starts with the variant measured fastest on B200 (6: 32 x 32 tiles,
- * 640 threads). */
+ * kernel's variants (tile shape, block size, faces per work item, load batching;
+ * 7 stages interior tiles with tensor-memory copies, falling back to plain loads
+ * where a row is not a multiple of 16 bytes). Every variant computes bit-identical
+ * results; this is a speed knob only, read at each launch (a captured graph keeps
+ * the variant it was captured with). The library starts with the variant measured
+ * fastest on B200 (6: 32 x 32 tiles, 640 threads). */
 int rb_hllc_set_kernel_variant(int32_t variant);
 int rb_hllc_kernel_variants(int32_t *count);
 /* The same for the local-inertial step (tile 32 x 16, 32 x 32, 64 x 16, 32 x 8, and
