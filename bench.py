@@ -273,6 +273,9 @@ def main(argv=None) -> int:
                     help="hllc_dambreak is the headline; the others measure the remaining configurations")
     ap.add_argument("--arith", default="fast", choices=["exact", "fast"],
                     help="arithmetic of the step kernels for the headline (the other build is timed beside it)")
+    ap.add_argument("--hllc-variant", type=int, default=None,
+                    help="HLLC stage-kernel variant for the headline (rb_hllc_set_kernel_variant; default: the "
+                         "library's)")
     ap.add_argument("--headline-only", action="store_true",
                     help="time the headline steps only (no e2e, other configurations, CPU or float64 legs)")
     ap.add_argument("--no-legs", action="store_true", help="skip the CPU and float64 legs of a --workload record")
@@ -364,6 +367,8 @@ def main(argv=None) -> int:
         return ms, clocks, [e[0].elapsed_time(e[1]) for e in ev], [e[1].elapsed_time(e[2]) for e in ev]
 
     # --- value: the selected arithmetic; then the other build, for comparison ---
+    if args.hllc_variant is not None:
+        _lib.check(L.rb_hllc_set_kernel_variant(args.hllc_variant))
     arith.set_arithmetic(args.arith)
     ms, clocks, stage1_ms, stage2_ms = timed_replay(True)
     # Whole job: the cells every replica stepped over the slowest replica's time.
