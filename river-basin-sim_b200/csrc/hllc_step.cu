@@ -403,6 +403,9 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
         mbar_wait_bounded(&S.bar, 0, kTmaWaitCycles);
         return;
       }
+      // every thread is past its wait: the barrier object is retired before its memory
+      // is anything else again
+      if (threadIdx.x == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(&S.bar)) : "memory");
       for (int k = threadIdx.x; k < RH * RW; k += NT) {
         const int r = k / RW, c = k - r * RW;
         const int l = r * LW + c + 1;  // the box starts one column left of the staged region
