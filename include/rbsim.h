@@ -269,7 +269,8 @@ int rb_ensemble_read(const rb_ensemble_layout *L, void *ens, rb_clock_state *out
  * No counterpart in the reference. A process-wide choice among the HLLC stage
  * kernel's variants (tile shape, block size, faces per work item, load batching;
  * 7 stages interior tiles with tensor-memory copies, falling back to plain loads
- * where a row is not a multiple of 16 bytes). Every variant computes bit-identical
+ * where a row is not a multiple of 16 bytes; 8 does the same with one persistent block
+ * per resident slot that prefetches the halo of its next tile). Every variant computes bit-identical
  * results; this is a speed knob only, read at each launch (a captured graph keeps
  * the variant it was captured with). The library starts with the variant measured
  * fastest on B200 (6: 32 x 32 tiles, 640 threads). */

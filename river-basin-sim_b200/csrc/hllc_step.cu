@@ -22,6 +22,7 @@
 // buffer of the caller's double-buffered (h, hu, hv).
 #include <cuda.h>  // CUtensorMap and its encoder's signature (reached through the runtime)
 
+#include <algorithm>
 #include <atomic>
 #include <cfloat>
 #include <cstring>
@@ -270,6 +271,7 @@ struct HllcSmemTma : HllcSmem<TX, TY> {
   static constexpr int LAND = (LW * LH + 31) / 32 * 32;  // floats per field, a multiple of 128 bytes
   alignas(128) float land[4][LAND];
   unsigned long long bar;
+  int iter;  // LP 3: how many tiles this persistent CTA has finished
 };
 
 template <int TX, int TY, int FU, int LP>
@@ -278,6 +280,10 @@ struct HllcSmemOf {
 };
 template <int TX, int TY>
 struct HllcSmemOf<TX, TY, 1, 2> {
+  using type = HllcSmemTma<TX, TY>;
+};
+template <int TX, int TY>
+struct HllcSmemOf<TX, TY, 1, 3> {
   using type = HllcSmemTma<TX, TY>;
 };
 
@@ -313,6 +319,55 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsig
 // A copy that has not landed after ~1 s at the B200's clock is treated as lost.
 constexpr long long kTmaWaitCycles = 2000000000LL;
 
+
+// A tile whose four halo boxes (columns x0-4 .. x0+TX+3, rows y0-3 .. y0+TY+2) lie
+// inside the domain.
+template <int TX, int TY>
+__device__ __forceinline__ bool tma_interior(int x0, int y0, int ny, int nx) {
+  return x0 >= 4 && x0 + TX + 4 <= nx && y0 >= 3 && y0 + TY + 3 <= ny;
+}
+
+// Thread 0: the four halo boxes of the tile at (x0, y0) into the landing areas, one
+// transaction on the barrier.
+template <int TX, int TY>
+__device__ __forceinline__ void tma_issue_halo(float (*land)[HllcSmemTma<TX, TY>::LAND], unsigned long long* bar,
+                                               const HllcMaps* maps, int stage, int cur, int x0, int y0) {
+  using ST = HllcSmemTma<TX, TY>;
+  constexpr unsigned kBytes = 4u * ST::LW * ST::LH * sizeof(float);
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(kBytes) : "memory");
+  tma_load_tile(&land[0][0], stage == 1 ? &maps->h[cur] : &maps->h1, x0 - 4, y0 - 3, bar);
+  tma_load_tile(&land[1][0], stage == 1 ? &maps->hu[cur] : &maps->hu1, x0 - 4, y0 - 3, bar);
+  tma_load_tile(&land[2][0], stage == 1 ? &maps->hv[cur] : &maps->hv1, x0 - 4, y0 - 3, bar);
+  tma_load_tile(&land[3][0], &maps->z, x0 - 4, y0 - 3, bar);
+}
+
+// The tile at (x0, y0) is staged from the landing areas (their copies can be issued).
+template <int TX, int TY, class SMEM>
+__device__ __forceinline__ bool tma_ready(SMEM& S, int x0, int y0, int ny, int nx) {
+  return (smem_addr(&S.land[0][0]) & 127u) == 0 && tma_interior<TX, TY>(x0, y0, ny, nx);
+}
+
+// Thread 0 of a persistent CTA at tile (bx, by): start the next phase of the barrier
+// for the CTA's next tile (gridDim.x tiles on, row-major), if it has one.
+template <int TX, int TY, class SMEM>
+__device__ __forceinline__ void tma_issue_for(SMEM& S, const HllcMaps* maps, int stage, int cur, int t, int ny,
+                                              int nx) {
+  const int tiles_x = (nx + TX - 1) / TX;
+  if (t >= tiles_x * ((ny + TY - 1) / TY)) return;
+  const int x0 = (t % tiles_x) * TX, y0 = (t / tiles_x) * TY;
+  if (tma_ready<TX, TY>(S, x0, y0, ny, nx))
+    tma_issue_halo<TX, TY>(S.land, &S.bar, maps, stage, cur, x0, y0);
+  else
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(&S.bar)) : "memory");
+}
+
+template <int TX, int TY, class SMEM>
+__device__ __forceinline__ void tma_prefetch_next(SMEM& S, const HllcMaps* maps, int stage, int cur, int bx, int by,
+                                                  int ny, int nx) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // the reads above come before the copies
+  tma_issue_for<TX, TY>(S, maps, stage, cur, by * ((nx + TX - 1) / TX) + bx + (int)gridDim.x, ny, nx);
+}
+
 // One Heun stage of tile (bx, by) of domain p; ledger slot `slot`. Called by every
 // thread of the block; returns uniformly. FU selects the face phase: 1, each face
 // reconstructs its four-cell stencil; 2 or 3, FU faces per work item in a rolling
@@ -320,8 +375,8 @@ constexpr long long kTmaWaitCycles = 2000000000LL;
 // its divisions. Every choice computes the same bits. LP 2 stages tiles whose halo lies inside the domain with tensor-memory
 // copies from the tensor maps in `maps` (edge tiles take the LP 1 path).
 template <int TX, int TY, int NT, int STAGE, int FU = 1, int LP = 1, class SMEM = HllcSmem<TX, TY>>
-__device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, size_t slot, SMEM& S,
-                                          const HllcMaps* maps = nullptr) {
+__device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, size_t slot, SMEM& S,
+                                          const HllcMaps* maps = nullptr, unsigned phase = 0) {
   static_assert(NT / 32 <= 32, "reduction scratch sized for <= 32 warps");
   using SM = HllcSmem<TX, TY>;
   constexpr int H = SM::H, RW = SM::RW, RH = SM::RH, XW = SM::XW, XH = SM::XH, YW = SM::YW, YH = SM::YH;
@@ -348,7 +403,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
   double wt = p.wt;
   if (p.clk != nullptr) {  // device-resident clock: this step's dt and forcing
     const DevClock* c = p.clk;
-    if (!c->active) return;
+    if (!c->active) return true;
     cur = c->cur;
     dt = c->dt32;
     wt = c->wt;
@@ -401,7 +456,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
       if (__syncthreads_or(!ok)) {
         if (threadIdx.x == 0) flag_error(p.err, RB_DEVERR_TIMEOUT);
         mbar_wait_bounded(&S.bar, 0, kTmaWaitCycles);
-        return;
+        return false;
       }
       // every thread is past its wait: the barrier object is retired before its memory
       // is anything else again
@@ -415,6 +470,27 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
         s_c[r][c] = make_float4(hh, u, v, S.land[3][l]);
       }
       static_assert(RH * LW <= LAND, "landing area too small");
+      staged = true;
+    }
+  }
+  if constexpr (LP == 3) {
+    using ST = HllcSmemTma<TX, TY>;
+    constexpr int LW = ST::LW;
+    if (tma_ready<TX, TY>(S, x0, y0, ny, nx)) {
+      const bool ok = mbar_wait_bounded(&S.bar, phase, kTmaWaitCycles);
+      if (__syncthreads_or(!ok)) {  // block-uniform: flag, wait once more (bounded), stop
+        if (threadIdx.x == 0) flag_error(p.err, RB_DEVERR_TIMEOUT);
+        mbar_wait_bounded(&S.bar, phase, kTmaWaitCycles);
+        return false;
+      }
+      for (int k = threadIdx.x; k < RH * RW; k += NT) {
+        const int r = k / RW, c = k - r * RW;
+        const int l = r * LW + c + 1;  // the box starts one column left of the staged region
+        const float hh = S.land[0][l];
+        float u, v;
+        primitives(hh, S.land[1][l], S.land[2][l], u, v);
+        s_c[r][c] = make_float4(hh, u, v, S.land[3][l]);
+      }
       staged = true;
     }
   }
@@ -634,6 +710,11 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
     }
   }
   __syncthreads();
+  if constexpr (LP == 3) {
+    // every thread has long read the landing areas: thread 0 refills them with the
+    // CTA's next tile's halo while this tile's update is computed
+    if (threadIdx.x == 0) tma_prefetch_next<TX, TY>(S, maps, STAGE, cur, bx, by, ny, nx);
+  }
 
   // 3. mass-only donor beta on the tile + ring (hllc.py:700-736).
   const float dtdx = dt / dx;
@@ -833,6 +914,7 @@ __device__ __forceinline__ void hllc_tile(const HllcParams& p, int bx, int by, s
     if (bad) flag_error(p.err, RB_DEVERR_NONFINITE);
   }
   __syncthreads();  // the shared tile is reused by the caller's next tile
+  return true;
 }
 
 // The single-domain stage kernel. Shared memory is dynamic (a 32 x 32 tile needs
@@ -885,6 +967,38 @@ __global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT)
   auto& S = *reinterpret_cast<HllcSmemTma<TX, TY>*>(hllc_tma_smem_raw);
   hllc_tile<TX, TY, NT, STAGE, 1, 2>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S,
                                      &maps);
+}
+
+// The persistent, prefetching form: a grid of as many CTAs as fit the device at once,
+// each taking tiles blockIdx.x, blockIdx.x + gridDim.x, ... (one ledger slot per tile,
+// as in the one-tile-per-block grid, so the sums are the same bits). While a CTA
+// computes one tile, the halo of its next interior tile is already on its way.
+template <int TX, int TY, int NT, int STAGE>
+__global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT)
+    hllc_stage_tma_pipe_kernel(const HllcParams p, const __grid_constant__ HllcMaps maps) {
+  extern __shared__ __align__(1024) unsigned char hllc_pipe_smem_raw[];
+  auto& S = *reinterpret_cast<HllcSmemTma<TX, TY>*>(hllc_pipe_smem_raw);
+  if (p.clk != nullptr && !p.clk->active) return;  // no tile works this step
+  const int cur = p.clk != nullptr ? p.clk->cur : p.cur;
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(&S.bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    tma_issue_for<TX, TY>(S, &maps, STAGE, cur, blockIdx.x, p.ny, p.nx);
+  }
+  if (threadIdx.x == 0) S.iter = 0;
+  __syncthreads();
+  // The tile counter lives in shared memory, so nothing of the loop is held in
+  // registers across a tile (the tile itself needs all 48 that two resident blocks of
+  // 640 threads leave a thread). The k-th tile of this CTA waits on barrier parity k & 1.
+  for (;;) {
+    const int k = S.iter;
+    const int tiles_x = (p.nx + TX - 1) / TX;
+    const int t = blockIdx.x + k * gridDim.x;
+    if (t >= tiles_x * ((p.ny + TY - 1) / TY)) return;
+    if (!hllc_tile<TX, TY, NT, STAGE, 1, 3>(p, t % tiles_x, t / tiles_x, (size_t)t, S, &maps, k & 1u)) return;
+    if (threadIdx.x == 0) S.iter++;  // every thread read it before the tile's last barrier
+    __syncthreads();
+  }
 }
 
 using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
@@ -968,9 +1082,37 @@ static void prepare_hllc_tma() {
   }
 }
 
-// Launch the TMA-staged kernel when every staged field can be mapped (16-byte aligned
-// rows, a grid at least one box large); otherwise the same tile with plain loads.
+// The resident-CTA count of the persistent kernel on the current device (its SMs times
+// the blocks one SM holds), found once per device; 0 if the device cannot hold a block.
 template <int TX, int TY, int NT>
+static int hllc_pipe_grid() {
+  static std::atomic<int> per_dev[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  int g = per_dev[dev & 63].load();
+  if (g == 0) {
+    constexpr int smem = (int)sizeof(HllcSmemTma<TX, TY>);
+    int sms = 0, per_sm = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaFuncSetAttribute(hllc_stage_tma_pipe_kernel<TX, TY, NT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem) != cudaSuccess ||
+        cudaFuncSetAttribute(hllc_stage_tma_pipe_kernel<TX, TY, NT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, hllc_stage_tma_pipe_kernel<TX, TY, NT, 2>, NT, smem) !=
+            cudaSuccess) {
+      cudaGetLastError();
+      per_sm = 0;
+    }
+    g = per_sm > 0 && sms > 0 ? per_sm * sms : -1;
+    per_dev[dev & 63].store(g);
+  }
+  return g > 0 ? g : 0;
+}
+
+// Launch a TMA-staged kernel when every staged field can be mapped (16-byte aligned
+// rows, a grid at least one box large); otherwise the same tile with plain loads.
+// PIPE selects the persistent, prefetching kernel.
+template <int TX, int TY, int NT, bool PIPE = false>
 static cudaError_t launch_hllc_tma(const HllcParams& p, int stage, cudaStream_t s) {
   constexpr size_t smem = sizeof(HllcSmemTma<TX, TY>);
   static_assert(smem <= 113 * 1024, "two blocks of the TMA-staged tile must fit an SM");
@@ -983,6 +1125,17 @@ static cudaError_t launch_hllc_tma(const HllcParams& p, int stage, cudaStream_t 
   ok = ok && field_map(m.z, p.z, p.ny, p.nx, BW, BH) && field_map(m.h1, p.h1, p.ny, p.nx, BW, BH) &&
        field_map(m.hu1, p.hu1, p.ny, p.nx, BW, BH) && field_map(m.hv1, p.hv1, p.ny, p.nx, BW, BH);
   if (!ok) return launch_hllc<TX, TY, NT, 1, 1>(p, stage, s);
+  const int tiles = ((p.nx + TX - 1) / TX) * ((p.ny + TY - 1) / TY);
+  if constexpr (PIPE) {
+    const int resident = hllc_pipe_grid<TX, TY, NT>();
+    if (resident == 0) return launch_hllc<TX, TY, NT, 1, 1>(p, stage, s);
+    const int grid = std::min(resident, tiles);
+    if (stage == 1)
+      hllc_stage_tma_pipe_kernel<TX, TY, NT, 1><<<grid, NT, smem, s>>>(p, m);
+    else
+      hllc_stage_tma_pipe_kernel<TX, TY, NT, 2><<<grid, NT, smem, s>>>(p, m);
+    return cudaGetLastError();
+  }
   prepare_hllc_tma<TX, TY, NT>();
   const dim3 grid((p.nx + TX - 1) / TX, (p.ny + TY - 1) / TY);
   if (stage == 1)
@@ -998,14 +1151,18 @@ static cudaError_t launch_hllc_tma(const HllcParams& p, int stage, cudaStream_t 
 // is the fastest measured on B200: 0.316 ms per 2048 x 2048 dam-break step against
 // 0.326 for 512 threads, 0.337 for 576, 0.323 for 608, 0.328 for 768 and 0.348 for
 // 800 (which spills at its 40-register bound). The 2380 face work items of a tile
-// fill 3.7 passes of 640 threads against 4.6 of 512.
+// fill 3.7 passes of 640 threads against 4.6 of 512. Staging interior tiles with
+// tensor-memory copies measures 0.319 ms (7: one tile a block) and 0.360 ms (8: one
+// resident block of 512 threads per slot walking the tiles and prefetching the next
+// one's halo, against 0.330 for the same block as a grid of tiles): the copies free no
+// issue slots the tile needs, and a static walk leaves SMs idle at the end.
 struct HllcKernelVariant {
   int tx, ty, nt, fu, lp;
 };
 static const HllcKernelVariant kHllcVariants[] = {
     {32, 16, 256, 1, 0}, {32, 16, 256, 1, 1}, {32, 16, 256, 3, 1},
     {32, 16, 256, 2, 1}, {32, 32, 512, 1, 1}, {64, 16, 512, 1, 1}, {32, 32, 640, 1, 1},
-    {32, 32, 640, 1, 2},
+    {32, 32, 640, 1, 2}, {32, 32, 512, 1, 3},
 };
 constexpr int kNumHllcVariants = (int)(sizeof(kHllcVariants) / sizeof(kHllcVariants[0]));
 constexpr int kDefaultHllcVariant = 6;
@@ -1026,6 +1183,7 @@ void hllc_prepare_device() {
   prepare_hllc<64, 16, 512, 1, 1>();
   prepare_hllc<32, 32, 640, 1, 1>();
   prepare_hllc_tma<32, 32, 640>();
+  hllc_pipe_grid<32, 32, 512>();
 #if !defined(RB_FAST_MATH)
   fast::hllc_prepare_device();
 #endif
@@ -1057,6 +1215,7 @@ cudaError_t hllc_stage_launch_variant(const HllcParams& p, int stage, int varian
     case 0: return launch_hllc<32, 16, 256, 1, 0>(p, stage, s);
     case 4: return launch_hllc<32, 32, 512, 1, 1>(p, stage, s);
     case 7: return launch_hllc_tma<32, 32, 640>(p, stage, s);
+    case 8: return launch_hllc_tma<32, 32, 512, true>(p, stage, s);
     default: return launch_hllc<32, 32, 640, 1, 1>(p, stage, s);
   }
 }

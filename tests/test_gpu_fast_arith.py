@@ -99,6 +99,25 @@ def test_hllc_dambreak_2048_within_tolerance():
     _close(got, _fixed_dt(case, got), "hllc2048")
 
 
+@pytest.mark.parametrize("variant", [7, 8])
+def test_tma_staged_variants_within_tolerance(variant):
+    """The tensor-copy staged stage kernels (7: one tile a block; 8: persistent blocks
+    prefetching their next tile) in fast arithmetic, on 1056 ragged 32 x 32 tiles."""
+    from gpu_api import GpuAPI
+    from rbsim import _lib
+    from test_gpu_parity import _synthetic_hllc
+
+    case = _synthetic_hllc(1000, 1028, seed=17)
+    case["steps"] = 6
+    L = _lib.lib()
+    try:
+        _lib.check(L.rb_hllc_set_kernel_variant(variant))
+        got = run_case(dict(case), GpuAPI())
+    finally:
+        _lib.check(L.rb_hllc_set_kernel_variant(6))
+    _close(got, _fixed_dt(case, got), f"hllc(1000, 1028) variant {variant}")
+
+
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_golden_cases_against_float64(name):
     from f64_error import check, error_vs_f64

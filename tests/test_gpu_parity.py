@@ -220,6 +220,28 @@ def test_every_hllc_kernel_variant_matches_oracle_bitwise(shape):
         _lib.check(L.rb_hllc_set_kernel_variant(6))  # the library's default
 
 
+def test_persistent_tma_variant_walks_more_tiles_than_resident_blocks():
+    """Variant 8 launches one block per resident slot (296 on a 148-SM B200) and walks
+    the tiles, copying the halo of each block's next interior tile while it computes
+    the current one. 1000 x 1028 has 1056 tiles of 32 x 32, about 3.6 a block, ragged
+    on both axes: the barrier phases alternate, edge tiles take plain loads between
+    copied ones, and the result is the oracle's bits."""
+    from gpu_api import GpuAPI
+    from rbsim import _lib
+
+    case = _synthetic_hllc(1000, 1028, seed=17)
+    case["boundaries"] = {"north": "open", "south": "closed", "east": "open", "west": "fixed_stage"}
+    case["stage_curves"] = {"west": [(0.0, 9.0), (10.0, 11.0)]}
+    case["steps"] = 6
+    want = _oracle_outputs(case)
+    L = _lib.lib()
+    try:
+        _lib.check(L.rb_hllc_set_kernel_variant(8))
+        _compare(run_case(case, GpuAPI()), want, "hllc(1000, 1028) variant 8")
+    finally:
+        _lib.check(L.rb_hllc_set_kernel_variant(6))
+
+
 @pytest.mark.parametrize("shape", [(333, 517), (1, 700), (37, 3)])
 def test_every_li_kernel_variant_matches_oracle_bitwise(shape):
     """The local-inertial step's tile variants are a speed choice only."""
