@@ -368,16 +368,28 @@ __device__ __forceinline__ void tma_prefetch_next(SMEM& S, const HllcMaps* maps,
   tma_issue_for<TX, TY>(S, maps, stage, cur, by * ((nx + TX - 1) / TX) + bx + (int)gridDim.x, ny, nx);
 }
 
+// A tile whose whole staged region (the tile and a 3-cell halo) lies inside the
+// domain: every bounds check and edge case of the tile is known to be false there.
+template <int TX, int TY>
+__device__ __forceinline__ bool hllc_deep_interior(int x0, int y0, int ny, int nx) {
+  return x0 >= 3 && y0 >= 3 && x0 + TX + 3 <= nx && y0 + TY + 3 <= ny;
+}
+
 // One Heun stage of tile (bx, by) of domain p; ledger slot `slot`. Called by every
-// thread of the block; returns uniformly. FU selects the face phase: 1, each face
-// reconstructs its four-cell stencil; 2 or 3, FU faces per work item in a rolling
-// window that reconstructs each cell once. LP 1 issues a thread's halo loads before
-// its divisions. Every choice computes the same bits. LP 2 stages tiles whose halo lies inside the domain with tensor-memory
-// copies from the tensor maps in `maps` (edge tiles take the LP 1 path).
-template <int TX, int TY, int NT, int STAGE, int FU = 1, int LP = 1, class SMEM = HllcSmem<TX, TY>>
+// thread of the block; returns uniformly (false only when a tensor copy never landed:
+// the block stops). FU selects the face phase: 1, each face reconstructs its
+// four-cell stencil; 2 or 3, FU faces per work item in a rolling window that
+// reconstructs each cell once. LP 1 issues a thread's halo loads before its
+// divisions; LP 2 stages tiles whose halo lies inside the domain with tensor-memory
+// copies from the tensor maps in `maps` (edge tiles take the LP 1 path); LP 3 does
+// the same for a persistent block whose next tile's copies complete barrier phase
+// `phase`. IN is the instantiation for a tile hllc_deep_interior admits, without the
+// bounds checks and edge cases. Every choice computes the same bits.
+template <int TX, int TY, int NT, int STAGE, int FU = 1, int LP = 1, bool IN = false, class SMEM = HllcSmem<TX, TY>>
 __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, size_t slot, SMEM& S,
                                           const HllcMaps* maps = nullptr, unsigned phase = 0) {
   static_assert(NT / 32 <= 32, "reduction scratch sized for <= 32 warps");
+  static_assert(HllcSmem<TX, TY>::H == 3, "hllc_deep_interior assumes a 3-cell halo");
   using SM = HllcSmem<TX, TY>;
   constexpr int H = SM::H, RW = SM::RW, RH = SM::RH, XW = SM::XW, XH = SM::XH, YW = SM::YW, YH = SM::YH;
   constexpr int BW = SM::BW, BH = SM::BH;
@@ -498,7 +510,8 @@ __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, s
   } else if constexpr (LP == 0) {
     for (int k = threadIdx.x; k < RH * RW; k += NT) {
       const int r = k / RW, c = k - r * RW;
-      const int gi = min(max(y0 - H + r, 0), ny - 1), gj = min(max(x0 - H + c, 0), nx - 1);
+      const int gi = IN ? y0 - H + r : min(max(y0 - H + r, 0), ny - 1);
+      const int gj = IN ? x0 - H + c : min(max(x0 - H + c, 0), nx - 1);
       const size_t id = (size_t)gi * nx + gj;
       const float hh = h_s[id];
       float u, v;
@@ -515,7 +528,8 @@ __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, s
       const int k = threadIdx.x + i * NT;
       if (k < RH * RW) {
         const int r = k / RW, c = k - r * RW;
-        const int gi = min(max(y0 - H + r, 0), ny - 1), gj = min(max(x0 - H + c, 0), nx - 1);
+        const int gi = IN ? y0 - H + r : min(max(y0 - H + r, 0), ny - 1);
+        const int gj = IN ? x0 - H + c : min(max(x0 - H + c, 0), nx - 1);
         const size_t id = (size_t)gi * nx + gj;
         lh[i] = h_s[id];
         lhu[i] = hu_s[id];
@@ -626,11 +640,15 @@ __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, s
     };
     // x-faces span columns x0-1 .. x0+TX+1 and rows y0-1 .. y0+TY, y-faces columns
     // x0-1 .. x0+TX and rows y0-1 .. y0+TY+1: all inner faces when these hold
-    const bool inner = x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= nx && y0 + TY + 2 <= ny;
-    if (inner)
+    if constexpr (IN) {
       face_loop(std::true_type{});
-    else
-      face_loop(std::false_type{});
+    } else {
+      const bool inner = x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= nx && y0 + TY + 2 <= ny;
+      if (inner)
+        face_loop(std::true_type{});
+      else
+        face_loop(std::false_type{});
+    }
   } else {
     // FU consecutive faces per work item along the normal, each cell reconstructed
     // once in a rolling window: the reference's face-local eta_l / eta_r are the
@@ -722,7 +740,7 @@ __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, s
     const int a = k / BW, b = k - a * BW;
     const int gi = y0 - 1 + a, gj = x0 - 1 + b;
     float beta = 1.0f;
-    if (gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
+    if (IN || (gi >= 0 && gi < ny && gj >= 0 && gj < nx)) {
       float q_out = 0.0f;
       const float fl = s_fxh[a][b];
       if (fl < 0.0f) q_out = q_out - fl;
@@ -763,7 +781,7 @@ __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, s
     const int k = threadIdx.x + i * NT;
     const int r = k / TX, c = k - r * TX;
     const int gi = y0 + r, gj = x0 + c;
-    if (k < TX * TY && gi < ny && gj < nx) {
+    if (k < TX * TY && (IN || (gi < ny && gj < nx))) {
       const size_t id = (size_t)gi * nx + gj;
       g_hus[i] = hu_s[id];
       g_hvs[i] = hv_s[id];
@@ -780,14 +798,14 @@ __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, s
     const int k = threadIdx.x + i * NT;
     const int r = k / TX, c = k - r * TX;
     const int gi = y0 + r, gj = x0 + c;
-    if (k >= TX * TY || gi >= ny || gj >= nx) continue;
+    if (k >= TX * TY || (!IN && (gi >= ny || gj >= nx))) continue;
     const size_t id = (size_t)gi * nx + gj;
     const int R = r + H, Cc = c + H;  // this cell in the staged region
     // west / east faces: the donor of q > 0 is the cell to the west, of q < 0 the
     // cell to the east, and a face with no donor cell inside the domain stays as is
     float qw = s_fxh[r + 1][c + 1];
     if (qw > 0.0f) {
-      if (gj >= 1) qw = qw * s_beta[r + 1][c];
+      if (IN || gj >= 1) qw = qw * s_beta[r + 1][c];
     } else if (qw < 0.0f) {
       qw = qw * s_beta[r + 1][c + 1];
     }
@@ -795,11 +813,11 @@ __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, s
     if (qe > 0.0f) {
       qe = qe * s_beta[r + 1][c + 1];
     } else if (qe < 0.0f) {
-      if (gj + 1 <= nx - 1) qe = qe * s_beta[r + 1][c + 2];
+      if (IN || gj + 1 <= nx - 1) qe = qe * s_beta[r + 1][c + 2];
     }
     float qn = s_fyh[r + 1][c + 1];
     if (qn > 0.0f) {
-      if (gi >= 1) qn = qn * s_beta[r][c + 1];
+      if (IN || gi >= 1) qn = qn * s_beta[r][c + 1];
     } else if (qn < 0.0f) {
       qn = qn * s_beta[r + 1][c + 1];
     }
@@ -807,9 +825,9 @@ __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, s
     if (qs > 0.0f) {
       qs = qs * s_beta[r + 1][c + 1];
     } else if (qs < 0.0f) {
-      if (gi + 1 <= ny - 1) qs = qs * s_beta[r + 2][c + 1];
+      if (IN || gi + 1 <= ny - 1) qs = qs * s_beta[r + 2][c + 1];
     }
-    if (p.ledger != nullptr) {
+    if (!IN && p.ledger != nullptr) {  // an interior tile has no edge face
       if (gj == 0 && p.bc[RB_EDGE_WEST] != RB_BC_CLOSED) loss -= wt * (double)qw;
       if (gj == nx - 1 && p.bc[RB_EDGE_EAST] != RB_BC_CLOSED) loss += wt * (double)qe;
       if (gi == 0 && p.bc[RB_EDGE_NORTH] != RB_BC_CLOSED) loss -= wt * (double)qn;
@@ -926,7 +944,11 @@ __global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT) hllc_stage_kerne
   extern __shared__ __align__(16) unsigned char hllc_smem_raw[];
   using SMEM = typename HllcSmemOf<TX, TY, FU, LP>::type;
   auto& S = *reinterpret_cast<SMEM*>(hllc_smem_raw);
-  hllc_tile<TX, TY, NT, STAGE, FU, LP>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S);
+  const size_t slot = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+  if (hllc_deep_interior<TX, TY>(blockIdx.x * TX, blockIdx.y * TY, p.ny, p.nx))
+    hllc_tile<TX, TY, NT, STAGE, FU, LP, true>(p, blockIdx.x, blockIdx.y, slot, S);
+  else
+    hllc_tile<TX, TY, NT, STAGE, FU, LP, false>(p, blockIdx.x, blockIdx.y, slot, S);
 }
 
 // The shared-memory opt-in is a per-device function attribute: set once per device
@@ -965,8 +987,11 @@ __global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT)
     hllc_stage_tma_kernel(const HllcParams p, const __grid_constant__ HllcMaps maps) {
   extern __shared__ __align__(1024) unsigned char hllc_tma_smem_raw[];
   auto& S = *reinterpret_cast<HllcSmemTma<TX, TY>*>(hllc_tma_smem_raw);
-  hllc_tile<TX, TY, NT, STAGE, 1, 2>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S,
-                                     &maps);
+  const size_t slot = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+  if (hllc_deep_interior<TX, TY>(blockIdx.x * TX, blockIdx.y * TY, p.ny, p.nx))
+    hllc_tile<TX, TY, NT, STAGE, 1, 2, true>(p, blockIdx.x, blockIdx.y, slot, S, &maps);
+  else
+    hllc_tile<TX, TY, NT, STAGE, 1, 2, false>(p, blockIdx.x, blockIdx.y, slot, S, &maps);
 }
 
 // The persistent, prefetching form: a grid of as many CTAs as fit the device at once,

@@ -133,9 +133,18 @@ struct LiSmem : LiGeom<TX, TY> {
   LiChanSmem<TX, TY, CH> ch;
 };
 
+// A tile whose staged region (the tile and a 2-cell halo) lies inside the domain:
+// all its faces are inner faces and no cell of it is on a domain edge.
+template <int TX, int TY>
+__device__ __forceinline__ bool li_deep_interior(int x0, int y0, int ny, int nx) {
+  return x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= nx && y0 + TY + 2 <= ny;
+}
+
 // One CTA-wide tile of the step: tile (bx, by) of domain p, ledger slot `slot`.
-// Called by every thread of the block; returns uniformly.
-template <int TX, int TY, int NT, bool CH = false>
+// Called by every thread of the block; returns uniformly. IN is the instantiation
+// for a tile li_deep_interior admits, without bounds checks and edge cases (the
+// same bits).
+template <int TX, int TY, int NT, bool CH = false, bool IN = false>
 __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_t slot, LiSmem<TX, TY, CH>& S) {
   static_assert(NT / 32 <= 16, "reduction scratch sized for <= 16 warps");
   using SM = LiSmem<TX, TY, CH>;
@@ -187,7 +196,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
       const int r = k / RW, c = k - r * RW;
       const int gi = y0 - 2 + r, gj = x0 - 2 + c;
       lh[i] = lz[i] = ln[i] = lw[i] = ld[i] = lc[i] = 0.0f;
-      if (k < RH * RW && gi >= 0 && gi < ny && gj >= 0 && gj < nx) {
+      if (k < RH * RW && (IN || (gi >= 0 && gi < ny && gj >= 0 && gj < nx))) {
         const size_t id = (size_t)gi * nx + gj;
         lh[i] = h_in[id];
         lz[i] = p.z[id];
@@ -225,7 +234,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
       const int a = k / XW, b = k - a * XW;
       const int gi = y0 - 1 + a, gj = x0 - 1 + b;
       fq[i] = fc[i] = ff[i] = 0.0f;
-      if (k < XH * XW && gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1) {
+      if (k < XH * XW && (IN || (gi >= 0 && gi < ny && gj >= 1 && gj <= nx - 1))) {
         const size_t fid = (size_t)gi * (nx + 1) + gj;
         if constexpr (CH) {
           fc[i] = p.qxcb[cur][fid];
@@ -241,7 +250,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
       const int a = k / YW, b = k - a * YW;
       const int gi = y0 - 1 + a, gj = x0 - 1 + b;
       gq[i] = gc[i] = gf[i] = 0.0f;
-      if (k < YH * YW && gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx) {
+      if (k < YH * YW && (IN || (gi >= 1 && gi <= ny - 1 && gj >= 0 && gj < nx))) {
         const size_t fid = (size_t)gi * nx + gj;
         if constexpr (CH) {
           gc[i] = p.qycb[cur][fid];
@@ -367,7 +376,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
   };
   // x-faces span columns x0-1 .. x0+TX+1 and rows y0-1 .. y0+TY, y-faces columns
   // x0-1 .. x0+TX and rows y0-1 .. y0+TY+1: all inner faces when these hold
-  if (x0 >= 2 && y0 >= 2 && x0 + TX + 2 <= nx && y0 + TY + 2 <= ny)
+  if (IN || li_deep_interior<TX, TY>(x0, y0, ny, nx))
     face_loop(std::true_type{});
   else
     face_loop(std::false_type{});
@@ -405,9 +414,9 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
       const int k = kk;
       const int a = 1 + k / (TX + 1), b = 1 + (k - (a - 1) * (TX + 1));
       const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-      if (gi >= ny || gj > nx) continue;
+      if (!IN && (gi >= ny || gj > nx)) continue;
       float q = s_qx[a][b];
-      if (limit && gj >= 1 && gj <= nx - 1) {
+      if (limit && (IN || (gj >= 1 && gj <= nx - 1))) {
         if constexpr (!CH) {
           if (q > 0.0f)
             q = q * s_beta[a][b - 1];
@@ -421,7 +430,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
         }
         s_qx[a][b] = q;
       }
-      if (b == TX + 1 && gj != nx) continue;
+      if (b == TX + 1 && (IN || gj != nx)) continue;
       const size_t fid = (size_t)gi * (nx + 1) + gj;
       qx_out[fid] = q;
       if constexpr (CH) {
@@ -440,7 +449,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
           p.qs_int_x[fid] = tot;
           p.qs_comp_x[fid] = comp;
         }
-      } else if (p.d50 != nullptr && gj >= 1 && gj <= nx - 1) {
+      } else if (p.d50 != nullptr && (IN || (gj >= 1 && gj <= nx - 1))) {
         const float eta_max = rmax(s_eta[a + 1][b], s_eta[a + 1][b + 1]);
         const float z_bank = rmax(s_z[a + 1][b], s_z[a + 1][b + 1]);
         const float h_face = eta_max - z_bank;
@@ -456,9 +465,9 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
       const int k = kk - NXW;
       const int a = 1 + k / TX, b = 1 + (k - (a - 1) * TX);
       const int gi = y0 - 1 + a, gj = x0 - 1 + b;
-      if (gj >= nx || gi > ny) continue;
+      if (!IN && (gj >= nx || gi > ny)) continue;
       float q = s_qy[a][b];
-      if (limit && gi >= 1 && gi <= ny - 1) {
+      if (limit && (IN || (gi >= 1 && gi <= ny - 1))) {
         if constexpr (!CH) {
           if (q > 0.0f)
             q = q * s_beta[a - 1][b];
@@ -472,7 +481,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
         }
         s_qy[a][b] = q;
       }
-      if (a == TY + 1 && gi != ny) continue;
+      if (a == TY + 1 && (IN || gi != ny)) continue;
       const size_t fid = (size_t)gi * nx + gj;
       qy_out[fid] = q;
       if constexpr (CH) {
@@ -490,7 +499,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
           p.qs_int_y[fid] = tot;
           p.qs_comp_y[fid] = comp;
         }
-      } else if (p.d50 != nullptr && gi >= 1 && gi <= ny - 1) {
+      } else if (p.d50 != nullptr && (IN || (gi >= 1 && gi <= ny - 1))) {
         const float eta_max = rmax(s_eta[a][b + 1], s_eta[a + 1][b + 1]);
         const float z_bank = rmax(s_z[a][b + 1], s_z[a + 1][b + 1]);
         const float h_face = eta_max - z_bank;
@@ -514,7 +523,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
   for (int k = threadIdx.x; k < TY * TX; k += NT) {
     const int r = k / TX, c = k - r * TX;
     const int gi = y0 + r, gj = x0 + c;
-    if (gi >= ny || gj >= nx) continue;
+    if (!IN && (gi >= ny || gj >= nx)) continue;
     const size_t id = (size_t)gi * nx + gj;
     const float qxl = s_qx[r + 1][c + 1], qxr = s_qx[r + 1][c + 2];
     const float qyt = s_qy[r + 1][c + 1], qyb = s_qy[r + 2][c + 1];
@@ -538,23 +547,24 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
       h = avail - inf;
       loss += (double)avail - (double)h;
     }
-    // boundaries.py:259-318, launched west, east, north, south.
-    if (p.bc[RB_EDGE_WEST] == RB_BC_OPEN && nx > 1 && gj == 0) {
+    // boundaries.py:259-318, launched west, east, north, south (no interior tile
+    // has a cell on an edge).
+    if (!IN && p.bc[RB_EDGE_WEST] == RB_BC_OPEN && nx > 1 && gj == 0) {
       const float avail = h;
       h = drain(avail, rmax(-qxr, 0.0f), dxdt);
       loss += (double)avail - (double)h;
     }
-    if (p.bc[RB_EDGE_EAST] == RB_BC_OPEN && nx > 1 && gj == nx - 1) {
+    if (!IN && p.bc[RB_EDGE_EAST] == RB_BC_OPEN && nx > 1 && gj == nx - 1) {
       const float avail = h;
       h = drain(avail, rmax(qxl, 0.0f), dxdt);
       loss += (double)avail - (double)h;
     }
-    if (p.bc[RB_EDGE_NORTH] == RB_BC_OPEN && ny > 1 && gi == 0) {
+    if (!IN && p.bc[RB_EDGE_NORTH] == RB_BC_OPEN && ny > 1 && gi == 0) {
       const float avail = h;
       h = drain(avail, rmax(-qyb, 0.0f), dxdt);
       loss += (double)avail - (double)h;
     }
-    if (p.bc[RB_EDGE_SOUTH] == RB_BC_OPEN && ny > 1 && gi == ny - 1) {
+    if (!IN && p.bc[RB_EDGE_SOUTH] == RB_BC_OPEN && ny > 1 && gi == ny - 1) {
       const float avail = h;
       h = drain(avail, rmax(qyt, 0.0f), dxdt);
       loss += (double)avail - (double)h;
@@ -583,7 +593,11 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
 template <int TX, int TY, int NT, bool CH, int MINB>
 __global__ void __launch_bounds__(NT, MINB) li_step_kernel(const LiParams p) {
   __shared__ LiSmem<TX, TY, CH> S;
-  li_tile<TX, TY, NT, CH>(p, blockIdx.x, blockIdx.y, (size_t)blockIdx.y * gridDim.x + blockIdx.x, S);
+  const size_t slot = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
+  if (li_deep_interior<TX, TY>(blockIdx.x * TX, blockIdx.y * TY, p.ny, p.nx))
+    li_tile<TX, TY, NT, CH, true>(p, blockIdx.x, blockIdx.y, slot, S);
+  else
+    li_tile<TX, TY, NT, CH, false>(p, blockIdx.x, blockIdx.y, slot, S);
 }
 
 template <int TX, int TY, int NT, bool CH, int MINB>
