@@ -37,11 +37,18 @@ namespace rb {
 RB_ARITH_BEGIN
 
 // hllc.py:158-165 _minmod
+#if defined(RB_FAST_MATH)
+// Fast arithmetic: minmod is the median of a, b and 0 (four min / max operations, no
+// compares). It differs from the reference's form only where a * b underflows to 0
+// for two same-signed slopes below 1e-19, and in the sign of a zero.
+__device__ __forceinline__ float minmod(float a, float b) { return fmaxf(fminf(a, b), fminf(fmaxf(a, b), 0.0f)); }
+#else
 __device__ __forceinline__ float minmod(float a, float b) {
   if (a * b <= 0.0f) return 0.0f;
   if (fabsf(a) < fabsf(b)) return a;
   return b;
 }
+#endif
 
 // hllc.py:174-188 _dryfactor
 __device__ __forceinline__ float dryfactor(float h0, float hm, float hp) {
@@ -85,6 +92,17 @@ __device__ __forceinline__ void hllc_flux(float hl, float ul, float vtl, float h
   const float fh_r = hr * ur;
   const float fmn_r = hr * ur * ur + 0.5f * g * hr * hr;
   float fh, fmn;
+#if defined(RB_FAST_MATH)
+  {
+    // Fast arithmetic: the three cases in one formula. With the wave speeds clamped
+    // to sl <= 0 <= sr, the HLL flux is the left flux when sl >= 0 and the right one
+    // when sr <= 0 (to rounding); sl < sr whenever one side is wet.
+    const float a = fminf(sl, 0.0f), b = fmaxf(sr, 0.0f);
+    const float inv = 1.0f / fmaxf(b - a, 1.0e-30f);
+    fh = (b * fh_l - a * fh_r + a * b * (hr - hl)) * inv;
+    fmn = (b * fmn_l - a * fmn_r + a * b * (hr * ur - hl * ul)) * inv;
+  }
+#else
   if (sl >= 0.0f) {
     fh = fh_l;
     fmn = fmn_l;
@@ -96,12 +114,19 @@ __device__ __forceinline__ void hllc_flux(float hl, float ul, float vtl, float h
     fh = (sr * fh_l - sl * fh_r + sl * sr * (hr - hl)) * inv;
     fmn = (sr * fmn_l - sl * fmn_r + sl * sr * (hr * ur - hl * ul)) * inv;
   }
+#endif
   // The contact speed s_star is read only through s_star >= 0 (hllc.py:231-238), so
   // its sign is decided without the division (quotient_nonneg).
   const float den_s = hr * (ur - sr) - hl * (ul - sl);
+#if defined(RB_FAST_MATH)
+  // fast arithmetic: the sign of the quotient from the sign of the product
+  const bool star_nonneg =
+      fabsf(den_s) > 1.0e-12f ? (sl * hr * (ur - sr) - sr * hl * (ul - sl)) * den_s >= 0.0f : ul + ur >= 0.0f;
+#else
   const bool star_nonneg = fabsf(den_s) > 1.0e-12f
                                ? quotient_nonneg(sl * hr * (ur - sr) - sr * hl * (ul - sl), den_s)
                                : 0.5f * (ul + ur) >= 0.0f;
+#endif
   const float vt = star_nonneg ? vtl : vtr;
   f0 = fh;
   f1 = fmn;
