@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -52,6 +53,14 @@ namespace rb {
 void set_last_error(const char* msg) { snprintf(g_err, sizeof g_err, "%s", msg); }
 
 int arith_mode() { return g_arith_mode.load(); }
+
+bool pdl_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("RBSIM_PDL");
+    return v == nullptr || std::strcmp(v, "0") != 0;
+  }();
+  return on;
+}
 
 // Argument checks shared by every entry point that takes a grid, edge kinds or a
 // timestep, so that all of them refuse the same inputs with the same messages.

@@ -145,7 +145,10 @@ __device__ void clock_plan(DevClock* c) {
   c->pending = 1;
 }
 
-__global__ void clock_plan_kernel(DevClock* c) { clock_plan(c); }
+__global__ void clock_plan_kernel(DevClock* c) {
+  pdl_enter();
+  clock_plan(c);
+}
 
 // One plan per domain of an ensemble (each domain has its own clock).
 __global__ void clock_plan_many_kernel(DevClock* clocks, int n) {
@@ -244,8 +247,7 @@ cudaError_t clock_inflow_launch(DevClock* clk, float* const* hb, cudaStream_t s)
 }
 
 cudaError_t clock_plan_launch(DevClock* clk, cudaStream_t s) {
-  clock_plan_kernel<<<1, 1, 0, s>>>(clk);
-  return cudaGetLastError();
+  return launch_chain(clock_plan_kernel, dim3(1), dim3(1), 0, s, clk);
 }
 
 cudaError_t clock_commit_launch(DevClock* clk, cudaStream_t s) {

@@ -969,6 +969,7 @@ __global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT) hllc_stage_kerne
   extern __shared__ __align__(16) unsigned char hllc_smem_raw[];
   using SMEM = typename HllcSmemOf<TX, TY, FU, LP>::type;
   auto& S = *reinterpret_cast<SMEM*>(hllc_smem_raw);
+  pdl_enter();
   const size_t slot = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
   if (hllc_deep_interior<TX, TY>(blockIdx.x * TX, blockIdx.y * TY, p.ny, p.nx))
     hllc_tile<TX, TY, NT, STAGE, FU, LP, true>(p, blockIdx.x, blockIdx.y, slot, S);
@@ -998,11 +999,8 @@ static cudaError_t launch_hllc(const HllcParams& p, int stage, cudaStream_t s) {
   static_assert(smem <= 227 * 1024, "tile does not fit in shared memory");
   prepare_hllc<TX, TY, NT, FU, LP>();
   const dim3 grid((p.nx + TX - 1) / TX, (p.ny + TY - 1) / TY);
-  if (stage == 1)
-    hllc_stage_kernel<TX, TY, NT, 1, FU, LP><<<grid, NT, smem, s>>>(p);
-  else
-    hllc_stage_kernel<TX, TY, NT, 2, FU, LP><<<grid, NT, smem, s>>>(p);
-  return cudaGetLastError();
+  return stage == 1 ? launch_chain(hllc_stage_kernel<TX, TY, NT, 1, FU, LP>, grid, dim3(NT), smem, s, p)
+                    : launch_chain(hllc_stage_kernel<TX, TY, NT, 2, FU, LP>, grid, dim3(NT), smem, s, p);
 }
 
 // The TMA-staged stage kernel: interior tiles copy their halo with tensor-memory
@@ -1012,6 +1010,7 @@ __global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT)
     hllc_stage_tma_kernel(const HllcParams p, const __grid_constant__ HllcMaps maps) {
   extern __shared__ __align__(1024) unsigned char hllc_tma_smem_raw[];
   auto& S = *reinterpret_cast<HllcSmemTma<TX, TY>*>(hllc_tma_smem_raw);
+  pdl_enter();
   const size_t slot = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
   if (hllc_deep_interior<TX, TY>(blockIdx.x * TX, blockIdx.y * TY, p.ny, p.nx))
     hllc_tile<TX, TY, NT, STAGE, 1, 2, true>(p, blockIdx.x, blockIdx.y, slot, S, &maps);
@@ -1028,6 +1027,7 @@ __global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT)
     hllc_stage_tma_pipe_kernel(const HllcParams p, const __grid_constant__ HllcMaps maps) {
   extern __shared__ __align__(1024) unsigned char hllc_pipe_smem_raw[];
   auto& S = *reinterpret_cast<HllcSmemTma<TX, TY>*>(hllc_pipe_smem_raw);
+  pdl_enter();
   if (p.clk != nullptr && !p.clk->active) return;  // no tile works this step
   const int cur = p.clk != nullptr ? p.clk->cur : p.cur;
   if (threadIdx.x == 0) {
@@ -1179,20 +1179,14 @@ static cudaError_t launch_hllc_tma(const HllcParams& p, int stage, cudaStream_t 
   if constexpr (PIPE) {
     const int resident = hllc_pipe_grid<TX, TY, NT>();
     if (resident == 0) return launch_hllc<TX, TY, NT, 1, 1>(p, stage, s);
-    const int grid = std::min(resident, tiles);
-    if (stage == 1)
-      hllc_stage_tma_pipe_kernel<TX, TY, NT, 1><<<grid, NT, smem, s>>>(p, m);
-    else
-      hllc_stage_tma_pipe_kernel<TX, TY, NT, 2><<<grid, NT, smem, s>>>(p, m);
-    return cudaGetLastError();
+    const dim3 grid(std::min(resident, tiles));
+    return stage == 1 ? launch_chain(hllc_stage_tma_pipe_kernel<TX, TY, NT, 1>, grid, dim3(NT), smem, s, p, m)
+                      : launch_chain(hllc_stage_tma_pipe_kernel<TX, TY, NT, 2>, grid, dim3(NT), smem, s, p, m);
   }
   prepare_hllc_tma<TX, TY, NT>();
   const dim3 grid((p.nx + TX - 1) / TX, (p.ny + TY - 1) / TY);
-  if (stage == 1)
-    hllc_stage_tma_kernel<TX, TY, NT, 1><<<grid, NT, smem, s>>>(p, m);
-  else
-    hllc_stage_tma_kernel<TX, TY, NT, 2><<<grid, NT, smem, s>>>(p, m);
-  return cudaGetLastError();
+  return stage == 1 ? launch_chain(hllc_stage_tma_kernel<TX, TY, NT, 1>, grid, dim3(NT), smem, s, p, m)
+                    : launch_chain(hllc_stage_tma_kernel<TX, TY, NT, 2>, grid, dim3(NT), smem, s, p, m);
 }
 
 // Kernel variants of the single-domain stage: tile, block size, faces per work item,

@@ -593,6 +593,7 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
 template <int TX, int TY, int NT, bool CH, int MINB>
 __global__ void __launch_bounds__(NT, MINB) li_step_kernel(const LiParams p) {
   __shared__ LiSmem<TX, TY, CH> S;
+  pdl_enter();
   const size_t slot = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
   if (li_deep_interior<TX, TY>(blockIdx.x * TX, blockIdx.y * TY, p.ny, p.nx))
     li_tile<TX, TY, NT, CH, true>(p, blockIdx.x, blockIdx.y, slot, S);
@@ -603,8 +604,7 @@ __global__ void __launch_bounds__(NT, MINB) li_step_kernel(const LiParams p) {
 template <int TX, int TY, int NT, bool CH, int MINB>
 static cudaError_t launch_li(const LiParams& p, cudaStream_t s) {
   const dim3 grid((p.nx + TX - 1) / TX, (p.ny + TY - 1) / TY);
-  li_step_kernel<TX, TY, NT, CH, MINB><<<grid, NT, 0, s>>>(p);
-  return cudaGetLastError();
+  return launch_chain(li_step_kernel<TX, TY, NT, CH, MINB>, grid, dim3(NT), 0, s, p);
 }
 
 // Tile variants of the single-domain step (sub-grid channels always use 32 x 16);

@@ -217,4 +217,38 @@ __device__ __forceinline__ void flag_error(unsigned int* err, unsigned int bit) 
 }
 
 RB_ARITH_END
+
+// Programmatic dependent launch of the step chain (plan -> stage 1 -> stage 2 ->
+// plan ..., or plan -> LI step -> plan ...). Each kernel of the chain first lets the
+// next kernel of the stream be scheduled (it launches once every block of this grid
+// has begun, so its blocks take the SM slots this grid's last wave frees), then
+// waits until the kernel before it has completed with its memory visible, before it
+// reads anything. A kernel launched without the attribute does not start early, and
+// for it the wait returns at once.
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
+// Whether the step chain is launched with programmatic stream serialization
+// (default on; RBSIM_PDL=0 in the environment turns it off, for comparison).
+bool pdl_enabled();
+
+// Launch a kernel of the step chain, with the programmatic-serialization attribute
+// when pdl_enabled(). The kernel must begin with pdl_enter().
+template <class... Params, class... Args>
+cudaError_t launch_chain(void (*kernel)(Params...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                         Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = pdl_enabled() ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, kernel, static_cast<Args&&>(args)...);
+}
 }  // namespace rb
