@@ -673,7 +673,11 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 3 : 6) ens_li_kernel(const LiP
       reinterpret_cast<unsigned*>(&sp)[threadIdx.x] = reinterpret_cast<const unsigned*>(P + m.x)[threadIdx.x];
     __syncthreads();
     const int tiles_x = (sp.nx + TX - 1) / TX;
-    li_tile<TX, TY, NT>(sp, m.y % tiles_x, m.y / tiles_x, (size_t)m.y, S);
+    const int bx = m.y % tiles_x, by = m.y / tiles_x;
+    if (li_deep_interior<TX, TY>(bx * TX, by * TY, sp.ny, sp.nx))
+      li_tile<TX, TY, NT, false, true>(sp, bx, by, (size_t)m.y, S);
+    else
+      li_tile<TX, TY, NT, false, false>(sp, bx, by, (size_t)m.y, S);
   }
 }
 
