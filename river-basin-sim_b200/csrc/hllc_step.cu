@@ -409,8 +409,12 @@ __device__ __forceinline__ bool hllc_deep_interior(int x0, int y0, int ny, int n
 // copies from the tensor maps in `maps` (edge tiles take the LP 1 path); LP 3 does
 // the same for a persistent block whose next tile's copies complete barrier phase
 // `phase`. IN is the instantiation for a tile hllc_deep_interior admits, without the
-// bounds checks and edge cases. Every choice computes the same bits.
-template <int TX, int TY, int NT, int STAGE, int FU = 1, int LP = 1, bool IN = false, class SMEM = HllcSmem<TX, TY>>
+// bounds checks and edge cases. SRC says whether stage 2 has per-cell sources (the
+// compensated rain's h_comp, a rain field, infiltration): 0 no, 1 yes, 2 read from
+// the pointers at run time; uniform rain is in every instantiation. Every choice
+// computes the same bits.
+template <int TX, int TY, int NT, int STAGE, int FU = 1, int LP = 1, bool IN = false, int SRC = 2,
+          class SMEM = HllcSmem<TX, TY>>
 __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, size_t slot, SMEM& S,
                                           const HllcMaps* maps = nullptr, unsigned phase = 0) {
   static_assert(NT / 32 <= 32, "reduction scratch sized for <= 32 warps");
@@ -908,14 +912,14 @@ __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, s
           }
         }
       }
-      if (rain_mode == 1) {
+      if (SRC != 0 && rain_mode == 1) {
         float comp = p.h_comp[id];
         kahan_add(hh, comp, rain32 * dt);
         p.h_comp[id] = comp;
       } else if (rain_mode == 2) {
         hh = hh + rain32 * dt;  // hllc.py:942-945
       }
-      if (p.rain_field != nullptr) {
+      if (SRC != 0 && p.rain_field != nullptr) {
         if (p.h_comp != nullptr) {
           float comp = p.h_comp[id];
           kahan_add(hh, comp, p.rain_field[id] * scale32 * dt);
@@ -924,7 +928,7 @@ __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, s
           hh = hh + p.rain_field[id] * scale32 * dt;
         }
       }
-      if (p.infil != nullptr) {  // local_inertial.py:170-194
+      if (SRC != 0 && p.infil != nullptr) {  // local_inertial.py:170-194
         const float avail = hh;
         float inf = p.infil[id] * dt;
         if (inf > avail) inf = avail;
@@ -964,7 +968,7 @@ __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, s
 // more than the 48 KB a static array may take); __launch_bounds__ asks for two
 // resident blocks of 512 threads or more (four of 256) per SM: at most 64 registers
 // a thread for 512, 51 for 640.
-template <int TX, int TY, int NT, int STAGE, int FU, int LP>
+template <int TX, int TY, int NT, int STAGE, int FU, int LP, int SRC>
 __global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT) hllc_stage_kernel(const HllcParams p) {
   extern __shared__ __align__(16) unsigned char hllc_smem_raw[];
   using SMEM = typename HllcSmemOf<TX, TY, FU, LP>::type;
@@ -972,9 +976,9 @@ __global__ void __launch_bounds__(NT, NT > 512 ? 2 : 1024 / NT) hllc_stage_kerne
   pdl_enter();
   const size_t slot = (size_t)blockIdx.y * gridDim.x + blockIdx.x;
   if (hllc_deep_interior<TX, TY>(blockIdx.x * TX, blockIdx.y * TY, p.ny, p.nx))
-    hllc_tile<TX, TY, NT, STAGE, FU, LP, true>(p, blockIdx.x, blockIdx.y, slot, S);
+    hllc_tile<TX, TY, NT, STAGE, FU, LP, true, SRC>(p, blockIdx.x, blockIdx.y, slot, S);
   else
-    hllc_tile<TX, TY, NT, STAGE, FU, LP, false>(p, blockIdx.x, blockIdx.y, slot, S);
+    hllc_tile<TX, TY, NT, STAGE, FU, LP, false, SRC>(p, blockIdx.x, blockIdx.y, slot, S);
 }
 
 // The shared-memory opt-in is a per-device function attribute: set once per device
@@ -987,8 +991,12 @@ static void prepare_hllc() {
   cudaGetDevice(&dev);
   const unsigned long long bit = 1ull << (dev & 63);
   if (!(attr_set.load() & bit)) {
-    cudaFuncSetAttribute(hllc_stage_kernel<TX, TY, NT, 1, FU, LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaFuncSetAttribute(hllc_stage_kernel<TX, TY, NT, 2, FU, LP>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaFuncSetAttribute(hllc_stage_kernel<TX, TY, NT, 1, FU, LP, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         smem);
+    cudaFuncSetAttribute(hllc_stage_kernel<TX, TY, NT, 2, FU, LP, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         smem);
+    cudaFuncSetAttribute(hllc_stage_kernel<TX, TY, NT, 2, FU, LP, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         smem);
     attr_set.fetch_or(bit);
   }
 }
@@ -999,8 +1007,11 @@ static cudaError_t launch_hllc(const HllcParams& p, int stage, cudaStream_t s) {
   static_assert(smem <= 227 * 1024, "tile does not fit in shared memory");
   prepare_hllc<TX, TY, NT, FU, LP>();
   const dim3 grid((p.nx + TX - 1) / TX, (p.ny + TY - 1) / TY);
-  return stage == 1 ? launch_chain(hllc_stage_kernel<TX, TY, NT, 1, FU, LP>, grid, dim3(NT), smem, s, p)
-                    : launch_chain(hllc_stage_kernel<TX, TY, NT, 2, FU, LP>, grid, dim3(NT), smem, s, p);
+  // stage 1 has no sources; stage 2 carries their code only when one is armed
+  if (stage == 1) return launch_chain(hllc_stage_kernel<TX, TY, NT, 1, FU, LP, 0>, grid, dim3(NT), smem, s, p);
+  const bool src = p.h_comp != nullptr || p.rain_field != nullptr || p.infil != nullptr;
+  return src ? launch_chain(hllc_stage_kernel<TX, TY, NT, 2, FU, LP, 1>, grid, dim3(NT), smem, s, p)
+             : launch_chain(hllc_stage_kernel<TX, TY, NT, 2, FU, LP, 0>, grid, dim3(NT), smem, s, p);
 }
 
 // The TMA-staged stage kernel: interior tiles copy their halo with tensor-memory
