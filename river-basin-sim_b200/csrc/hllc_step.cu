@@ -952,7 +952,10 @@ __device__ __forceinline__ bool hllc_tile(const HllcParams& p, int bx, int by, s
     }
   }
 
-  if (p.ledger != nullptr) {
+  // An interior tile banks nothing but infiltration (it has no edge face), so without
+  // infiltration its loss is 0 and its slot, zero from the start, stays exactly 0:
+  // the block sum is skipped.
+  if (p.ledger != nullptr && (!IN || (STAGE == 2 && SRC != 0 && p.infil != nullptr))) {
     const double s = block_sum<NT>(loss, s_red);
     if (threadIdx.x == 0) ledger_add(p.ledger + 2 * slot, s);
   }

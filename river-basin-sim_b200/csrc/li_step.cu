@@ -646,7 +646,10 @@ __device__ __forceinline__ void li_tile(const LiParams& p, int bx, int by, size_
     bad |= !(fabsf(h) <= FLT_MAX);
   }
 
-  if (p.ledger != nullptr) {
+  // An interior tile banks nothing but infiltration (no cell of it drains through an
+  // edge), so without infiltration its loss is 0 and its slot, zero from the start,
+  // stays exactly 0: the block sum is skipped.
+  if (p.ledger != nullptr && (!IN || p.infil != nullptr)) {
     const double s = block_sum<NT>(loss, s_red);
     if (threadIdx.x == 0) ledger_add(p.ledger + 2 * slot, s);
   }
