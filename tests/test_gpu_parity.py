@@ -133,6 +133,18 @@ def test_hllc_seeded_grids_match_oracle_bitwise(shape):
     _compare(run_case(case, GpuAPI()), _oracle_outputs(case), f"hllc{shape}")
 
 
+def test_li_open_edges_without_infiltration_match_oracle_bitwise():
+    """Open edges bank their outflow in the float64 ledger; without infiltration an
+    interior tile banks nothing, and its block sum is skipped. 300 x 420 has 80 interior
+    tiles of 32 x 32 between edge tiles that bank, and the banked total must still be
+    the oracle's."""
+    from gpu_api import GpuAPI
+
+    case = _synthetic_li(300, 420, seed=21)
+    del case["infil"]
+    _compare(run_case(case, GpuAPI()), _oracle_outputs(case), "li(300, 420) without infiltration")
+
+
 def test_li_config_scale_512_matches_oracle_bitwise():
     """The 512 x 512 rain-on-grid configuration shape, 60 steps."""
     from gpu_api import GpuAPI
