@@ -1264,6 +1264,12 @@ cudaError_t hllc_stage_launch(const HllcParams& p, int stage, cudaStream_t s) {
 cudaError_t hllc_stage_launch_variant(const HllcParams& p, int stage, int variant, cudaStream_t s) {
 #if !defined(RB_FAST_MATH)
   if (arith_mode() == RB_ARITH_FAST) return fast::hllc_stage_launch_variant(p, stage, variant, s);
+  return hllc_stage_launch_exact(p, stage, variant, s);
+}
+
+// This build's stage kernel whatever the arithmetic mode (the exact build: what the
+// ensembles, which run exact arithmetic only, launch for their large domains).
+cudaError_t hllc_stage_launch_exact(const HllcParams& p, int stage, int variant, cudaStream_t s) {
 #endif
   switch (variant) {
     case 1: return launch_hllc<32, 16, 256, 1, 1>(p, stage, s);

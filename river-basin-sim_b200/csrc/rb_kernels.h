@@ -137,6 +137,8 @@ int hllc_tiles(int ny, int nx);
 int hllc_current_variant();
 int hllc_tiles_of(int variant, int ny, int nx);
 cudaError_t hllc_stage_launch_variant(const HllcParams& p, int stage, int variant, cudaStream_t s);
+// The exact build's stage kernel regardless of the arithmetic mode.
+cudaError_t hllc_stage_launch_exact(const HllcParams& p, int stage, int variant, cudaStream_t s);
 int li_kernel_variant_count();
 bool li_set_kernel_variant(int v);
 int hllc_kernel_variant_count();

@@ -70,6 +70,44 @@ def test_members_equal_solo_runs(variants):
             assert st.loss_cum.total() == pytest.approx(loss, rel=1e-12)
 
 
+LARGE_SPECS = [  # at least 1024 tiles of 32 x 32: stepped by the single-domain kernels
+    ("local_inertial", 1024, 1100, 10.0, 300.0, 2e-5),
+    ("hllc_fv", 1024, 1056, 1.0, 1.0, 0.0),
+    ("local_inertial", 96, 130, 10.0, 400.0, 2e-5),
+    ("hllc_fv", 45, 77, 2.0, 5.0, 1e-4),
+]
+
+
+def test_large_members_on_the_single_domain_kernels_equal_solo_runs():
+    """Members of 1024 tiles or more run the single-domain kernels inside the ensemble's
+    step (launched per member), the others the persistent kernels; every member still
+    equals its run alone, bit for bit."""
+    from rbsim.device_clock import DeviceClock
+    from rbsim.ensemble import Ensemble
+
+    alpha = {"local_inertial": 0.7, "hllc_fv": 0.45}
+    solo = []
+    for k, (sch, ny, nx, dx, hz, rain) in enumerate(LARGE_SPECS):
+        st = _member(sch, ny, nx, dx, seed=60 + k)
+        clk = DeviceClock(st, sch, alpha=alpha[sch], dt_max=30.0, sync_times=[hz], rain_rate=rain,
+                          rain_until=hz, graph_steps=16)  # fmt: skip
+        clk.run_until(hz)
+        solo.append((st.h.cpu().numpy(), clk.steps, st.loss_cum.total() if st.loss_cum is not None else 0.0))
+        clk.close()
+        del st
+    members = [_member(sch, ny, nx, dx, seed=60 + k) for k, (sch, ny, nx, dx, _, _) in enumerate(LARGE_SPECS)]
+    ens = Ensemble(members, [s[0] for s in LARGE_SPECS], alpha=[alpha[s[0]] for s in LARGE_SPECS], dt_max=30.0,
+                   sync_times=[[s[4]] for s in LARGE_SPECS], rain_rate=[s[5] for s in LARGE_SPECS],
+                   rain_until=[s[4] for s in LARGE_SPECS], li_variant=3, hllc_variant=2,
+                   graph_steps=8)  # fmt: skip
+    ens.run_until([s[4] for s in LARGE_SPECS])
+    for k, (st, (h, steps, loss)) in enumerate(zip(members, solo, strict=True)):
+        assert ens.clock[k].steps == steps, k
+        np.testing.assert_array_equal(st.h.cpu().numpy(), h, err_msg=f"member {k}")
+        if loss:
+            assert st.loss_cum.total() == pytest.approx(loss, rel=1e-12)
+
+
 def test_autotune_picks_a_candidate_and_keeps_results_exact():
     from rbsim.device_clock import DeviceClock
     from rbsim.ensemble import Ensemble, autotune
