@@ -4,7 +4,9 @@ Each member is an ordinary ``State`` (local inertial or HLLC) with its own
 workspace, rain and horizon; the ensemble gives every member its own device clock
 and steps all of them with one persistent kernel per scheme over a (domain, tile)
 work-list (librbsim ``rb_ensemble_*``), ``graph_steps`` ensemble steps per CUDA
-graph replay. A member's arithmetic is that of its single-domain step, so its
+graph replay. A member of 1024 tiles of 32 x 32 or more fills the GPU by itself and
+is stepped by the single-domain kernels, launched for it alone in the same step
+(faster than the persistent kernels at that size on B200). A member's arithmetic is that of its single-domain step, so its
 result is bit-identical to running it alone; members that reach their target stop
 (their tiles return immediately) while the others continue.
 

@@ -4,7 +4,8 @@ Requests (scheme, grid side, horizon, seeded synthetic terrain, optional Exner
 morphology) arrive over wall-clock time. The server admits them in arrival order
 while the HBM they need fits the budget, keeps every admitted solve resident, and
 steps all of them together as one ``Ensemble`` (one persistent kernel per scheme
-over every member's tiles, each member on its own device clock). Between graph
+over the members' tiles, the single-domain kernels for members large enough to fill
+the GPU alone; each member on its own device clock). Between graph
 replays it retires finished solves (their results at once; a finished member stays
 in the batch, idle, until the next rebuild -- an admission, or finished members
 holding most of the batch's cells -- frees its memory), runs due slow processes
