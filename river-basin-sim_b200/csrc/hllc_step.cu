@@ -1329,21 +1329,23 @@ __global__ void __launch_bounds__(NT, 768 / NT) ens_hllc_kernel(const HllcParams
   ens_hllc_items<TX, TY, NT, STAGE>(P, map, total, S, sp);
 }
 
-// The 32 x 32 tile of the single-domain default, with its shared memory (more than a
-// static array may take) dynamic: the tile, then the staged parameters. 512 threads
-// and two blocks per SM measured faster than 640 (whose 51-register bound spills
-// here): 9.9 Gcell-updates/s for 4 domains of 2048 x 2048 against 9.2 for the 32 x 16
-// variant.
-constexpr int kEnsWideNT = 512;
-constexpr size_t kEnsWideParamsAt = (sizeof(HllcSmem<32, 32>) + 15) / 16 * 16;
-constexpr size_t kEnsWideSmem = kEnsWideParamsAt + sizeof(HllcParams);
+// The 32 x 32 tile of the single-domain default as a plain grid: one block of 640
+// threads per (domain, tile) work item, the domain's parameters read from global
+// memory (shared memory, more than a static array may take, is dynamic). Measured
+// against a persistent form of the same tile (512 threads, parameters staged in
+// shared memory, which spilled at its 64-register bound): 11.4 vs 9.4
+// Gcell-updates/s on dam breaks of 8 x 512^2, 16 x 256^2 and 2 x 768^2.
+constexpr int kEnsWideNT = 640;
+constexpr size_t kEnsWideSmem = sizeof(HllcSmem<32, 32>);
 template <int STAGE>
 __global__ void __launch_bounds__(kEnsWideNT, 2) ens_hllc_wide_kernel(const HllcParams* __restrict__ P,
-                                                                     const int2* __restrict__ map, long long total) {
+                                                                     const int2* __restrict__ map) {
   extern __shared__ __align__(16) unsigned char ens_wide_smem[];
   auto& S = *reinterpret_cast<HllcSmem<32, 32>*>(ens_wide_smem);
-  auto& sp = *reinterpret_cast<HllcParams*>(ens_wide_smem + kEnsWideParamsAt);
-  ens_hllc_items<32, 32, kEnsWideNT, STAGE>(P, map, total, S, sp);
+  const int2 m = map[blockIdx.x];
+  const HllcParams& p = P[m.x];
+  const int tiles_x = (p.nx + 31) / 32;
+  hllc_tile<32, 32, kEnsWideNT, STAGE>(p, m.y % tiles_x, m.y / tiles_x, (size_t)m.y, S);
 }
 
 template <int TX, int TY, int NT>
@@ -1356,8 +1358,8 @@ static int ens_hllc_grid() {
 }
 
 // Sets the wide kernel's shared-memory opt-in on the current device (outside any
-// stream capture: called while an ensemble is initialised) and sizes its grid; 0
-// when the device refuses the opt-in or cannot hold one block.
+// stream capture: called while an ensemble is initialised); 0 when the device refuses
+// the opt-in or cannot hold one block (its launches are one block per work item).
 static int ens_hllc_wide_grid() {
   int dev = 0, sms = 0, per_sm = 0;
   cudaGetDevice(&dev);
@@ -1390,11 +1392,11 @@ cudaError_t ens_hllc_launch(int variant, int grid, int stage, const HllcParams* 
                             cudaStream_t s) {
   if (total <= 0) return cudaSuccess;
   const int g = (int)(total < grid ? total : grid);
-  if (variant == 2) {
+  if (variant == 2) {  // one block per work item
     if (stage == 1)
-      ens_hllc_wide_kernel<1><<<g, kEnsWideNT, kEnsWideSmem, s>>>(P, map, total);
+      ens_hllc_wide_kernel<1><<<(unsigned)total, kEnsWideNT, kEnsWideSmem, s>>>(P, map);
     else
-      ens_hllc_wide_kernel<2><<<g, kEnsWideNT, kEnsWideSmem, s>>>(P, map, total);
+      ens_hllc_wide_kernel<2><<<(unsigned)total, kEnsWideNT, kEnsWideSmem, s>>>(P, map);
   } else if (variant == 1) {
     if (stage == 1)
       ens_hllc_kernel<32, 8, 256, 1><<<g, 256, 0, s>>>(P, map, total);

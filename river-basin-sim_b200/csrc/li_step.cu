@@ -754,6 +754,22 @@ __global__ void __launch_bounds__(NT, NT >= 512 ? 3 : 6) ens_li_kernel(const LiP
   }
 }
 
+// The 32 x 32 tile as a plain grid: one block per (domain, tile) work item, the
+// domain's parameters read from global memory, three resident blocks of 512 threads
+// per SM as in the single-domain step.
+__global__ void __launch_bounds__(512, 3) ens_li_grid_kernel(const LiParams* __restrict__ P,
+                                                             const int2* __restrict__ map) {
+  __shared__ LiSmem<32, 32> S;
+  const int2 m = map[blockIdx.x];
+  const LiParams& p = P[m.x];
+  const int tiles_x = (p.nx + 31) / 32;
+  const int bx = m.y % tiles_x, by = m.y / tiles_x;
+  if (li_deep_interior<32, 32>(bx * 32, by * 32, p.ny, p.nx))
+    li_tile<32, 32, 512, false, true>(p, bx, by, (size_t)m.y, S);
+  else
+    li_tile<32, 32, 512, false, false>(p, bx, by, (size_t)m.y, S);
+}
+
 template <int TX, int TY, int NT>
 static int ens_li_grid() {
   int dev = 0, sms = 0, per_sm = 0;
@@ -785,7 +801,7 @@ cudaError_t ens_li_launch(int variant, int grid, const LiParams* P, const int2* 
   switch (variant) {
     case 1: ens_li_kernel<32, 8, 256><<<g, 256, 0, s>>>(P, map, total); break;
     case 2: ens_li_kernel<64, 8, 256><<<g, 256, 0, s>>>(P, map, total); break;
-    case 3: ens_li_kernel<32, 32, 512><<<g, 512, 0, s>>>(P, map, total); break;
+    case 3: ens_li_grid_kernel<<<(unsigned)total, 512, 0, s>>>(P, map); break;  // one block per work item
     default: ens_li_kernel<32, 16, 256><<<g, 256, 0, s>>>(P, map, total); break;
   }
   return cudaGetLastError();

@@ -27,7 +27,7 @@ from . import _lib, graphs
 from .state import State
 
 LI_VARIANTS = (0, 1, 2, 3)  # tiles 32x16, 32x8, 64x8, 32x32 (512 threads)
-HLLC_VARIANTS = (0, 1, 2)  # tiles 32x16, 32x8 (256 threads), 32x32 (512 threads)
+HLLC_VARIANTS = (0, 1, 2)  # tiles 32x16, 32x8 (256 threads, persistent), 32x32 (640 threads, one block per tile)
 
 
 class Ensemble:
