@@ -316,8 +316,8 @@ __device__ __forceinline__ unsigned smem_addr(const void* ptr) {
   return static_cast<unsigned>(__cvta_generic_to_shared(ptr));
 }
 
-// One 2-D tile copy global -> this CTA's shared memory, completing on `bar`. No
-// multicast: every copy reads this GPU's own memory into its own CTA.
+// One 2-D tile copy global -> this CTA's shared memory, completing on `bar`. Every
+// copy reads this GPU's own memory into the issuing CTA alone.
 __device__ __forceinline__ void tma_load_tile(void* dst, const TileMap* map, int x, int y, unsigned long long* bar) {
   asm volatile(
       "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::"r"(
