@@ -117,6 +117,28 @@ class OracleBackend:
     def cell_area(self, st):
         return st.dx * st.dx
 
+    def fill_span(self, span, dt_raw):
+        return self.o.fill_span(span, dt_raw)
+
+    def arm_sediment(self, st, d50, porosity):
+        st.arm_sediment(d50, porosity)
+
+    def morphology(self, st, interval_s, dz_lo, dz_hi):
+        """An object whose ``advance(t, dt_slow)`` applies one Exner activation."""
+        o = self.o
+
+        class _Morph:
+            def advance(self, t, dt_slow):
+                o.exner_activate(st, dz_lo, dz_hi)
+
+        return _Morph()
+
+    def z(self, st):
+        return st.z.copy()
+
+    def dz_cum(self, st):
+        return st.sediment.dz_cum.copy()
+
 
 class GpuBackend:
     name = "cuda"
@@ -215,6 +237,27 @@ class GpuBackend:
 
     def cell_area(self, st):
         return st.grid.cell_area
+
+    def fill_span(self, span, dt_raw):
+        from rbsim.scheduler import fill_span
+
+        return fill_span(span, dt_raw)
+
+    def arm_sediment(self, st, d50, porosity):
+        from rbsim.sediment import arm_sediment
+
+        arm_sediment(st, d50, porosity)
+
+    def morphology(self, st, interval_s, dz_lo, dz_hi):
+        from rbsim.processes.morphology import MorphologyProcess
+
+        return MorphologyProcess(st, interval_s, dz_lo=dz_lo, dz_hi=dz_hi)
+
+    def z(self, st):
+        return st.z.cpu().numpy()
+
+    def dz_cum(self, st):
+        return st.sediment.dz_cum.cpu().numpy()
 
 
 def flat(n, depth, be, dx=100.0):
