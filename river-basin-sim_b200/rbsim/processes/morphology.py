@@ -94,7 +94,9 @@ class MorphologyProcess:
     def advance(self, t: float, dt_slow: float) -> BedChangeRecord:
         if dt_slow > self.interval_s * (1.0 + 1e-6) + EPS_T:
             raise SedimentError(
-                f"morphology was handed {dt_slow} s to apply but is configured for {self.interval_s} s"
+                f"morphology was handed {dt_slow} s to apply but is configured for {self.interval_s} s: "
+                "several intervals collapsed into one bed update coarsen the operator splitting, "
+                "and no balance would show it"
             )
         st, sed, g = self.state, self.sediment, self.state.grid
         prev_dz = sed.dz_cum.clone()
