@@ -1,12 +1,14 @@
-"""The reference's edge gates for the HLLC scheme, re-expressed against a backend.
+"""The reference's edge gates, re-expressed against a backend.
 
 These restate ``validation/test_fixed_stage.py`` (the prescribed-stage ghost: inert
 at equilibrium, a source that fills a dry domain from each edge, a sink that drains
 into the limiter regime with exact banking, tracking a time-varying level) and
 ``validation/test_hllc_boundaries.py`` (each open edge drains its own way, a full
 drain to empty under the mass gate, a closed wall that reflects a moving slab, and a
-steady channel at its Manning normal depth). The thresholds are the reference
-tests'. The drivers are this build's own.
+steady channel at its Manning normal depth), and the local-inertial half of
+``validation/test_channel_flow.py`` (an open edge that never over-drains, a channel
+near normal depth). The thresholds are the reference tests'. The drivers are this
+build's own.
 
 ``EDGE_GATES`` maps a name to a gate that takes a backend from tests/backends.py.
 """
@@ -287,6 +289,58 @@ def gate_hllc_channel_normal_depth(be):
     assert np.isfinite(h).all() and h.min() > H_DRY
     assert led.max_rel_error < MASS_GATE and rec.outflow_cum > 0.0
     assert abs(float(np.median(h[10 : nx - 10])) - h_n) < 0.02 * h_n
+
+
+# --- the local-inertial open edge (validation/test_channel_flow.py) ------------- #
+LI = "local_inertial"
+
+
+def gate_li_open_edge_drains_and_stays_nonnegative(be):
+    """validation/test_channel_flow.py:38 -- a 2 % basin open to the east, 2000 steps.
+
+    The capped edge sink cannot over-drain: depth never below -1e-6 m, mass closed,
+    more than half the water out through the edge.
+    """
+    ny, nx, dx = 20, 40, 10.0
+    st = be.make(_sloped(ny, nx, dx, "east", 0.02), dx, depth=0.5, manning=0.03)
+    be.set_bc(st, _only("east", "open"))
+    led = be.ledger(st)
+    t = 0.0
+    for _ in range(2000):
+        dt = be.compute_dt(st, LI, 0.7, 5.0)
+        be.step(st, LI, dt)
+        t += dt
+    rec = led.record(st, t)
+    h = be.h(st)
+    assert np.isfinite(h).all() and h.min() >= -1e-6
+    assert led.max_rel_error < MASS_GATE
+    assert rec.outflow_cum > 0.5 * led.v0 and rec.volume < 0.5 * led.v0
+
+
+def gate_li_channel_normal_depth(be):
+    """validation/test_channel_flow.py:70 -- a mild 1 x 80 channel settles near Manning normal depth.
+
+    The local-inertial scheme is diffusive, so the bar is the reference's: the
+    interior median within [0.5, 2] x (q n / sqrt(S))^(3/5) after 4000 steps, water
+    leaving the toe, mass closed.
+    """
+    nx, dx, slope, n, discharge = 80, 10.0, 0.001, 0.03, 2.0
+    bed = ((nx - 1 - np.arange(nx)) * dx * slope).reshape(1, nx).astype(np.float32)
+    st = be.make(bed, dx, depth=0.0, manning=n)
+    be.set_bc(st, _only("east", "open"))
+    inj = be.injector([((0, 0), [(0.0, discharge), (1.0e9, discharge)])], st)
+    led = be.ledger(st)
+    t = 0.0
+    for _ in range(4000):
+        dt = be.compute_dt(st, LI, 0.7, 10.0)
+        led.add_inflow(inj.apply(st, t, dt))
+        be.step(st, LI, dt)
+        t += dt
+    rec = led.record(st, t)
+    h_n = (discharge / dx * n / math.sqrt(slope)) ** 0.6
+    median = float(np.median(be.h(st)[0][5 : nx - 5]))
+    assert led.max_rel_error < MASS_GATE and rec.outflow_cum > 0.0
+    assert 0.5 * h_n < median < 2.0 * h_n, (median, h_n)
 
 
 EDGE_GATES = {
