@@ -162,8 +162,13 @@ def _field(value, base: Path, shape, name):
 
 def load_config(path) -> Scenario:
     path = Path(path)
-    with open(path, "rb") as f:
-        doc = tomllib.load(f)
+    try:
+        with open(path, "rb") as f:
+            doc = tomllib.load(f)
+    except FileNotFoundError as e:  # both refusals are ConfigError, as config.py:791-797 raises them
+        raise ConfigError(f"scenario config not found: {path}") from e
+    except tomllib.TOMLDecodeError as e:
+        raise ConfigError(f"{path} is not valid TOML: {e}") from e
     base = path.parent
     for t in _UNSUPPORTED:
         if t in doc:

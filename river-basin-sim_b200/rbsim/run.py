@@ -234,12 +234,18 @@ def main(argv=None) -> int:
     ap.add_argument("--status", default=None)
     ap.add_argument("--host-loop", action="store_true", help="step through compute_dt/step on the host")
     args = ap.parse_args(argv)
-    sc = load_config(args.config)
-    out = args.out or str(Path(args.config).with_suffix(".zarr").name)
-    status = StatusWriter(args.status, sc.end_time) if args.status else None
+    # The status channel opens before anything that can fail, the config included, so a
+    # viewer polling it sees state "error" rather than a file that never appears. Its
+    # end time is set once the scenario is known.
+    status = StatusWriter(args.status, 1.0) if args.status else None
     try:
         if status:
-            status.write("starting")
+            status.write("starting", message="reading the scenario")
+        sc = load_config(args.config)
+        out = args.out or str(Path(args.config).with_suffix(".zarr").name)
+        if status:
+            status.end_time = float(sc.end_time)
+            status.write("starting", message=sc.name)
         t0 = time.time()
         run_simulation(sc, None, out, status=status, use_device_clock=not args.host_loop)
         if status:

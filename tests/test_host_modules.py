@@ -220,3 +220,33 @@ def test_config_loader(tmp_path):
                    'release_m3_s = 2.0\npool = [0, 0, 2, 4]\noutlet = [1, 2]\n')
     with pytest.raises(ConfigError, match="overlaps the pool"):
         load_config(bad)
+
+
+def test_main_writes_error_status_on_bad_config(tmp_path):
+    """solver/test_run.py:142: a config the loader refuses is reported through status.json
+    (state "error", the loader's message) and re-raised, so a polling viewer does not wait forever."""
+    from rbsim.config import ConfigError
+    from rbsim.run import main
+
+    cfg = tmp_path / "bad.toml"
+    cfg.write_text("[rainfall]\ntype = 'storm_cells'\n", encoding="utf-8")
+    status = tmp_path / "status.json"
+    with pytest.raises(ConfigError):
+        main(["--config", str(cfg), "--out", str(tmp_path / "out.zarr"), "--status", str(status)])
+    rec = json.loads(status.read_text(encoding="utf-8"))
+    assert rec["state"] == "error" and "storm_cells" in rec["message"]
+    with pytest.raises(ConfigError, match="not found"):
+        main(["--config", str(tmp_path / "missing.toml"), "--status", str(status)])
+    assert json.loads(status.read_text(encoding="utf-8"))["state"] == "error"
+
+
+def test_a_config_that_cannot_be_read_is_a_config_error(tmp_path):
+    """solver/io/test_config.py:316, and a file that is not TOML."""
+    from rbsim.config import ConfigError, load_config
+
+    with pytest.raises(ConfigError, match="not found"):
+        load_config(tmp_path / "nope.toml")
+    broken = tmp_path / "broken.toml"
+    broken.write_text("[grid\ndx = ", encoding="utf-8")
+    with pytest.raises(ConfigError, match="not valid TOML"):
+        load_config(broken)
