@@ -11,6 +11,7 @@ outside this build's path.
 from __future__ import annotations
 
 import tomllib
+import warnings
 from dataclasses import dataclass, field
 from pathlib import Path
 
@@ -129,6 +130,43 @@ class Scenario:
     channel_manning: float | np.ndarray | None = None  # None: the floodplain roughness
     structures: list = field(default_factory=list)
     bed: np.ndarray | None = None
+
+    def __post_init__(self) -> None:
+        self.validate()
+
+    def validate(self) -> None:
+        """Refuse run parameters no run can honour (config.py:357-498); ``load_config``
+        calls it again once every table is read, so both construction paths are checked.
+
+        Raises ValueError (``load_config`` re-raises it as ConfigError) and warns above
+        the CFL number the local-inertial scheme is stable at.
+        """
+        for name, v in (("end_time", self.end_time), ("output_every", self.output_every), ("dt_max", self.dt_max),
+                        ("cfl", self.alpha)):  # fmt: skip
+            if not v > 0:
+                raise ValueError(f"{name} must be > 0, got {v}")
+        frames = self.end_time / self.output_every
+        if abs(frames - round(frames)) > 1e-6:
+            raise ValueError(f"end_time ({self.end_time}) must be a whole multiple of output_every "
+                             f"({self.output_every}): frames land on its multiples, so the state at end_time "
+                             "would never be written")  # fmt: skip
+        for name, v in (("manning_n", self.manning), ("infiltration", self.infiltration_mm_hr),
+                        ("rainfall rate", self.rain_mm_hr), ("rainfall duration", self.rain_duration)):  # fmt: skip
+            if np.any(np.asarray(v) < 0):
+                raise ValueError(f"{name} must be >= 0")
+        unknown = sorted(f"{e}={v!r}" for e, v in self.boundaries.items() if v not in ("closed", "open", "fixed_stage"))
+        if unknown:
+            raise ValueError(f"unknown boundary type(s): {', '.join(unknown)}; use closed, open or fixed_stage")
+        staged = [e for e, v in self.boundaries.items() if v == "fixed_stage"]
+        if staged and self.scheme != "hllc_fv":
+            raise ValueError(f"fixed_stage edges ({', '.join(staged)}) need scheme = 'hllc_fv': the local-inertial "
+                             "scheme has no boundary face to impose a water level on")  # fmt: skip
+        missing = [e for e in staged if not self.stage_curves.get(e)]
+        if missing:
+            raise ValueError(f"fixed_stage edge(s) {', '.join(missing)} have no stage curve")
+        if self.alpha > 0.9:
+            warnings.warn(f"cfl={self.alpha} is above the ~0.7 stability limit of the local-inertial scheme; the run "
+                          "may go unstable", stacklevel=3)  # fmt: skip
 
     @property
     def rain_m_s(self) -> float:
@@ -273,4 +311,8 @@ def load_config(path) -> Scenario:
             ))  # fmt: skip
         except (TypeError, ValueError, IndexError) as e:
             raise ConfigError(f"[[structures]] #{k} ('{name}'): {e}") from e
+    try:
+        sc.validate()
+    except ValueError as e:
+        raise ConfigError(str(e)) from e
     return sc

@@ -250,3 +250,59 @@ def test_a_config_that_cannot_be_read_is_a_config_error(tmp_path):
     broken.write_text("[grid\ndx = ", encoding="utf-8")
     with pytest.raises(ConfigError, match="not valid TOML"):
         load_config(broken)
+
+
+_RUN = ('[meta]\nname = "r"\nscheme = "local_inertial"\n[grid]\ndx = 10.0\n'
+        '[run]\nend_time = 1200.0\noutput_every = 300.0\ndt_max = 20.0\ncfl = 0.6\n'
+        '[rainfall]\ntype = "uniform"\nrate_mm_hr = 40.0\nduration_s = 600.0\n'
+        '[parameters]\nmanning_n = 0.03\ninfiltration = 1.0\n')  # fmt: skip
+
+
+@pytest.mark.parametrize(("mutation", "repl", "needle"), [
+    ("output_every = 300.0", "output_every = 0.0", "output_every"),
+    ("end_time = 1200.0", "end_time = -5.0", "end_time"),
+    ("dt_max = 20.0", "dt_max = 0.0", "dt_max"),
+    ("cfl = 0.6", "cfl = 0.0", "cfl"),
+    ("end_time = 1200.0", "end_time = 1000.0", "multiple of output_every"),
+    ("manning_n = 0.03", "manning_n = -0.01", "manning_n"),
+    ("infiltration = 1.0", "infiltration = -1.0", "infiltration"),
+    ("rate_mm_hr = 40.0", "rate_mm_hr = -1.0", "rainfall rate"),
+])  # fmt: skip
+def test_bad_run_params_rejected(tmp_path, mutation, repl, needle):
+    """solver/io/test_config.py:337."""
+    from rbsim.config import ConfigError, load_config
+
+    assert mutation in _RUN
+    cfg = tmp_path / "r.toml"
+    cfg.write_text(_RUN.replace(mutation, repl))
+    with pytest.raises(ConfigError, match=needle):
+        load_config(cfg)
+
+
+def test_high_cfl_warns_but_loads(tmp_path):
+    """solver/io/test_config.py:343."""
+    from rbsim.config import load_config
+
+    cfg = tmp_path / "r.toml"
+    cfg.write_text(_RUN.replace("cfl = 0.6", "cfl = 5.0"))
+    with pytest.warns(UserWarning, match="stability limit"):
+        assert load_config(cfg).alpha == 5.0
+
+
+def test_scenario_validates_direct_construction():
+    """solver/io/test_config.py:349 and solver/test_run.py:205, :220: the in-code path is checked too."""
+    from rbsim.config import Scenario
+
+    with pytest.raises(ValueError, match="output_every"):
+        Scenario(output_every=0.0)
+    with pytest.raises(ValueError, match="multiple of output_every"):
+        Scenario(end_time=3500.0, output_every=300.0)
+    stage = {"north": "fixed_stage", "south": "closed", "east": "closed", "west": "closed"}
+    with pytest.raises(ValueError, match="hllc_fv"):
+        Scenario(scheme="local_inertial", boundaries=stage, stage_curves={"north": [(0.0, 1.0)]})
+    with pytest.raises(ValueError, match="no stage curve"):
+        Scenario(scheme="hllc_fv", boundaries=stage)
+    with pytest.raises(ValueError, match="unknown boundary"):
+        Scenario(boundaries={"north": "leaky"})
+    Scenario(scheme="hllc_fv", boundaries=stage, stage_curves={"north": [(0.0, 1.0)]}, end_time=600.0,
+             output_every=300.0)  # fmt: skip
