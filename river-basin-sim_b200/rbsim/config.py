@@ -186,16 +186,50 @@ class Scenario:
 
 
 def _field(value, base: Path, shape, name):
-    if isinstance(value, (int, float)):
+    if isinstance(value, (int, float)) and not isinstance(value, bool):  # TOML true is not a roughness
         return float(value)
     if isinstance(value, str):
         if shape is None:
             raise ConfigError(f"{name}: a field file needs [grid] shape")
+        if not (base / value).is_file():
+            raise ConfigError(f"{name}: field file {value} not found next to the config")
         arr = np.fromfile(base / value, dtype="<f4")
         if arr.size != shape[0] * shape[1]:
             raise ConfigError(f"{name}: {value} has {arr.size} values, grid is {shape}")
         return arr.reshape(shape)
     raise ConfigError(f"{name}: expected a number or a .r32 path, got {value!r}")
+
+
+def _number(value, what: str) -> float:
+    if isinstance(value, bool) or not isinstance(value, (int, float)):
+        raise ConfigError(f"{what} must be a number, got {value!r}")
+    return float(value)
+
+
+def _stage_edge(edge: str, table, scheme: str) -> list[tuple[float, float]]:
+    """One ``[boundaries]`` table: ``{ type = "fixed_stage", level = L }`` or ``stage = [[t, L], ...]``
+    (config.py:600-667). Returns the stage curve, knot times non-decreasing."""
+    kind = table.get("type")
+    if kind != "fixed_stage":
+        raise ConfigError(f"[boundaries] {edge}: unknown boundary type {kind!r}; a table edge is "
+                          "{ type = 'fixed_stage', level = ... } or { type = 'fixed_stage', stage = [[t, level], ...] }")
+    if ("level" in table) == ("stage" in table):
+        raise ConfigError(f"[boundaries] {edge}: a fixed_stage edge takes exactly one of 'level' or 'stage'")
+    if scheme != "hllc_fv":
+        raise ConfigError(f"[boundaries] {edge}: fixed_stage needs scheme = 'hllc_fv'")
+    if "level" in table:
+        return [(0.0, _number(table["level"], f"[boundaries] {edge} level"))]
+    knots = table["stage"]
+    if not isinstance(knots, list) or not knots:
+        raise ConfigError(f"[boundaries] {edge}: stage must be a non-empty list of [time_s, level_m] pairs")
+    curve = []
+    for k in knots:
+        if not (isinstance(k, list) and len(k) == 2):
+            raise ConfigError(f"[boundaries] {edge}: each stage knot must be [time_s, level_m], got {k!r}")
+        curve.append((_number(k[0], f"[boundaries] {edge} stage time"), _number(k[1], f"[boundaries] {edge} stage")))
+    if any(b[0] < a[0] for a, b in zip(curve, curve[1:], strict=False)):
+        raise ConfigError(f"[boundaries] {edge}: stage knot times must be non-decreasing")
+    return curve
 
 
 def load_config(path) -> Scenario:
@@ -214,7 +248,7 @@ def load_config(path) -> Scenario:
     meta, grid, run = doc.get("meta", {}), doc.get("grid", {}), doc.get("run", {})
     sc = Scenario(name=meta.get("name", path.stem), scheme=meta.get("scheme", "local_inertial"))
     if sc.scheme not in KNOWN_SCHEMES:
-        raise ConfigError(f"unknown scheme {sc.scheme!r}; known: {list(KNOWN_SCHEMES)}")
+        raise ConfigError(f"unknown scheme {sc.scheme!r}; known schemes: {list(KNOWN_SCHEMES)}")
     shape = tuple(grid["shape"]) if "shape" in grid else None
     sc.dx = float(grid["dx"]) if "dx" in grid else None
     if "dem" in grid:
@@ -230,7 +264,9 @@ def load_config(path) -> Scenario:
         raise ConfigError(f"rainfall type {sc.rain_type!r} is not supported (uniform | field)")
     sc.rain_duration = float(rain.get("duration_s", 0.0))
     if sc.rain_type == "uniform":
-        sc.rain_mm_hr = float(rain.get("rate_mm_hr", 0.0))
+        sc.rain_mm_hr = _number(rain.get("rate_mm_hr", 0.0), "[rainfall] rate_mm_hr")
+    elif "field" not in rain:
+        raise ConfigError("[rainfall] type = 'field' requires a 'field' path (a .r32 grid of mm/hr)")
     else:
         sc.rain_field = _field(rain["field"], base, shape, "[rainfall] field")
     par = doc.get("parameters", {})
@@ -241,22 +277,24 @@ def load_config(path) -> Scenario:
     for e in EDGES:
         v = bc.get(e, default)
         if isinstance(v, dict):
-            if v.get("type") != "fixed_stage":
-                raise ConfigError(f"[boundaries] {e}: a table must be type = 'fixed_stage'")
-            if sc.scheme != "hllc_fv":
-                raise ConfigError("fixed_stage boundaries need scheme = 'hllc_fv'")
-            curve = v.get("stage", [[0.0, v["level"]]] if "level" in v else None)
-            if not curve:
-                raise ConfigError(f"[boundaries] {e}: fixed_stage needs level or stage")
-            sc.stage_curves[e] = [(float(t), float(s)) for t, s in curve]
+            sc.stage_curves[e] = _stage_edge(e, v, sc.scheme)
             sc.boundaries[e] = "fixed_stage"
         elif v in ("closed", "open"):
             sc.boundaries[e] = v
+        elif v == "fixed_stage":
+            raise ConfigError(f"[boundaries] {e}: a fixed_stage edge needs its level, so write it as a fixed_stage "
+                              "table: { type = 'fixed_stage', level = ... }")  # fmt: skip
         else:
-            raise ConfigError(f"[boundaries] {e}: unknown kind {v!r}")
-    for entry in doc.get("inflow", []):
-        sc.inflows.append(Inflow(cell=tuple(entry["cell"]), hydrograph=[tuple(map(float, p))
-                                                                         for p in entry["hydrograph"]]))  # fmt: skip
+            raise ConfigError(f"[boundaries] {e}: must be 'closed', 'open' or a fixed_stage table, got {v!r}")
+    for k, entry in enumerate(doc.get("inflow", [])):
+        cell = entry.get("cell")
+        if not (isinstance(cell, list) and len(cell) == 2):
+            raise ConfigError(f"[[inflow]] #{k}: cell must be [row, col], got {cell!r}")
+        try:
+            hydrograph = [(float(t), float(q)) for t, q in entry["hydrograph"]]
+        except (KeyError, TypeError, ValueError) as err:
+            raise ConfigError(f"[[inflow]] #{k}: hydrograph must be a list of [time_s, discharge_m3_s]") from err
+        sc.inflows.append(Inflow(cell=(int(cell[0]), int(cell[1])), hydrograph=hydrograph))
     sed = doc.get("sediment")
     if sed is not None:
         if sc.scheme != "local_inertial":

@@ -306,3 +306,74 @@ def test_scenario_validates_direct_construction():
         Scenario(boundaries={"north": "leaky"})
     Scenario(scheme="hllc_fv", boundaries=stage, stage_curves={"north": [(0.0, 1.0)]}, end_time=600.0,
              output_every=300.0)  # fmt: skip
+
+
+_HLLC_RUN = _RUN.replace('scheme = "local_inertial"', 'scheme = "hllc_fv"') + '[boundaries]\ndefault = "closed"\n'
+
+
+@pytest.mark.parametrize(("table", "needle"), [
+    ('{ type = "fixed_stage" }', "exactly one of"),
+    ('{ type = "fixed_stage", level = 1.0, stage = [[0.0, 1.0]] }', "exactly one of"),
+    ('{ type = "fixed_stage", level = "high" }', "must be a number"),
+    ('{ type = "fixed_stage", stage = [] }', "non-empty"),
+    ('{ type = "fixed_stage", stage = [[10.0, 1.0], [0.0, 2.0]] }', "non-decreasing"),
+    ('{ type = "tidal" }', "unknown boundary type"),
+    ("42", "must be 'closed'"),
+    ('"fixed_stage"', "fixed_stage table"),
+])  # fmt: skip
+def test_fixed_stage_malformed(tmp_path, table, needle):
+    """solver/io/test_config.py:423, :429."""
+    from rbsim.config import ConfigError, load_config
+
+    cfg = tmp_path / "s.toml"
+    cfg.write_text(_HLLC_RUN + f"east = {table}\n")
+    with pytest.raises(ConfigError, match=needle):
+        load_config(cfg)
+
+
+def test_fixed_stage_level_and_curve(tmp_path):
+    """solver/io/test_config.py:380, :390: a level is a one-point curve; curve knots are sync events."""
+    from rbsim.config import load_config
+
+    cfg = tmp_path / "s.toml"
+    cfg.write_text(_HLLC_RUN + 'east = { type = "fixed_stage", level = 10.35 }\n'
+                   'west = { type = "fixed_stage", stage = [[0.0, 9.7], [3600.0, 10.35], [7200.0, 9.7]] }\n')  # fmt: skip
+    sc = load_config(cfg)
+    assert sc.boundaries["east"] == sc.boundaries["west"] == "fixed_stage"
+    assert sc.stage_curves["east"] == [(0.0, 10.35)]
+    assert sc.stage_curves["west"] == [(0.0, 9.7), (3600.0, 10.35), (7200.0, 9.7)]
+    assert sc.stage_events == [0.0, 3600.0, 7200.0]
+
+
+@pytest.mark.parametrize(("mutation", "repl", "needle"), [
+    ('type = "uniform"\nrate_mm_hr = 40.0', 'type = "field"', "requires a 'field' path"),
+    ("manning_n = 0.03", "manning_n = true", "manning_n"),
+    ('scheme = "local_inertial"', 'scheme = "quantum_flux"', "known scheme"),
+    ("infiltration = 1.0", 'infiltration = "absent.r32"', "not found"),
+])  # fmt: skip
+def test_config_refusals(tmp_path, mutation, repl, needle):
+    """solver/io/test_config.py:156, :218, :310: a missing rain field path, a boolean roughness, an
+    unknown scheme, and a field file that is not there."""
+    from rbsim.config import ConfigError, load_config
+
+    cfg = tmp_path / "r.toml"
+    cfg.write_text(_RUN.replace(mutation, repl).replace("[grid]\n", "[grid]\nshape = [4, 5]\n"))
+    with pytest.raises(ConfigError, match=needle):
+        load_config(cfg)
+
+
+def test_inflow_hydrograph_parsed_and_bad_shapes_rejected(tmp_path):
+    """solver/io/test_config.py:162, :173."""
+    from rbsim.config import ConfigError, load_config
+
+    cfg = tmp_path / "r.toml"
+    cfg.write_text(_RUN + "[[inflow]]\ncell = [10, 20]\nhydrograph = [[0.0, 0.0], [600.0, 5.0]]\n")
+    (inf,) = load_config(cfg).inflows
+    assert inf.cell == (10, 20) and inf.breakpoints == [0.0, 600.0]
+    assert inf.discharge_at(300.0) == pytest.approx(2.5) and inf.discharge_at(1e9) == 0.0
+    cfg.write_text(_RUN + "[[inflow]]\ncell = [10]\nhydrograph = [[0.0, 0.0]]\n")
+    with pytest.raises(ConfigError, match="cell"):
+        load_config(cfg)
+    cfg.write_text(_RUN + "[[inflow]]\ncell = [1, 2]\nhydrograph = [[0.0]]\n")
+    with pytest.raises(ConfigError, match="hydrograph"):
+        load_config(cfg)
