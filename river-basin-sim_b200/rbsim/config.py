@@ -25,6 +25,7 @@ _UNSUPPORTED: tuple[str, ...] = ()
 _STRUCTURE_KINDS = {"dam", "levee"}
 _RELEASE_RULES = {"none", "fixed", "target_stage"}
 _DEFAULT_RELEASE_INTERVAL_S = 900.0
+_SEDIMENT_KEYS = {"d50", "porosity", "law", "interval_s", "alluvium_thickness"}
 
 
 class ConfigError(ValueError):
@@ -296,16 +297,31 @@ def load_config(path) -> Scenario:
             raise ConfigError(f"[[inflow]] #{k}: hydrograph must be a list of [time_s, discharge_m3_s]") from err
         sc.inflows.append(Inflow(cell=(int(cell[0]), int(cell[1])), hydrograph=hydrograph))
     sed = doc.get("sediment")
-    if sed is not None:
+    if sed is not None:  # config.py:444-490, 905-940: the table's presence arms morphology
+        for key in sed:
+            if key not in _SEDIMENT_KEYS:
+                warnings.warn(f"[sediment] unknown key '{key}' ignored", stacklevel=2)
         if sc.scheme != "local_inertial":
-            raise ConfigError("[sediment] is local-inertial-only (with scheme = 'hllc_fv' it is refused)")
+            raise ConfigError("[sediment] requires scheme='local_inertial': morphology is local-inertial-only "
+                              f"(with scheme = '{sc.scheme}' it is refused)")  # fmt: skip
         if sed.get("law", "mpm") != "mpm":
-            raise ConfigError("only the Meyer-Peter-Mueller law ('mpm') is implemented")
-        sc.sediment_d50 = _field(sed["d50"], base, shape, "[sediment] d50")
-        sc.sediment_porosity = float(sed.get("porosity", 0.4))
-        sc.sediment_interval_s = float(sed.get("interval_s", 900.0))
+            raise ConfigError(f"[sediment] law={sed['law']!r} is not a transport law this solver has; only 'mpm' "
+                              "(Meyer-Peter-Mueller) is implemented")  # fmt: skip
+        d50 = _field(sed["d50"], base, shape, "[sediment] d50") if "d50" in sed else 0.0
+        if np.isscalar(d50) and not d50 > 0.0:
+            raise ConfigError("[sediment] needs a grain size: set d50 (metres, or a .r32 field); the table itself "
+                              "arms morphology, so no d50 means 'off'")  # fmt: skip
+        sc.sediment_d50 = d50
+        sc.sediment_porosity = _number(sed.get("porosity", 0.4), "[sediment] porosity")
+        if not 0.0 < sc.sediment_porosity < 1.0:
+            raise ConfigError(f"[sediment] porosity must be in (0, 1), got {sc.sediment_porosity}")
+        sc.sediment_interval_s = _number(sed.get("interval_s", 900.0), "[sediment] interval_s")
+        if not sc.sediment_interval_s > 0.0:
+            raise ConfigError(f"[sediment] interval_s must be > 0, got {sc.sediment_interval_s}")
         if "alluvium_thickness" in sed:
             sc.alluvium_thickness = _field(sed["alluvium_thickness"], base, shape, "alluvium_thickness")
+            if np.any(np.asarray(sc.alluvium_thickness) < 0):
+                raise ConfigError("[sediment] alluvium_thickness must be >= 0 m (0 is bedrock)")
     chan = doc.get("channels")
     if chan is not None:  # config.py:873-885, validated as :421-441
         sc.channel_width = _field(chan.get("width", 0.0), base, shape, "[channels] width")

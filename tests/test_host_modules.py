@@ -377,3 +377,37 @@ def test_inflow_hydrograph_parsed_and_bad_shapes_rejected(tmp_path):
     cfg.write_text(_RUN + "[[inflow]]\ncell = [1, 2]\nhydrograph = [[0.0]]\n")
     with pytest.raises(ConfigError, match="hydrograph"):
         load_config(cfg)
+
+
+def test_sediment_table(tmp_path):
+    """solver/io/test_config.py:545-630: defaults, refusals, and the typo guard."""
+    from rbsim.config import ConfigError, load_config
+
+    cfg = tmp_path / "r.toml"
+    cfg.write_text(_RUN + '[sediment]\nd50 = 0.008\nporosity = 0.35\nlaw = "mpm"\ninterval_s = 600.0\n'
+                   "alluvium_thickness = 2.0\n")  # fmt: skip
+    sc = load_config(cfg)
+    assert sc.has_sediment and sc.sediment_d50 == 0.008 and sc.sediment_porosity == 0.35
+    assert sc.sediment_interval_s == 600.0 and sc.alluvium_thickness == 2.0
+    cfg.write_text(_RUN + "[sediment]\nd50 = 0.01\n")
+    sc = load_config(cfg)
+    assert sc.sediment_porosity == 0.4 and sc.sediment_interval_s == 900.0 and sc.alluvium_thickness is None
+    cfg.write_text(_RUN)
+    assert not load_config(cfg).has_sediment
+    for bad, needle in (("porosity = 0.4", "needs a grain size"), ("d50 = 0.0", "needs a grain size"),
+                        ("d50 = 0.008\nporosity = 0.0", r"porosity must be in \(0, 1\)"),
+                        ("d50 = 0.008\nporosity = 1.0", r"porosity must be in \(0, 1\)"),
+                        ("d50 = 0.008\ninterval_s = 0.0", "interval_s must be > 0"),
+                        ("d50 = 0.008\nalluvium_thickness = -1.0", "alluvium_thickness must be >= 0"),
+                        ('d50 = 0.008\nlaw = "engelund_hansen"', "not a transport law"),
+                        ('d50 = 0.008\nporosity = "wet"', r"\[sediment\] porosity must be a number")):  # fmt: skip
+        cfg.write_text(_RUN + f"[sediment]\n{bad}\n")
+        with pytest.raises(ConfigError, match=needle):
+            load_config(cfg)
+    cfg.write_text(_RUN + "[sediment]\nd_50 = 0.008\n")
+    with pytest.warns(UserWarning, match="unknown key 'd_50'"):
+        with pytest.raises(ConfigError, match="needs a grain size"):
+            load_config(cfg)
+    cfg.write_text(_RUN.replace('scheme = "local_inertial"', 'scheme = "hllc_fv"') + "[sediment]\nd50 = 0.008\n")
+    with pytest.raises(ConfigError, match="requires scheme='local_inertial'"):
+        load_config(cfg)
