@@ -356,7 +356,7 @@ def load_config(path) -> Scenario:
         try:
             sc.structures.append(Structure(
                 name=name, kind=str(entry.get("type", "dam")),
-                cells=[(int(c[0]), int(c[1])) for c in entry.get("cells", [])],
+                cells=[(int(c[0]), int(c[1])) for c in entry.get("cells", [entry["cell"]] if "cell" in entry else [])],
                 crest_m=float(entry["crest_m"]), release_rule=str(entry.get("release_rule", "none")),
                 release_m3_s=float(entry.get("release_m3_s", 0.0)),
                 target_stage_m=float(entry["target_stage_m"]) if "target_stage_m" in entry else None,

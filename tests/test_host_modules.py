@@ -411,3 +411,53 @@ def test_sediment_table(tmp_path):
     cfg.write_text(_RUN.replace('scheme = "local_inertial"', 'scheme = "hllc_fv"') + "[sediment]\nd50 = 0.008\n")
     with pytest.raises(ConfigError, match="requires scheme='local_inertial'"):
         load_config(cfg)
+
+
+_DAM_TOML = ('[[structures]]\nname = "upper_dam"\ntype = "dam"\ncells = [[6, 4], [7, 4]]\ncrest_m = 145.0\n'
+             'release_rule = "target_stage"\ntarget_stage_m = 143.0\nrelease_max_m3_s = 40.0\npool = [2, 0, 5, 9]\n'
+             'outlet = [8, 4]\ninterval_s = 600.0\n')  # fmt: skip
+
+
+def test_structures_parse(tmp_path):
+    """solver/io/test_config.py:241-275: a dam with a target-stage rule, a one-cell levee, a fixed rule."""
+    from rbsim.config import load_config
+
+    cfg = tmp_path / "r.toml"
+    cfg.write_text(_RUN + _DAM_TOML)
+    (s,) = load_config(cfg).structures
+    assert (s.name, s.kind, s.cells) == ("upper_dam", "dam", [(6, 4), (7, 4)])
+    assert (s.crest_m, s.target_stage_m, s.release_max_m3_s, s.interval_s) == (145.0, 143.0, 40.0, 600.0)
+    assert s.pool == (2, 0, 5, 9) and s.outlet == (8, 4, 8, 4)
+    assert s.discharge_at(None) == 0.0 and s.discharge_at(142.0) == 0.0
+    assert s.discharge_at(144.0) == pytest.approx(20.0) and s.discharge_at(150.0) == 40.0
+    cfg.write_text(_RUN + '[[structures]]\ntype = "levee"\ncell = [3, 3]\ncrest_m = 12.0\n')
+    (s,) = load_config(cfg).structures
+    assert s.kind == "levee" and s.release_rule == "none" and s.cells == [(3, 3)]
+    cfg.write_text(_RUN + '[[structures]]\ntype = "dam"\ncell = [5, 5]\ncrest_m = 20.0\nrelease_rule = "fixed"\n'
+                   'release_m3_s = 7.5\npool = [0, 0, 4, 9]\noutlet = [6, 5]\n')  # fmt: skip
+    (s,) = load_config(cfg).structures
+    assert s.discharge_at(19.0) == 7.5 and s.discharge_at(1.0) == 7.5 and s.discharge_at(None) == 0.0
+
+
+@pytest.mark.parametrize(("body", "needle"), [
+    ('type = "weir"\ncell = [1, 1]\ncrest_m = 5.0', "type must be one of"),
+    ('type = "dam"\ncrest_m = 5.0', "at least one barrier cell"),
+    ('type = "dam"\ncell = [1, 1]', "crest_m' is required"),
+    ('type = "dam"\ncell = [1, 1]\ncrest_m = 5.0\nrelease_rule = "spill"', "release_rule"),
+    ('type = "levee"\ncell = [1, 1]\ncrest_m = 5.0\nrelease_rule = "fixed"\nrelease_m3_s = 1.0\npool = [0, 0, 0, 1]\n'
+     "outlet = [3, 3]", "levee is barrier geometry only"),
+    ('type = "dam"\ncell = [1, 1]\ncrest_m = 5.0\nrelease_rule = "fixed"\nrelease_m3_s = 1.0',
+     "needs both a 'pool' box and an 'outlet'"),
+    ('type = "dam"\ncell = [1, 1]\ncrest_m = 5.0\nrelease_rule = "fixed"\nrelease_m3_s = 1.0\npool = [0, 0, 3, 3]\n'
+     "outlet = [1, 1]", "overlaps the pool"),
+    ('type = "dam"\ncell = [1, 1]\ncrest_m = 5.0\nrelease_rule = "target_stage"\ntarget_stage_m = 6.0\n'
+     "release_max_m3_s = 2.0\npool = [0, 0, 0, 1]\noutlet = [3, 3]", "must be below crest_m"),
+])  # fmt: skip
+def test_structure_validation(tmp_path, body, needle):
+    """solver/io/test_config.py:305."""
+    from rbsim.config import ConfigError, load_config
+
+    cfg = tmp_path / "r.toml"
+    cfg.write_text(_RUN + "[[structures]]\n" + body + "\n")
+    with pytest.raises(ConfigError, match=needle):
+        load_config(cfg)
