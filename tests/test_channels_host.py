@@ -88,3 +88,25 @@ def test_no_channel_normalises_to_zero_in_both_fields():
     w_out, d_out, _ = validate_geometry(w, d, np.full((2, 2), 0.03, np.float32), grid)
     assert w_out[0, 0] == 0.0 and d_out[0, 0] == 0.0
     assert w_out[0, 1] == 10.0 and d_out[0, 1] == 2.0
+
+
+def test_kernel_storage_curve_matches_the_host_reference():
+    """solver/core/test_channels.py:71: the oracle's compute_eta_channels kernel and the host
+    storage curve agree (in-bank and overbank cells, channel and plain cells)."""
+    import ctypes
+
+    import oracle
+
+    ny, nx, dx = 4, 16, 100.0
+    rng = np.random.default_rng(7)
+    h = rng.uniform(0.0, 2.0, (ny, nx)).astype(np.float32)
+    z = rng.uniform(5.0, 15.0, (ny, nx)).astype(np.float32)
+    w = np.where(rng.random((ny, nx)) < 0.5, 0.0, rng.uniform(5.0, 40.0, (ny, nx))).astype(np.float32)
+    d = np.where(w > 0, rng.uniform(0.5, 4.0, (ny, nx)), 0.0).astype(np.float32)
+    eta = np.zeros((ny, nx), np.float32)
+    p = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    oracle.lib().rbo_compute_eta_channels_f32(ny, nx, p(h), p(z), p(w), p(d), ctypes.c_float(dx), p(eta))
+    np.testing.assert_allclose(eta, eta_from_h(h, z, w, d, dx), rtol=1e-5, atol=1e-5)
+    plain = w == 0
+    assert plain.any() and (~plain).any()
+    np.testing.assert_array_equal(eta[plain], (z + h)[plain])
