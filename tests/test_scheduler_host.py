@@ -179,3 +179,22 @@ def test_get_scheme_dispatches_by_name():
         assert callable(mod.compute_dt) and callable(mod.step)
     with pytest.raises(ValueError, match="unknown scheme"):
         get_scheme("nope")
+
+
+def test_fill_span_properties_over_random_spans():
+    """For any span and CFL step: 0 < dt <= dt_raw, a whole number of steps tiles the span, and
+    that number is the fewest that respect dt_raw (one more only where span / n rounds up)."""
+    hypothesis = pytest.importorskip("hypothesis")
+    st = hypothesis.strategies
+
+    @hypothesis.settings(max_examples=400, deadline=None)
+    @hypothesis.given(st.floats(1e-3, 1e5), st.floats(1e-4, 1e4))
+    def check(span, dt_raw):
+        dt = fill_span(span, dt_raw)
+        assert 0.0 < dt <= dt_raw
+        n = round(span / dt)
+        assert abs(n * dt - span) <= 1e-9 * span
+        fewest = max(1, math.ceil(span / dt_raw))
+        assert n in (fewest, fewest + 1)
+
+    check()
