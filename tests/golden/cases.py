@@ -270,6 +270,56 @@ CASES = {
 }
 
 
+# --- combinations of branches ------------------------------------------------- #
+# The cases above reach each branch on its own. These two run many at once, as the
+# reach (configuration 3) and a storm over an HLLC basin do, and pin the oracle
+# against the reference kernels on those combinations. They sit outside CASES, which
+# the GPU runners also iterate: the CUDA path is checked against the oracle on the
+# reach combination at full width (tests/test_gpu_parity.py, 200 steps of an
+# 8192-wide band with inflows, infiltration, a Manning field, bedload and Exner).
+
+
+def combined_li_reach():
+    """A small valley reach: cross-slope, lognormal Manning, infiltration field, two
+    triangular inflow hydrographs, the east edge open, bedload on a floored bed with a
+    frozen cell, Exner every 8 steps."""
+    rng = np.random.default_rng(21)
+    ny, nx, dx = 10, 24, 5.0
+    yy, xx = np.mgrid[0:ny, 0:nx].astype(np.float64)
+    bed = (4e-3 * (nx - 1 - xx) * dx + 0.04 * np.abs(yy - 4.5) * dx + 0.05 * np.sin(0.9 * xx)).astype(np.float32)
+    manning = np.exp(np.log(0.035) + 0.3 * rng.standard_normal((ny, nx))).astype(np.float32)
+    infil = (rng.uniform(0.0, 20.0, (ny, nx)) / 1000.0 / 3600.0).astype(np.float32)
+    inflows = [((4, 0), [(0.0, 0.0), (40.0, 6.0), (120.0, 0.5)]), ((5, 1), [(0.0, 1.0), (400.0, 1.0)])]
+    lo = np.full((ny, nx), -0.003, np.float32)
+    hi = np.full((ny, nx), np.inf, np.float32)
+    lo[5, 12] = hi[5, 12] = 0.0
+    return dict(scheme="local_inertial", bed=bed, dx=dx, depth=0.2, manning=manning, infil=infil,
+                inflows=inflows, boundaries=_bc(east="open"),
+                sediment=dict(d50=0.002, porosity=0.4, every=8, dz_lo=lo, dz_hi=hi),
+                steps=32, alpha=0.7, dt_max=3.0)  # fmt: skip
+
+
+def combined_hllc_storm():
+    """A bumpy basin with moving water: compensated rain field, infiltration, open south
+    and west edges and a rising fixed stage on the east edge."""
+    rng = np.random.default_rng(22)
+    ny, nx, dx = 12, 13, 8.0
+    bed = (_bumps(ny, nx, dx, rng, 5, (0.2, 1.0), (8.0, 30.0)) + 0.01 * np.arange(nx) * dx).astype(np.float32)
+    depth = np.maximum(1.2 - bed, 0.0).astype(np.float32)
+    hu0 = (rng.uniform(-0.2, 0.2, (ny, nx)) * (depth > 0)).astype(np.float32)
+    hv0 = (rng.uniform(-0.2, 0.2, (ny, nx)) * (depth > 0)).astype(np.float32)
+    rain = rng.uniform(0.0, 4e-5, (ny, nx)).astype(np.float32)
+    infil = rng.uniform(0.0, 1e-5, (ny, nx)).astype(np.float32)
+    return dict(scheme="hllc_fv", bed=bed, dx=dx, depth=depth, manning=0.03, hu0=hu0, hv0=hv0,
+                rain_field=rain, rain_scale=1.0, infil=infil, compensated=True,
+                boundaries=_bc(south="open", west="open", east="fixed_stage"),
+                stage_curves={"east": [(0.0, 1.3), (15.0, 1.6), (90.0, 1.6)]},
+                steps=14, alpha=0.45, dt_max=4.0)  # fmt: skip
+
+
+COMBINED_CASES = {"li_reach_combined": combined_li_reach, "hllc_storm_combined": combined_hllc_storm}
+
+
 def run_case(case: dict, api) -> dict:
     """Step ``case`` through ``api`` and return the recorded outputs.
 

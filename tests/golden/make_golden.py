@@ -174,14 +174,15 @@ def main(argv=None):
 
     fake_warp.install()
     sys.path.insert(0, os.path.abspath(args.reference))
-    from cases import CASES, run_case
+    from cases import CASES, COMBINED_CASES, run_case
 
     make_scheduler_fixture(os.path.join(HERE, "scheduler_ticks.json"))
     api = ReferenceAPI()
-    names = args.cases or list(CASES)
+    every = {**CASES, **COMBINED_CASES}
+    names = args.cases or list(every)
     for name in names:
         t0 = time.time()
-        out = run_case(CASES[name](), api)
+        out = run_case(every[name](), api)
         np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
         print(f"{name}: {time.time() - t0:.1f}s  keys={sorted(out)}")
 

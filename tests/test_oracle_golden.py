@@ -18,7 +18,7 @@ import numpy as np
 import pytest
 
 import oracle
-from cases import CASES, run_case
+from cases import CASES, COMBINED_CASES, run_case
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 
@@ -112,17 +112,20 @@ def _pow_mode_reset():
     oracle.set_pow_mode(0)
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+_ALL = {**CASES, **COMBINED_CASES}
+
+
+@pytest.mark.parametrize("name", sorted(_ALL))
 def test_oracle_matches_reference_kernels_bitwise(name):
     oracle.set_pow_mode(0)
     want = _golden(name)
-    got = run_case(CASES[name](), OracleAPI())
+    got = run_case(_ALL[name](), OracleAPI())
     assert sorted(got) == sorted(want)
     for key in want:
         np.testing.assert_array_equal(got[key], want[key], err_msg=f"{name}:{key}")
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
+@pytest.mark.parametrize("name", sorted(_ALL))
 def test_deterministic_powers_stay_within_float32_roundoff_of_reference(name):
     """pow_mode=1 (the CUDA path's arithmetic) against the same fixtures.
 
@@ -133,7 +136,7 @@ def test_deterministic_powers_stay_within_float32_roundoff_of_reference(name):
     """
     oracle.set_pow_mode(1)
     want = _golden(name)
-    got = run_case(CASES[name](), OracleAPI())
+    got = run_case(_ALL[name](), OracleAPI())
     for key in want:
         if key in ("h_comp", "qs_comp_x", "qs_comp_y"):
             continue  # compensation residues are round-off-sized by construction
