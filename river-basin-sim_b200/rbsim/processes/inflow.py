@@ -8,7 +8,6 @@ cell area -- the ledger's independent witness, exactly as in the reference.
 
 from __future__ import annotations
 
-import ctypes
 from dataclasses import dataclass
 
 import numpy as np

@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 from make_golden import SCHEDULER_CASES, _dt_fn
-from rbsim.scheduler import EPS_T, MultiRateScheduler, SlowProcess, fill_span
+from rbsim.scheduler import MultiRateScheduler, SlowProcess, fill_span
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden", "scheduler_ticks.json")
 
