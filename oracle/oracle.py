@@ -1,8 +1,8 @@
 """CPU oracle for the river-basin solver hot path -- Python side.
 
 TEST INFRASTRUCTURE: the checker the CUDA path is compared against. Only ``tests/``,
-``__graft_entry__.smoke`` and ``bench.py``'s CPU-baseline leg use it; the product
-package never imports it.
+``__graft_entry__.smoke`` and the CPU-baseline and float64-error legs of ``bench.py``
+use it; the product package never imports it.
 
 The kernels live in ``rbo.c`` (built into ``_build/librbo_{f32,f64}.so`` by the
 ``Makefile`` beside it); this module holds the state arrays, binds the C entry

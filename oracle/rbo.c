@@ -7,8 +7,8 @@
  *   boundaries.py:223-318, hllc.py:158-967, sediment.py:161-441,
  *   solver/processes/inflow.py:74-113, morphology.py:261-276.
  * It is the checker the CUDA path is compared against (by tests/, by
- * __graft_entry__.smoke and by bench.py's CPU baseline) and is never linked into
- * the product library.
+ * __graft_entry__.smoke and by bench.py's CPU-baseline and float64-error legs) and
+ * is never linked into the product library.
  *
  * Arithmetic model: one IEEE rounding per operation in the reference's expression
  * order (build with -ffp-contract=off, no fast-math), `wp.max(a,b)` = a > b ? a : b,
