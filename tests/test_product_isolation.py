@@ -70,9 +70,9 @@ def test_a_missing_library_is_an_error_not_a_fallback(monkeypatch):
 
 
 def test_a_state_refuses_the_cpu_device():
-    import rbsim
-
     import torch
+
+    import rbsim
 
     with pytest.raises((ValueError, RuntimeError), match="CUDA|no CPU fallback"):
         rbsim.State.from_bed(np.zeros((4, 4), np.float32), 10.0, device="cpu")
