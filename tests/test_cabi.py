@@ -128,3 +128,52 @@ def test_ensemble_layout_counts_each_variants_tiles():
     assert L.rb_ensemble_layout_make(3, scheme, ny, nx, 0, 3, ctypes.byref(out)) == _lib.RB_ERR_ARG
     assert "unknown tile variant" in _lib.last_error()
     assert L.rb_ensemble_layout_make(3, scheme, ny, nx, 4, 0, ctypes.byref(out)) == _lib.RB_ERR_ARG
+
+
+def test_both_hllc_step_entry_points_refuse_the_same_inputs_without_a_device():
+    """rb_hllc_step and rb_hllc_step_noalloc apply the same argument checks, all before
+    any device call: each case below carries exactly one defect on otherwise valid
+    arguments (the buffer addresses are never dereferenced on the host)."""
+    from rbsim import _lib
+
+    L = _lib.lib()
+
+    def fields(ny=64, nx=48):
+        f = _lib.HllcFields()
+        f.ny, f.nx, f.dx = ny, nx, 2.0
+        for k, name in enumerate(("h", "hu", "hv")):
+            getattr(f, name)[0], getattr(f, name)[1] = 4096 * (2 * k + 1), 4096 * (2 * k + 2)
+        f.z, f.n = 4096 * 7, 4096 * 8
+        f.bc[:] = [0, 1, 2, 0]
+        return f
+
+    def args(dt=0.5):
+        return _lib.StepArgs(dt, 0.0, 1.0, 1, 0)
+
+    def both(f, a, cur=0):
+        ws = ctypes.c_void_p(4096 * 16)
+        return (L.rb_hllc_step(f if f is None else ctypes.byref(f), cur, ctypes.byref(a), ws, None),
+                L.rb_hllc_step_noalloc(f if f is None else ctypes.byref(f), cur, ctypes.byref(a), None, None))
+
+    cases = []
+    cases.append(("null fields", both(None, args()), _lib.RB_ERR_ARG))
+    f = fields(0, 48)
+    cases.append(("empty grid", both(f, args()), _lib.RB_ERR_ARG))
+    f = fields()
+    f.dx = float("inf")
+    cases.append(("infinite dx", both(f, args()), _lib.RB_ERR_ARG))
+    cases.append(("infinite dt", both(fields(), args(float("inf"))), _lib.RB_ERR_STEP))
+    cases.append(("nan dt", both(fields(), args(float("nan"))), _lib.RB_ERR_STEP))
+    cases.append(("zero dt", both(fields(), args(0.0)), _lib.RB_ERR_STEP))
+    f = fields()
+    f.bc[2] = 7
+    cases.append(("unknown edge kind", both(f, args()), _lib.RB_ERR_ARG))
+    cases.append(("cur 2", both(fields(), args(), cur=2), _lib.RB_ERR_ARG))
+    f = fields()
+    f.hv[1] = None
+    cases.append(("missing buffer", both(f, args()), _lib.RB_ERR_ARG))
+    for what, got, want in cases:
+        assert got == (want, want), what
+    f = fields(1025, 1024)
+    assert L.rb_hllc_step_noalloc(ctypes.byref(f), 0, ctypes.byref(args()), None, None) == _lib.RB_ERR_ARG
+    assert "1048576-cell" in _lib.last_error()
