@@ -406,6 +406,7 @@ int rb_hllc_clock_start(const rb_hllc_fields* f, int32_t cur, const rb_clock_con
   rb::HllcParams p;
   int rc = hllc_params(f, ws, p, "rb_hllc_clock_start");
   if (rc) return rc;
+  if (cfg == nullptr) return fail(RB_ERR_ARG, "rb_hllc_clock_start: null config");  // read just below
   for (int e = 0; e < 4; e++)
     if (f->bc[e] == RB_BC_STAGE && cfg->stage_off[e + 1] <= cfg->stage_off[e])
       return fail(RB_ERR_ARG, "rb_hllc_clock_start: fixed_stage edge %d has no stage curve", e);

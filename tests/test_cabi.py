@@ -177,3 +177,44 @@ def test_both_hllc_step_entry_points_refuse_the_same_inputs_without_a_device():
     f = fields(1025, 1024)
     assert L.rb_hllc_step_noalloc(ctypes.byref(f), 0, ctypes.byref(args()), None, None) == _lib.RB_ERR_ARG
     assert "1048576-cell" in _lib.last_error()
+
+
+def test_clock_start_refuses_bad_configs_without_a_device():
+    """The device clock's start checks its configuration before reading it: a null
+    config (with a fixed_stage edge, whose stage curve the HLLC start looks up), a bad
+    buffer index, a missing sync array, non-positive alpha or dt_max, point sources
+    without their tables, and a fixed_stage edge without a stage curve."""
+    from rbsim import _lib
+
+    L = _lib.lib()
+    ws = ctypes.c_void_p(4096 * 16)
+    f = _lib.HllcFields()
+    f.ny, f.nx, f.dx = 32, 32, 1.0
+    for k, name in enumerate(("h", "hu", "hv")):
+        getattr(f, name)[0], getattr(f, name)[1] = 4096 * (2 * k + 1), 4096 * (2 * k + 2)
+    f.z, f.n = 4096 * 7, 4096 * 8
+    f.bc[:] = [0, 0, 2, 0]  # east fixed_stage
+    assert L.rb_hllc_clock_start(ctypes.byref(f), 0, None, ws, None) == _lib.RB_ERR_ARG
+    assert "null config" in _lib.last_error()
+
+    def cfg(**kw):
+        c = _lib.ClockConfig()
+        c.alpha, c.dt_max, c.nsync = 0.45, 5.0, 0
+        c.stage_off[:] = [0, 0, 0, 2, 2]  # two knots for edge 2 (east)
+        for k, v in kw.items():
+            setattr(c, k, v)
+        return c
+
+    for bad in (dict(nsync=3), dict(alpha=0.0), dict(dt_max=-1.0), dict(nsrc=2)):
+        assert L.rb_hllc_clock_start(ctypes.byref(f), 0, ctypes.byref(cfg(**bad)), ws, None) == _lib.RB_ERR_ARG, bad
+    assert L.rb_hllc_clock_start(ctypes.byref(f), 2, ctypes.byref(cfg()), ws, None) == _lib.RB_ERR_ARG
+    no_curve = cfg()
+    no_curve.stage_off[:] = [0, 0, 0, 0, 0]
+    assert L.rb_hllc_clock_start(ctypes.byref(f), 0, ctypes.byref(no_curve), ws, None) == _lib.RB_ERR_ARG
+    assert "no stage curve" in _lib.last_error()
+    li = _lib.LiFields()
+    li.ny, li.nx, li.dx = 32, 32, 1.0
+    for k, name in enumerate(("h", "qx", "qy")):
+        getattr(li, name)[0], getattr(li, name)[1] = 4096 * (2 * k + 1), 4096 * (2 * k + 2)
+    li.z, li.n = 4096 * 7, 4096 * 8
+    assert L.rb_li_clock_start(ctypes.byref(li), 0, None, ws, None) == _lib.RB_ERR_ARG
