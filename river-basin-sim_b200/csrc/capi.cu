@@ -226,6 +226,7 @@ int rb_li_compute_dt(const rb_li_fields* f, int32_t cur, double alpha, double dt
   int rc = check_grid(f->ny, f->nx, f->dx, "rb_li_compute_dt");
   if (rc) return rc;
   if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_li_compute_dt: cur must be 0 or 1");
+  if (!f->h[cur]) return fail(RB_ERR_ARG, "rb_li_compute_dt: missing depth buffer");
   cudaStream_t s = (cudaStream_t)stream;
   unsigned int* key = &header(ws)->red_key;
   if (f->chan_w && !f->chan_d) return fail(RB_ERR_ARG, "rb_li_compute_dt: chan_w given without chan_d");
@@ -322,6 +323,7 @@ int rb_hllc_compute_dt(const rb_hllc_fields* f, int32_t cur, double alpha, doubl
   int rc = check_grid(f->ny, f->nx, f->dx, "rb_hllc_compute_dt");
   if (rc) return rc;
   if (cur != 0 && cur != 1) return fail(RB_ERR_ARG, "rb_hllc_compute_dt: cur must be 0 or 1");
+  if (!f->h[cur] || !f->hu[cur] || !f->hv[cur]) return fail(RB_ERR_ARG, "rb_hllc_compute_dt: missing state buffer");
   cudaStream_t s = (cudaStream_t)stream;
   unsigned int* key = &header(ws)->red_key;
   RB_CUDA(rb::reduce_wavespeed(f->h[cur], f->hu[cur], f->hv[cur], (size_t)f->ny * f->nx, key, s),
@@ -644,6 +646,22 @@ int rb_ensemble_init(rb_ensemble_layout* L, void* ens, const int32_t* scheme, co
                      void* stream) {
   if (!L || !ens || !scheme || !dom_ws || !cfg || !cur) return fail(RB_ERR_ARG, "rb_ensemble_init: null argument");
   if ((L->n_li > 0 && !li) || (L->n_hllc > 0 && !hl)) return fail(RB_ERR_ARG, "rb_ensemble_init: missing fields");
+  // The layout sizes every host vector and device area below: it must be the one
+  // rb_ensemble_layout_make made for this scheme array.
+  if (L->ndom < 1 || L->n_li < 0 || L->n_hllc < 0 || L->n_li + L->n_hllc != L->ndom || L->li_variant < 0 ||
+      L->li_variant > 3 || L->hllc_variant < 0 || L->hllc_variant > 2)
+    return fail(RB_ERR_ARG, "rb_ensemble_init: the layout is not one rb_ensemble_layout_make made");
+  {
+    int32_t n_li = 0, n_hllc = 0;
+    for (int d = 0; d < L->ndom; d++) {
+      if (scheme[d] != 0 && scheme[d] != 1)
+        return fail(RB_ERR_ARG, "rb_ensemble_init: domain %d has unknown scheme %d", d, scheme[d]);
+      if (cur[d] != 0 && cur[d] != 1) return fail(RB_ERR_ARG, "rb_ensemble_init: domain %d: cur must be 0 or 1", d);
+      (scheme[d] == 0 ? n_li : n_hllc)++;
+    }
+    if (n_li != L->n_li || n_hllc != L->n_hllc)
+      return fail(RB_ERR_ARG, "rb_ensemble_init: the scheme array does not match the layout");
+  }
   cudaStream_t s = (cudaStream_t)stream;
   char* base = (char*)ens;
   rb::DevClock* clocks = (rb::DevClock*)(base + L->off_clocks);
@@ -716,6 +734,8 @@ int rb_ensemble_init(rb_ensemble_layout* L, void* ens, const int32_t* scheme, co
     c.limit = k.limit ? 1 : 0;
     hc[d] = c;
   }
+  if ((int64_t)mli.size() > L->li_tiles || (int64_t)mhl.size() > L->hllc_tiles)
+    return fail(RB_ERR_ARG, "rb_ensemble_init: the domains have more tiles than the layout was made for");
   // the persistent kernels walk the small domains' tiles only
   L->li_tiles = (int64_t)mli.size();
   L->hllc_tiles = (int64_t)mhl.size();

@@ -218,3 +218,78 @@ def test_clock_start_refuses_bad_configs_without_a_device():
         getattr(li, name)[0], getattr(li, name)[1] = 4096 * (2 * k + 1), 4096 * (2 * k + 2)
     li.z, li.n = 4096 * 7, 4096 * 8
     assert L.rb_li_clock_start(ctypes.byref(li), 0, None, ws, None) == _lib.RB_ERR_ARG
+
+
+def _fake_li(ny, nx):
+    from rbsim import _lib
+
+    f = _lib.LiFields()
+    f.ny, f.nx, f.dx = ny, nx, 10.0
+    for k, name in enumerate(("h", "qx", "qy")):
+        getattr(f, name)[0], getattr(f, name)[1] = 4096 * (2 * k + 1), 4096 * (2 * k + 2)
+    f.z, f.n = 4096 * 7, 4096 * 8
+    return f
+
+
+def _fake_hllc(ny, nx):
+    from rbsim import _lib
+
+    f = _lib.HllcFields()
+    f.ny, f.nx, f.dx = ny, nx, 10.0
+    for k, name in enumerate(("h", "hu", "hv")):
+        getattr(f, name)[0], getattr(f, name)[1] = 4096 * (2 * k + 1), 4096 * (2 * k + 2)
+    f.z, f.n = 4096 * 7, 4096 * 8
+    return f
+
+
+def test_compute_dt_refuses_a_missing_current_buffer():
+    """A null current depth (or momentum) buffer is an argument error, not a kernel launch on NULL."""
+    from rbsim import _lib
+
+    L = _lib.lib()
+    ws, dt = ctypes.c_void_p(4096 * 16), ctypes.c_double()
+    li = _fake_li(8, 8)
+    li.h[1] = None
+    assert L.rb_li_compute_dt(ctypes.byref(li), 1, 0.7, 5.0, ws, None, ctypes.byref(dt)) == _lib.RB_ERR_ARG
+    assert "missing depth buffer" in _lib.last_error()
+    hl = _fake_hllc(8, 8)
+    hl.hu[0] = None
+    assert L.rb_hllc_compute_dt(ctypes.byref(hl), 0, 0.45, 5.0, ws, None, ctypes.byref(dt)) == _lib.RB_ERR_ARG
+    assert "missing state buffer" in _lib.last_error()
+
+
+def test_ensemble_init_refuses_a_layout_that_does_not_fit_its_domains():
+    """rb_ensemble_init sizes host vectors and device areas from the layout, so it checks
+    the layout against the scheme array, the buffer indices and the domains' tiles first."""
+    from rbsim import _lib
+
+    L = _lib.lib()
+    n = 3
+    scheme = (ctypes.c_int32 * n)(0, 1, 1)
+    ny = (ctypes.c_int32 * n)(40, 30, 20)
+    nx = (ctypes.c_int32 * n)(40, 30, 20)
+    lay = _lib.EnsembleLayout()
+    assert L.rb_ensemble_layout_make(n, scheme, ny, nx, 0, 0, ctypes.byref(lay)) == 0
+    li = (_lib.LiFields * 1)(_fake_li(40, 40))
+    hl = (_lib.HllcFields * 2)(_fake_hllc(30, 30), _fake_hllc(20, 20))
+    wss = (ctypes.c_void_p * n)(4096 * 32, 4096 * 48, 4096 * 64)
+    cfgs = (_lib.ClockConfig * n)()
+    for c in cfgs:
+        c.alpha, c.dt_max = 0.5, 5.0
+    cur = (ctypes.c_int32 * n)(0, 1, 0)
+    ens = ctypes.c_void_p(4096 * 128)
+
+    def init(layout, sch=scheme, cr=cur, hls=hl):
+        return L.rb_ensemble_init(ctypes.byref(layout), ens, sch, li, hls, wss, cfgs, cr, None)
+
+    assert init(lay, sch=(ctypes.c_int32 * n)(0, 0, 1)) == _lib.RB_ERR_ARG
+    assert "does not match the layout" in _lib.last_error()
+    assert init(lay, cr=(ctypes.c_int32 * n)(0, 2, 0)) == _lib.RB_ERR_ARG
+    assert "cur must be 0 or 1" in _lib.last_error()
+    forged = _lib.EnsembleLayout.from_buffer_copy(lay)
+    forged.n_li = 5
+    assert init(forged) == _lib.RB_ERR_ARG
+    assert "not one rb_ensemble_layout_make made" in _lib.last_error()
+    bigger = (_lib.HllcFields * 2)(_fake_hllc(300, 300), _fake_hllc(20, 20))
+    assert init(_lib.EnsembleLayout.from_buffer_copy(lay), hls=bigger) == _lib.RB_ERR_ARG
+    assert "more tiles than the layout" in _lib.last_error()
