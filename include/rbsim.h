@@ -141,7 +141,9 @@ int rb_hllc_compute_dt(const rb_hllc_fields *f, int32_t cur, double alpha, doubl
 
 /* --- sources, morphology, ledger ---------------------------------------- */
 /* Point sources: replaces the _inject_point_sources[_c] launch of
- * InflowInjector.apply (inflow.py:74-113, :183-199). comp == NULL adds plainly. */
+ * InflowInjector.apply (inflow.py:74-113, :183-199). comp == NULL adds plainly.
+ * rows / cols (device, nsrc each) must name distinct cells inside the ny x nx grid, as
+ * InflowInjector checks on the host; a source outside the grid adds nothing. */
 int rb_inject_points(float *h, int32_t ny, int32_t nx, int32_t nsrc, const int32_t *rows, const int32_t *cols,
                      const float *add_depth, float *comp, void *stream);
 /* Exner activation: replaces exner_update + rebuild_bed (sediment.py:383-441) as
@@ -182,7 +184,7 @@ typedef struct rb_clock_config {
   double rain_field_sum;     /* float64 sum of the rain field, m/s (run.py:276) */
   int32_t limit;             /* LI donor limiter */
   int32_t nsrc;              /* point sources (0: none) */
-  const int32_t *src_cell;   /* device, nsrc: row * nx + col, distinct cells */
+  const int32_t *src_cell;   /* device, nsrc: row * nx + col, distinct cells (one outside the grid adds nothing) */
   const int32_t *knot_off;   /* device, nsrc + 1: source k's hydrograph knots are [off[k], off[k+1]) */
   const double *knot_t;      /* device: knot times (s), non-decreasing per source */
   const double *knot_q;      /* device: knot discharges (m^3/s) */

@@ -109,11 +109,13 @@ cudaError_t sum_ledger(const double* ledger, size_t nslots, double* partials, do
 
 // inflow.py:74-113: one thread per source entry; entries name distinct cells
 // (the injector rejects duplicates), so the non-atomic add does not race.
-__global__ void inject_kernel(float* h, int nx, int nsrc, const int32_t* rows, const int32_t* cols,
+__global__ void inject_kernel(float* h, int ny, int nx, int nsrc, const int32_t* rows, const int32_t* cols,
                               const float* add, float* comp) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= nsrc) return;
-  const size_t c = (size_t)rows[k] * nx + cols[k];
+  const int r = rows[k], col = cols[k];
+  if (r < 0 || r >= ny || col < 0 || col >= nx) return;  // a source outside the grid adds nothing
+  const size_t c = (size_t)r * nx + col;
   if (comp != nullptr) {
     float tot = h[c], cp = comp[k];
     kahan_add(tot, cp, add[k]);
@@ -175,10 +177,10 @@ cudaError_t reservoir_deliver(float* h, int nx, int r0, int c0, int rows, int co
   return cudaGetLastError();
 }
 
-cudaError_t inject_points(float* h, int nx, int nsrc, const int32_t* rows, const int32_t* cols,
+cudaError_t inject_points(float* h, int ny, int nx, int nsrc, const int32_t* rows, const int32_t* cols,
                           const float* add, float* comp, cudaStream_t s) {
   if (nsrc <= 0) return cudaSuccess;
-  inject_kernel<<<(nsrc + 127) / 128, 128, 0, s>>>(h, nx, nsrc, rows, cols, add, comp);
+  inject_kernel<<<(nsrc + 127) / 128, 128, 0, s>>>(h, ny, nx, nsrc, rows, cols, add, comp);
   return cudaGetLastError();
 }
 

@@ -849,7 +849,7 @@ int rb_inject_points(float* h, int32_t ny, int32_t nx, int32_t nsrc, const int32
   if (ny < 1 || nx < 1 || nsrc < 0) return fail(RB_ERR_ARG, "rb_inject_points: bad sizes");
   if (nsrc == 0) return RB_OK;
   if (!h || !rows || !cols || !add_depth) return fail(RB_ERR_ARG, "rb_inject_points: null argument");
-  RB_CUDA(rb::inject_points(h, nx, nsrc, rows, cols, add_depth, comp, (cudaStream_t)stream), "rb_inject_points");
+  RB_CUDA(rb::inject_points(h, ny, nx, nsrc, rows, cols, add_depth, comp, (cudaStream_t)stream), "rb_inject_points");
   return RB_OK;
 }
 

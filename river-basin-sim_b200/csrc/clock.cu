@@ -221,7 +221,9 @@ __global__ void __launch_bounds__(INFLOW_NT) clock_inflow_kernel(DevClock* c, fl
       const double vol = discharge_at(c->knot_t + a, c->knot_q + a, b - a, t_mid) * c->dt;
       add = (float)(vol / c->cell_area);
       const int cell = c->src_cell[k];
-      if (c->src_comp != nullptr) {
+      if (cell < 0 || (double)cell >= c->n_cells) {
+        add = 0.0f;  // a source outside the grid adds, and banks, nothing
+      } else if (c->src_comp != nullptr) {
         float tot = h[cell], cp = c->src_comp[k];
         kahan_add(tot, cp, add);
         h[cell] = tot;

@@ -177,7 +177,7 @@ cudaError_t reservoir_withdraw(float* h, int nx, int r0, int c0, int rows, int c
                                cudaStream_t s);
 cudaError_t reservoir_deliver(float* h, int nx, int r0, int c0, int rows, int cols, double add_depth,
                               double* ledger_slot, cudaStream_t s);
-cudaError_t inject_points(float* h, int nx, int nsrc, const int32_t* rows, const int32_t* cols,
+cudaError_t inject_points(float* h, int ny, int nx, int nsrc, const int32_t* rows, const int32_t* cols,
                           const float* add, float* comp, cudaStream_t s);
 cudaError_t exner_apply(int ny, int nx, float dx32, float inv1mp, float* qs_int_x, float* qs_int_y,
                         const float* dz_lo, const float* dz_hi, double* dz_cum, double* dz_unapplied,
