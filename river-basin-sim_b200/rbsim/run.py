@@ -18,6 +18,7 @@ Two ways through the ticks, with identical results:
   tick exactly as the reference's run loop.
 
     python -m rbsim.run --config scenario.toml --out results.zarr [--status status.json]
+        [--frames-dir frames] [--no-frames] [--host-loop]
 """
 
 from __future__ import annotations
@@ -228,31 +229,38 @@ def run_simulation(scenario: Scenario, bed=None, out_path="results.zarr", *, dev
 
 
 def main(argv=None) -> int:
+    """The run-loop CLI (solver/run.py:486-580): a scenario in, a result store, the
+    viewer's frames and ``status.json`` out."""
     ap = argparse.ArgumentParser(prog="python -m rbsim.run")
-    ap.add_argument("--config", required=True)
-    ap.add_argument("--out", default=None)
-    ap.add_argument("--status", default=None)
+    ap.add_argument("--config", required=True, help="scenario TOML")
+    ap.add_argument("--out", default=None, help="result store; default <config name>.zarr")
+    ap.add_argument("--status", default=None, help="status.json path; default <out-dir>/status.json")
+    ap.add_argument("--frames-dir", default=None, help="viewer frames; default <out-dir>/frames")
+    ap.add_argument("--no-frames", action="store_true", help="skip the viewer frame export")
     ap.add_argument("--host-loop", action="store_true", help="step through compute_dt/step on the host")
     args = ap.parse_args(argv)
+    out = Path(args.out or Path(args.config).with_suffix(".zarr").name)
+    out.parent.mkdir(parents=True, exist_ok=True)
     # The status channel opens before anything that can fail, the config included, so a
     # viewer polling it sees state "error" rather than a file that never appears. Its
     # end time is set once the scenario is known.
-    status = StatusWriter(args.status, 1.0) if args.status else None
+    status = StatusWriter(args.status or out.parent / "status.json", 1.0)
     try:
-        if status:
-            status.write("starting", message="reading the scenario")
+        status.write("starting", message="reading the scenario")
         sc = load_config(args.config)
-        out = args.out or str(Path(args.config).with_suffix(".zarr").name)
-        if status:
-            status.end_time = float(sc.end_time)
-            status.write("starting", message=sc.name)
+        status.end_time = float(sc.end_time)
+        status.write("starting", message=sc.name)
         t0 = time.time()
-        run_simulation(sc, None, out, status=status, use_device_clock=not args.host_loop)
-        if status:
-            status.write("done", sim_time=sc.end_time, message=f"wall {time.time() - t0:.1f}s")
+        ledger = run_simulation(sc, None, str(out), status=status, use_device_clock=not args.host_loop)
+        if not args.no_frames:
+            from .io.viewer_export import export_frames
+
+            status.write("writing", sim_time=sc.end_time, message="exporting viewer frames")
+            export_frames(out, args.frames_dir or out.parent / "frames")
+        status.write("done", sim_time=sc.end_time,
+                     message=f"mass_max_rel_err={ledger.max_rel_error:.2e}, wall {time.time() - t0:.1f}s")  # fmt: skip
     except Exception as e:
-        if status:
-            status.write("error", message=str(e))
+        status.write("error", message=f"{type(e).__name__}: {e}")
         raise
     return 0
 

@@ -461,3 +461,63 @@ def test_structure_validation(tmp_path, body, needle):
     cfg.write_text(_RUN + "[[structures]]\n" + body + "\n")
     with pytest.raises(ConfigError, match=needle):
         load_config(cfg)
+
+
+def _fake_run(calls):
+    """Stands in for run_simulation (which needs the device): writes a small result store
+    of a filling basin, as a run would, and returns a ledger-shaped record."""
+    from types import SimpleNamespace
+
+    from rbsim.grid import Grid
+    from rbsim.io.zarr_writer import ZarrWriter
+
+    def run(sc, bed, out, **kw):
+        calls.append((sc.name, str(out), kw))
+        grid = Grid(ny=6, nx=9, dx=10.0)
+        w = ZarrWriter(out, grid, 3, {"scheme": sc.scheme, "dx": 10.0, "coarsen": 1})
+        z = np.linspace(0.0, 1.0, 54, dtype=np.float32).reshape(6, 9)
+        w.write_bed(z)
+        for i in range(3):
+            d = np.full((6, 9), 0.1 * i, np.float32)
+            w.append(300.0 * i, d, d * 0, d * 0)
+        w.finalize({})
+        return SimpleNamespace(max_rel_error=3.0e-9)
+
+    return run
+
+
+def test_main_runs_exports_frames_and_reports_done(tmp_path, monkeypatch):
+    """solver/run.py:530-580: status.json beside the store by default, the viewer frames
+    exported after the run (unless --no-frames), state "done" with the mass error."""
+    import rbsim.run as run_mod
+
+    calls = []
+    monkeypatch.setattr(run_mod, "run_simulation", _fake_run(calls))
+    cfg = tmp_path / "s.toml"
+    cfg.write_text(_RUN)
+    out = tmp_path / "res" / "r.zarr"
+    assert run_mod.main(["--config", str(cfg), "--out", str(out)]) == 0
+    rec = json.loads((out.parent / "status.json").read_text())
+    assert rec["state"] == "done" and rec["progress"] == 1.0 and "mass_max_rel_err=3.00e-09" in rec["message"]
+    assert (out.parent / "frames" / "manifest.json").is_file()
+    assert calls[0][0] == "r" and calls[0][2]["use_device_clock"] is True
+    out2 = tmp_path / "other" / "r.zarr"
+    assert run_mod.main(["--config", str(cfg), "--out", str(out2), "--no-frames", "--host-loop",
+                         "--status", str(tmp_path / "st.json")]) == 0  # fmt: skip
+    assert not (out2.parent / "frames").exists() and calls[1][2]["use_device_clock"] is False
+    assert json.loads((tmp_path / "st.json").read_text())["state"] == "done"
+
+
+def test_main_reports_a_failed_run_with_its_exception_type(tmp_path, monkeypatch):
+    import rbsim.run as run_mod
+
+    def boom(*a, **kw):
+        raise RuntimeError("the device clock made no progress")
+
+    monkeypatch.setattr(run_mod, "run_simulation", boom)
+    cfg = tmp_path / "s.toml"
+    cfg.write_text(_RUN)
+    with pytest.raises(RuntimeError):
+        run_mod.main(["--config", str(cfg), "--out", str(tmp_path / "r.zarr")])
+    rec = json.loads((tmp_path / "status.json").read_text())
+    assert rec["state"] == "error" and rec["message"] == "RuntimeError: the device clock made no progress"
