@@ -189,3 +189,60 @@ def test_cli_entry_point(tmp_path):
     store, _ = _store(tmp_path)
     assert main([str(store), str(tmp_path / "cli")]) == 0
     assert (tmp_path / "cli" / "manifest.json").exists()
+
+
+def _reassemble(out, tiles, names, shape):
+    full = np.zeros(shape, np.float32)
+    for t, name in zip(tiles, names, strict=True):
+        block = np.fromfile(out / name, dtype="<f4").reshape(t["height"], t["width"])
+        full[t["y"] : t["y"] + t["height"], t["x"] : t["x"] + t["width"]] = block
+    return full
+
+
+def test_static_fields_are_tiled_with_the_frame_layout(tmp_path):
+    """solver/io/test_viewer_export.py:149, :371: in a tiled export the bed and the channel
+    geometry ride the frames' tile grid, so one reader decodes all of them."""
+    ny, nx = 16, 20
+    w = np.zeros((ny, nx), np.float32)
+    d = np.zeros((ny, nx), np.float32)
+    w[:, nx // 2], d[:, nx // 2] = 8.0, 1.0
+    store, bed = _store(tmp_path, ny=ny, nx=nx, channels=(w, d))
+    out = tmp_path / "tiled"
+    manifest = json.loads(export_frames(store, out, tile_size=8).read_text())
+    tiles = manifest["tile_grid"]["tiles"]
+    static = manifest["static"]
+    assert static["files"] == {} and len(tiles) > 1
+    for name, want in (("bed", bed), ("channel_width", w), ("channel_depth", d)):
+        assert np.array_equal(_reassemble(out, tiles, static["tiles"][name], (ny, nx)), want), name
+
+
+def test_a_still_bed_and_a_channel_free_run_add_nothing_to_the_manifest(tmp_path):
+    """solver/io/test_viewer_export.py:258, :435: no morphology note, no channel keys or files."""
+    store, _ = _store(tmp_path)
+    out = tmp_path / "f"
+    manifest = json.loads(export_frames(store, out).read_text())
+    assert "morphology" not in manifest
+    static = manifest["static"]
+    assert static["fields"] == ["bed"] and "channel" not in static and list(static["files"]) == ["bed"]
+    assert not any("channel" in p.name for p in out.iterdir())
+
+
+def test_a_cell_without_a_channel_is_drawn_exactly_as_before():
+    """solver/io/test_viewer_export.py:327: z + h bit for bit, also for half a channel."""
+    z = np.array([1.0, 250.0, -3.5])
+    h = np.array([0.0, 0.001, 2.25])
+    zeros = np.zeros(3)
+    assert np.array_equal(render_eta(h, z, zeros, zeros, 20.0), z + h)
+    assert np.array_equal(render_eta(h, z, np.full(3, 8.0), zeros, 20.0), z + h)
+    assert np.array_equal(render_eta(h, z, zeros, np.full(3, 1.0), 20.0), z + h)
+
+
+def test_one_tile_exports_the_same_bytes_whatever_the_tile_size(tmp_path):
+    """solver/io/test_viewer_export.py:449: a frame that fits one tile is written identically."""
+    store, _ = _store(tmp_path)
+    a, b = tmp_path / "a", tmp_path / "b"
+    export_frames(store, a)
+    export_frames(store, b, tile_size=4096)
+    for fr in json.loads((a / "manifest.json").read_text())["frames"]:
+        name = fr["files"]["depth"]
+        assert (a / name).read_bytes() == (b / name).read_bytes()
