@@ -78,3 +78,29 @@ def test_arming_is_idempotent_and_preserves_the_running_debt(be):
     assert np.any(before != 0.0)
     be.arm_comp(st)
     assert np.array_equal(be.hcomp(st), before)
+
+
+def test_uniform_rain_balances_to_gate(be):
+    """solver/core/test_massbalance.py:41: 40 steps of 50 mm/h on a closed basin close the ledger."""
+    st = be.make(np.zeros((16, 16), np.float32), 10.0, depth=0.2, manning=0.03)
+    led = be.ledger(st)
+    rain, t = 50.0 / 1000.0 / 3600.0, 0.0
+    for _ in range(40):
+        dt = be.compute_dt(st, LI, 0.5, 5.0)
+        be.step(st, LI, dt, rain=rain)
+        led.add_rain_step(rain, dt, be.n_cells(st))
+        t += dt
+    rec = led.record(st, t)
+    assert led.max_rel_error < 1e-6 and rec.volume > led.v0
+
+
+def test_uncapped_infiltration_removes_exactly_its_rate(be):
+    """solver/core/test_massbalance.py:81: 20 steps of 2 s at 5e-5 m/s on 0.3 m of water
+    bank rate x time x area, to 1e-3 (the mass gate cannot see a mis-scaled rate)."""
+    rate = 5.0e-5
+    st = be.make(np.zeros((5, 5), np.float32), 10.0, depth=0.3)
+    be.set_infil(st, np.full((5, 5), rate, np.float32))
+    for _ in range(20):
+        be.step(st, LI, 2.0)
+    want = rate * 2.0 * 20 * be.cell_area(st) * be.n_cells(st)
+    assert abs(be.loss_volume(st) - want) < 1e-3 * want
