@@ -1,6 +1,8 @@
-"""Areal rain sources: the reference's remaining source tests on the oracle.
+"""Areal rain sources and the sinks beside them: the reference's remaining tests on the oracle.
 
-These restate solver/core/test_sources.py:109, :180, :202 and :225. The rest of
+These restate solver/core/test_sources.py:109, :180, :202 and :225, and
+solver/core/test_massbalance.py:41 and :81 (uniform rain balancing to the gate, the
+uncapped infiltration rate). The rest of
 that file is in tests/gates.py (sub-ulp rain, the compensation canary, storm drift,
 the field on both schemes). Those gates run on the CUDA path too, and the CUDA rain
 paths equal the oracle bit for bit on the golden rain cases.
