@@ -1,14 +1,18 @@
 """The bedload law, its face integral and Exner: the reference's kernel tests on the oracle.
 
-These restate solver/core/test_sediment.py:174-640 against the oracle's
-``rbo_accumulate_qs``, ``rbo_exner_update`` and ``rbo_rebuild_bed``, and against
+These restate solver/core/test_sediment.py:174-740 against the oracle's
+``rbo_accumulate_qs``, ``rbo_accumulate_qs_channels``, ``rbo_exner_update`` and
+``rbo_rebuild_bed``, and against
 this package's host references (``rbsim.sediment``). The CUDA step fuses the same
 face integral into the local-inertial tile and runs the same Exner update in
 ``rb_exner_apply``. It equals the oracle bit for bit on the golden sediment cases and
 on the long bed-wave run. The checks are: MPM by hand; a bit-exact zero below
 threshold and on dry faces; the integral equal to transport times elapsed time, with
 its compensation kept; the x and y kernels transposes of each other; Exner's
-divergence, bounds and banking; and the bed rebuilt from the pristine bed.
+divergence, bounds and banking; and the bed rebuilt from the pristine bed. Also a
+channel face carries its conveyance fraction, the channel kernel collapses onto the
+plain one at zero width, clearing keeps the compensation debt, and a zero grain size
+does not immobilise a cell.
 """
 
 from __future__ import annotations
@@ -232,3 +236,67 @@ def test_no_shear_means_no_celerity():
     assert float(bed_celerity(0.0, 1.0, 0.03, 0.008, 0.4)) == 0.0
     assert float(shields_from_flow(1.0, 20.0, 0.03, 0.008)) < SHIELDS_CRITICAL
     assert float(bed_celerity(1.0, 20.0, 0.03, 0.008, 0.4)) == 0.0
+
+
+def accumulate_channels(qx_ch, qx_fp, eta, z, n, d50, w, d, cn, dx, dt, acc):
+    """One ``rbo_accumulate_qs_channels`` call over x-faces (the y components are zero)."""
+    ny, nx = z.shape
+    zy = np.zeros((ny + 1, nx), np.float32)
+    args = [_f32(a) for a in (qx_ch, qx_fp)] + [zy, zy.copy()] + [_f32(a) for a in (eta, z, n, d50, w, d, cn)]
+    oracle.lib().rbo_accumulate_qs_channels_f32(ny, nx, *(_p(a) for a in args), ctypes.c_float(dx),
+                                                ctypes.c_float(dt), *(_p(a) for a in acc))  # fmt: skip
+
+
+def test_a_channel_face_carries_its_conveyance_fraction():
+    """test_sediment.py:402: with the floodplain dry, the cell-width flux is the channel's
+    capacity (from its own depth and radius A/P) scaled by w / dx."""
+    ny, nx, dx = 1, 4, 200.0
+    w, bank, n_ch, d50, h_ch, q_ch = 20.0, 1.0, 0.028, 0.008, 0.5, 1.8
+    z = np.full((ny, nx), 10.0, np.float32)
+    acc = new_acc(ny, nx)
+    accumulate_channels(np.full((ny, nx + 1), q_ch), np.zeros((ny, nx + 1)), z - bank + h_ch, z,
+                        np.full((ny, nx), 0.05), np.full((ny, nx), d50), np.full((ny, nx), w),
+                        np.full((ny, nx), bank), np.full((ny, nx), n_ch), dx, 1.0, acc)  # fmt: skip
+    qs_channel = float(capacity_from_flow(q_ch, h_ch, n_ch, d50, radius=w * h_ch / (w + 2.0 * h_ch)))
+    assert qs_channel > 0.0
+    assert float(acc[0][0, 1]) * dx == pytest.approx(qs_channel * w, rel=1e-4)
+    assert float(capacity_from_flow(q_ch, h_ch * w / dx, n_ch, d50)) > 10.0 * qs_channel
+
+
+def test_the_channel_kernel_collapses_onto_the_plain_one_at_zero_width():
+    """test_sediment.py:446: w = d = 0 is the no-channel case, bit for bit."""
+    ny, nx, dx, dt = 3, 6, 50.0, 3.0
+    rng = np.random.default_rng(3)
+    z = (10.0 - 0.05 * np.arange(nx)[None, :] * np.ones((ny, 1))).astype(np.float32)
+    eta = (z + rng.uniform(0.3, 1.5, (ny, nx))).astype(np.float32)
+    qx = rng.uniform(-2.0, 2.0, (ny, nx + 1)).astype(np.float32)
+    n, d50, zero = np.full((ny, nx), 0.033), np.full((ny, nx), 0.006), np.zeros((ny, nx))
+    plain, chan = new_acc(ny, nx), new_acc(ny, nx)
+    accumulate(qx, np.zeros((ny + 1, nx)), eta, z, n, d50, dt, plain)
+    accumulate_channels(np.zeros((ny, nx + 1)), qx, eta, z, n, d50, zero, zero, zero, dx, dt, chan)
+    assert (plain[0] == chan[0]).all() and (plain[1] == chan[1]).all() and np.abs(plain[0]).max() > 0.0
+
+
+def test_clearing_keeps_the_compensation_debt():
+    """test_sediment.py:479: an activation consumes the integral; the bits it never held stay owed."""
+    st = oracle.State.from_bed(np.full((2, 3), 5.0, np.float32), 10.0, depth=0.5)
+    st.arm_sediment(0.002, 0.4)
+    sed = st.sediment
+    sed.qs_int_x[...] = 4.0
+    sed.qs_comp_x[...] = 1.25e-9
+    lo, hi = np.full((2, 3), -np.inf, np.float32), np.full((2, 3), np.inf, np.float32)
+    oracle.exner_activate(st, lo, hi)
+    assert (sed.qs_int_x == 0.0).all() and (sed.qs_comp_x == np.float32(1.25e-9)).all()
+
+
+def test_a_zero_grain_size_does_not_make_a_cell_immobile():
+    """test_sediment.py:727: d50 is face-averaged, so a lone zero cell's faces still transport
+    and its bed moves (immobility is what a zero alluvium bound is for)."""
+    ny, nx = 1, 3
+    d50 = np.array([[0.004, 0.0, 0.004]], np.float32)
+    acc = new_acc(ny, nx)
+    accumulate(np.array([[0.0, 2.0, 2.6, 0.0]]), np.zeros((ny + 1, nx)), np.ones((ny, nx)), np.zeros((ny, nx)),
+               np.full((ny, nx), 0.03), d50, 60.0, acc)  # fmt: skip
+    assert (acc[0][0, 1:3] != 0.0).all()
+    dz, _ = exner(acc[0], acc[2], dx=5.0)
+    assert dz[0, 1] != 0.0
