@@ -300,3 +300,50 @@ def test_a_zero_grain_size_does_not_make_a_cell_immobile():
     assert (acc[0][0, 1:3] != 0.0).all()
     dz, _ = exner(acc[0], acc[2], dx=5.0)
     assert dz[0, 1] != 0.0
+
+
+def _armed_reach():
+    """A wet 4 x 6 reach with a bedload integral of an uneven flow, armed at bed z0."""
+    ny, nx = 4, 6
+    rng = np.random.default_rng(8)
+    st = oracle.State.from_bed((100.0 + 0.02 * rng.standard_normal((ny, nx))).astype(np.float32), 10.0, depth=0.6)
+    st.arm_sediment(0.004, 0.4)
+    acc = new_acc(ny, nx)
+    accumulate(rng.uniform(0.5, 3.0, (ny, nx + 1)), rng.uniform(-1.0, 1.0, (ny + 1, nx)), st.z + st.h, st.z,
+               np.full((ny, nx), 0.03), np.full((ny, nx), 0.004), 30.0, acc)  # fmt: skip
+    sed = st.sediment
+    sed.qs_int_x[...], sed.qs_comp_x[...], sed.qs_int_y[...], sed.qs_comp_y[...] = acc
+    return st
+
+
+def test_an_activation_rebuilds_the_bed_from_z0_and_leaves_the_water():
+    """solver/processes/test_morphology.py:164, :194: z = float32(z0 + dz_cum), the integral
+    cleared, depth untouched, eta refreshed from the new bed."""
+    st = _armed_reach()
+    h0, z0 = st.h.copy(), st.sediment.z0.copy()
+    free = np.full(z0.shape, -np.inf, np.float32), np.full(z0.shape, np.inf, np.float32)
+    oracle.exner_activate(st, *free)
+    sed = st.sediment
+    assert np.abs(sed.dz_cum).max() > 0.0
+    assert (st.z == (z0.astype(np.float64) + sed.dz_cum).astype(np.float32)).all()
+    assert (sed.qs_int_x == 0.0).all() and (sed.qs_int_y == 0.0).all()
+    assert (st.h == h0).all() and (st.eta == (st.h + st.z)).all()
+
+
+def test_a_frozen_cell_banks_exactly_what_the_free_bed_moved_there():
+    """solver/processes/test_morphology.py:257: the same integral applied with and without a
+    frozen cell; the frozen run keeps that cell's bed and banks the free run's change there."""
+    free_st, frozen_st = _armed_reach(), _armed_reach()
+    shape = free_st.z.shape
+    lo, hi = np.full(shape, -np.inf, np.float32), np.full(shape, np.inf, np.float32)
+    oracle.exner_activate(free_st, lo, hi)
+    lo_f, hi_f = lo.copy(), hi.copy()
+    lo_f[2, 3] = hi_f[2, 3] = 0.0
+    oracle.exner_activate(frozen_st, lo_f, hi_f)
+    want = free_st.sediment.dz_cum[2, 3]
+    assert want != 0.0
+    assert frozen_st.sediment.dz_cum[2, 3] == 0.0 and frozen_st.z[2, 3] == frozen_st.sediment.z0[2, 3]
+    assert frozen_st.sediment.dz_unapplied[2, 3] == want
+    others = np.ones(shape, bool)
+    others[2, 3] = False
+    assert (frozen_st.sediment.dz_cum[others] == free_st.sediment.dz_cum[others]).all()
